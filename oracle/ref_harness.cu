@@ -1,0 +1,391 @@
+// Test harness around the reference's OWN CUDA kernels and host drivers
+// (test infrastructure only).  oracle/Makefile compiles the reference sources
+// from the reference tree together with this file into oracle/_ref/libdemref.so;
+// tests/golden/make_golden.py and bench.py load it with ctypes on a GPU box to
+// produce golden vectors and the reference-GPU timing.  Nothing here is part of
+// the product.
+//
+// Every entry point takes and returns host arrays in the reference layout
+// (SoA x[0..N) y[N..2N) z[2N..3N); IonP slots per particle; float3 per slot)
+// and launches the reference kernels exactly as its drivers do
+// (md_calculationuniaxialcompression.cu:155-314, md_calculationbraziltest.cu:144-231).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unistd.h>
+#include <sys/stat.h>
+
+#include "md.h"
+#include "mp.h"
+
+namespace {
+
+int g_err = 0;
+void chk(cudaError_t e) {
+  if (e != cudaSuccess && g_err == 0) g_err = (int)e;
+}
+
+struct DevArrays {
+  float *R = nullptr, *V = nullptr, *W = nullptr, *F = nullptr, *M = nullptr, *Oiwt = nullptr;
+  uint *IL = nullptr, *ILtype = nullptr;
+  float* invL0 = nullptr;
+  float3 *Rij = nullptr, *Oijt = nullptr, *Mijn = nullptr, *Mijt = nullptr, *Fijn = nullptr, *Fijt = nullptr,
+         *Mijadd = nullptr;
+};
+
+template <class T>
+T* dalloc(size_t n) {
+  T* p = nullptr;
+  chk(cudaMalloc((void**)&p, n * sizeof(T) + 64));
+  chk(cudaMemset(p, 0, n * sizeof(T) + 64));
+  return p;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+// cell_data set-up identical to cuc_createCD (md_calculationuniaxialcompression.cu:65-74)
+void cells_create(md_task_data& td) {
+  chk(cudaMalloc((void**)&td.C.d_IP, td.P.N * sizeof(uint)));
+  d_FillIndex<<<td.A.bloks, SMEMDIM>>>(td.C.d_IP, td.P.N);
+  chk(cudaMalloc((void**)&td.C.d_CI, td.P.N * sizeof(uint)));
+  chk(cudaMalloc((void**)&td.C.d_CIs, 2 * td.P.N * sizeof(uint) + 64));
+  chk(cudaMemset(td.C.d_CIs, 0xFF, 2 * td.P.N * sizeof(uint) + 64));
+  chk(cudaMalloc((void**)&td.C.d_pnC, 2 * td.C.N * sizeof(uint)));
+  td.C.dtmpN_old = 128;
+  chk(cudaMalloc((void**)&td.C.d_tmp_old, td.C.dtmpN_old));
+}
+
+void cells_free(md_task_data& td) {
+  dfree(td.C.d_IP);
+  dfree(td.C.d_CI);
+  dfree(td.C.d_CIs);
+  dfree(td.C.d_pnC);
+  dfree(td.C.d_tmp_old);
+  td.C.d_IP = td.C.d_CI = td.C.d_CIs = td.C.d_pnC = nullptr;
+  td.C.d_tmp_old = td.C.d_tmp = nullptr;
+}
+
+void setup_task(md_task_data& td, uint32_t N, float a, uint32_t nx, uint32_t ny, uint32_t nz) {
+  initArrays(td.A, td.P, td.C, td.IL, td.R);
+  td.P.N = N;
+  td.C.a = a;
+  td.C._1d_a = 1.0 / double(a);
+  td.C.Nr = make_uint3(nx, ny, nz);
+  td.C.N = nx * ny * nz;
+  td.A.CalculateParameters(N, N * 32);
+}
+
+}  // namespace
+
+extern "C" {
+
+int refh_last_error(void) { return g_err; }
+
+// CellDistribution (md_cell_distribution.cu:130-179) on given positions.
+int refh_cell_distribution(const float* hR, uint32_t N, float a, uint32_t nx, uint32_t ny, uint32_t nz,
+                           uint32_t* CI, uint32_t* CIs, uint32_t* pnC) {
+  g_err = 0;
+  md_task_data td;
+  setup_task(td, N, a, nx, ny, nz);
+  td.P.d_R = dalloc<float>(3 * N);
+  chk(cudaMemcpy(td.P.d_R, hR, 3 * N * sizeof(float), cudaMemcpyHostToDevice));
+  cells_create(td);
+  CellDistribution(td.P, td.A, td.S, td.C);
+  chk(cudaDeviceSynchronize());
+  chk(cudaMemcpy(CI, td.C.d_CI, N * sizeof(uint), cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(CIs, td.C.d_CIs, 2 * N * sizeof(uint), cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(pnC, td.C.d_pnC, 2 * td.C.N * sizeof(uint), cudaMemcpyDeviceToHost));
+  cells_free(td);
+  dfree(td.P.d_R);
+  td.P.d_R = nullptr;
+  return g_err;
+}
+
+// Set-up of a loading test: CellDistribution + InteractionListConstruct +
+// d_ConstructBoundInteractions + d_DeleteFarLinks
+// (md_calculationuniaxialcompression.cu:155-157, 212-213).
+int refh_setup_bonds(const float* hR, uint32_t N, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t IonP,
+                     float il_aacut, float aa_farcut, float b_dd, float b_r, uint32_t* IL, uint32_t* ILtype,
+                     float* invL0) {
+  g_err = 0;
+  md_task_data td;
+  setup_task(td, N, a, nx, ny, nz);
+  size_t S = (size_t)N * IonP;
+  DevArrays d;
+  td.P.d_R = dalloc<float>(3 * N);
+  td.P.d_V = dalloc<float>(3 * N);
+  td.P.d_W = dalloc<float>(3 * N);
+  chk(cudaMemcpy(td.P.d_R, hR, 3 * N * sizeof(float), cudaMemcpyHostToDevice));
+  td.IL.IonP = IonP;
+  td.IL.N = S;
+  td.IL.aacut = il_aacut;
+  td.IL.d_IL = dalloc<uint>(S);
+  td.IL.d_ILtype = dalloc<uint>(S);
+  td.IL.d_1d_iL = dalloc<float>(S);
+  td.IL.d_rij = dalloc<float3>(S);
+  td.IL.d_Oijt = dalloc<float3>(S);
+  td.IL.d_Fijn = dalloc<float3>(S);
+  td.IL.d_Fijt = dalloc<float3>(S);
+  td.IL.d_Mijn = dalloc<float3>(S);
+  td.IL.d_Mijt = dalloc<float3>(S);
+  td.IL.d_Mijadd = dalloc<float3>(S);
+  cells_create(td);
+  CellDistribution(td.P, td.A, td.S, td.C);
+  InteractionListConstruct(td.P, td.A, td.S, td.IL, td.C);
+  d_ConstructBoundInteractions<<<td.A.bloks, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                                        td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Fijn,
+                                                        td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt, td.IL.d_Mijadd,
+                                                        N, IonP, b_dd, b_r);
+  d_DeleteFarLinks<<<td.A.bloks, SMEMDIM>>>(td.P.d_R, N, td.IL.d_IL, td.IL.d_ILtype, td.IL.d_1d_iL, td.IL.d_rij,
+                                            td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                            td.IL.d_Mijadd, IonP, aa_farcut);
+  chk(cudaDeviceSynchronize());
+  chk(cudaMemcpy(IL, td.IL.d_IL, S * sizeof(uint), cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(ILtype, td.IL.d_ILtype, S * sizeof(uint), cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(invL0, td.IL.d_1d_iL, S * sizeof(float), cudaMemcpyDeviceToHost));
+  cells_free(td);
+  dfree(td.P.d_R);
+  dfree(td.P.d_V);
+  dfree(td.P.d_W);
+  dfree(td.IL.d_IL);
+  dfree(td.IL.d_ILtype);
+  dfree(td.IL.d_1d_iL);
+  dfree(td.IL.d_rij);
+  dfree(td.IL.d_Oijt);
+  dfree(td.IL.d_Fijn);
+  dfree(td.IL.d_Fijt);
+  dfree(td.IL.d_Mijn);
+  dfree(td.IL.d_Mijt);
+  dfree(td.IL.d_Mijadd);
+  return g_err;
+}
+
+// Scalars of one loading step.  All float, as the reference passes them to its
+// kernels (md_calculationuniaxialcompression.cu:269-310).
+typedef struct {
+  float a;
+  uint32_t nx, ny, nz, IonP;
+  float il_aacut, aa_farcut;
+  float dt, m_E, m_G, b_r, m_Ec, m_Gc;
+  float hm_E, hm_G, p_A, p_mu, p_mur, p_m, p_r;
+  float wall_E, wall_G;        // 2*hm_E, 2*hm_G (uniaxial) or hm_E, hm_G (Brazilian)
+  float center[3];             // Compress.center
+  float wall_RR, wall_top, wall_bot, wall_V, Zcut;
+  float dt_d_m, dt_d_I;
+  float s_center[3], s_spacesized2[3], hidenpoint[3];  // S.center, S.spacesized2, S.hidenpoint
+  int brazil;
+  int stages;                  // bit 0: rebuild IL; 1: forces; 2: platen; 3: increments; 4: cut; 5: delete far
+} refh_step_params;
+
+// One pass of the hot loop body (cells, IL rebuild, forces, platen, increments,
+// escape restriction, far-link deletion) on a full state; FL returns the
+// per-block platen partials (2*bloks floats).
+int refh_step(const refh_step_params* p, uint32_t N, float* R, float* V, float* W, float* F, float* M, float* Oiwt,
+              uint32_t* IL, uint32_t* ILtype, float* invL0, float* Rij, float* Oijt, float* Mijn, float* Mijt,
+              float* FL) {
+  g_err = 0;
+  md_task_data td;
+  setup_task(td, N, p->a, p->nx, p->ny, p->nz);
+  const uint32_t IonP = p->IonP;
+  size_t S = (size_t)N * IonP;
+  td.P.d_R = dalloc<float>(3 * N);
+  td.P.d_V = dalloc<float>(3 * N);
+  td.P.d_W = dalloc<float>(3 * N);
+  td.P.d_F = dalloc<float>(3 * N);
+  td.P.d_M = dalloc<float>(3 * N);
+  td.P.d_Oiwt = dalloc<float>(3 * N);
+  td.IL.IonP = IonP;
+  td.IL.N = S;
+  td.IL.aacut = p->il_aacut;
+  td.IL.d_IL = dalloc<uint>(S);
+  td.IL.d_ILtype = dalloc<uint>(S);
+  td.IL.d_1d_iL = dalloc<float>(S);
+  td.IL.d_rij = dalloc<float3>(S);
+  td.IL.d_Oijt = dalloc<float3>(S);
+  td.IL.d_Fijn = dalloc<float3>(S);
+  td.IL.d_Fijt = dalloc<float3>(S);
+  td.IL.d_Mijn = dalloc<float3>(S);
+  td.IL.d_Mijt = dalloc<float3>(S);
+  td.IL.d_Mijadd = dalloc<float3>(S);
+  td.R.d_FL = dalloc<float>(2 * td.A.bloks);
+  chk(cudaMemcpy(td.P.d_R, R, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_V, V, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_W, W, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_F, F, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_M, M, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_Oiwt, Oiwt, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_IL, IL, S * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_ILtype, ILtype, S * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_1d_iL, invL0, S * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_rij, Rij, S * 12, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_Oijt, Oijt, S * 12, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_Mijn, Mijn, S * 12, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_Mijt, Mijt, S * 12, cudaMemcpyHostToDevice));
+  cells_create(td);
+  const uint bl = td.A.bloks;
+  if (p->stages & 1) {
+    CellDistribution(td.P, td.A, td.S, td.C);
+    InteractionListReConstructBPM(td.P, td.A, td.S, td.IL, td.C);
+  }
+  if (p->stages & 2) {
+    chk(cudaMemset(td.P.d_F, 0, 3 * N * sizeof(float)));
+    chk(cudaMemset(td.P.d_M, 0, 3 * N * sizeof(float)));
+    if (p->brazil)
+      d_CalculateForcesDEM_22<<<4 * bl, 256>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                               td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                               td.P.d_F, td.P.d_M, N, IonP, p->dt, p->m_E, p->m_G, p->b_r, p->m_Ec,
+                                               p->m_Gc);
+    else
+      d_CalculateForcesDEM_22<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                               td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                               td.P.d_F, td.P.d_M, N, IonP, p->dt, p->m_E, p->m_G, p->b_r, p->m_Ec,
+                                               p->m_Gc);
+    d_CalculateForcesDEM_21<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                             td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.P.d_F, td.P.d_M, N, IonP,
+                                             p->dt, p->hm_E, p->hm_G, p->p_A, p->p_mu, p->p_mur, p->p_m, p->p_r);
+  }
+  if (p->stages & 4) {
+    float3 c = make_float3(p->center[0], p->center[1], p->center[2]);
+    if (p->brazil)
+      d_BrazilCompression_hm<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_Oiwt, td.P.d_F, td.P.d_M, N, p->dt,
+                                              p->wall_E, p->wall_G, p->p_A, p->p_mu, p->p_mur, p->p_m, p->p_r,
+                                              td.R.d_FL, c, p->wall_RR, p->wall_top, p->wall_bot, p->wall_V, p->Zcut);
+    else
+      d_UniaxialCompression_hm<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_Oiwt, td.P.d_F, td.P.d_M, N,
+                                                p->dt, p->wall_E, p->wall_G, p->p_A, p->p_mu, p->p_mur, p->p_m,
+                                                p->p_r, td.R.d_FL, c, p->wall_RR, p->wall_top, p->wall_bot, p->wall_V,
+                                                p->Zcut);
+  }
+  if (p->stages & 8)
+    d_CalculateIncrementsDEM<<<bl, SMEMDIM>>>(td.P.d_F, td.P.d_V, td.P.d_R, td.P.d_M, td.P.d_W, N, p->dt_d_m, p->dt,
+                                              p->dt_d_I);
+  if (p->stages & 16) {
+    float3 c = make_float3(p->s_center[0], p->s_center[1], p->s_center[2]);
+    float3 s2 = make_float3(p->s_spacesized2[0], p->s_spacesized2[1], p->s_spacesized2[2]);
+    float3 hp = make_float3(p->hidenpoint[0], p->hidenpoint[1], p->hidenpoint[2]);
+    d_ParallelepipedCutRestriction<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_F, N, c, s2, hp);
+  }
+  if (p->stages & 32)
+    d_DeleteFarLinks<<<bl, SMEMDIM>>>(td.P.d_R, N, td.IL.d_IL, td.IL.d_ILtype, td.IL.d_1d_iL, td.IL.d_rij,
+                                      td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                      td.IL.d_Mijadd, IonP, p->aa_farcut);
+  chk(cudaDeviceSynchronize());
+  chk(cudaGetLastError());
+  chk(cudaMemcpy(R, td.P.d_R, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(V, td.P.d_V, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(W, td.P.d_W, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(F, td.P.d_F, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(M, td.P.d_M, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(Oiwt, td.P.d_Oiwt, 3 * N * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(IL, td.IL.d_IL, S * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(ILtype, td.IL.d_ILtype, S * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(invL0, td.IL.d_1d_iL, S * 4, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(Rij, td.IL.d_rij, S * 12, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(Oijt, td.IL.d_Oijt, S * 12, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(Mijn, td.IL.d_Mijn, S * 12, cudaMemcpyDeviceToHost));
+  chk(cudaMemcpy(Mijt, td.IL.d_Mijt, S * 12, cudaMemcpyDeviceToHost));
+  if (FL) chk(cudaMemcpy(FL, td.R.d_FL, 2 * bl * 4, cudaMemcpyDeviceToHost));
+  cells_free(td);
+  void* ps[] = {td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_F, td.P.d_M, td.P.d_Oiwt, td.IL.d_IL, td.IL.d_ILtype,
+                td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                td.IL.d_Mijadd, td.R.d_FL};
+  for (void* q : ps) dfree(q);
+  return g_err;
+}
+
+// Full reference loading test through the reference's own entry points:
+// h_LoadCylinderSample + compression_data::Calculate{U,B}Parameters +
+// h_Calculation{UniaxialCompression,BrazilTest} (mp_calculateonesample.cu:151-214).
+// The sample file ./result/Sample_<isample><part>.txt must exist under workdir.
+typedef struct {
+  double E, Ec, Gc, b_r, gap;      // SI units, as mp_calculateonesample.cu:47-51 receives them
+  double p_r_m, rho, nu, p_e, p_mu, p_mur, farcut_factor;
+  double space_si[3], lsi[3];      // SpaceSize and LSi (metres), mp_calculateonesample.cu:91
+  double velocity_si, minstress_si, maxstrain, condfract;
+  uint32_t dNsave, fileN, isample;
+} refh_test_params;
+
+typedef struct {
+  double FractureStress, FractureStrain, LinearityDeviation, Destruction, Strain;
+  double dt, seconds;
+  uint64_t steps_hint;
+  uint32_t N, stepsave;
+} refh_test_result;
+
+int refh_run_test(int brazil, const char* workdir, const char* part, const refh_test_params* q,
+                  refh_test_result* out) {
+  g_err = 0;
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof cwd)) return -1;
+  if (chdir(workdir) != 0) return -2;
+  mkdir("result", 0755);
+  {
+    mp_mdparameters_data mpMDP;
+    md_task_data& td = mpMDP.mdTD[0];
+    initArrays(td.A, td.P, td.C, td.IL, td.R);
+    // SetInitialParameters (mp_determineconjgradient.cu:15-47) with caller values
+    td.IL.IonP = 32;
+    td.Po.m_nu = q->nu;
+    td.Po.m_E = q->E / stress_const;
+    td.Po.m_Ec = q->Ec / stress_const;
+    td.Po.m_Gc = q->Gc / stress_const;
+    td.Po.m_ro = q->rho / density_const;
+    td.Po.b_r = q->b_r / length_const;
+    td.Po.p_r = q->p_r_m / length_const;
+    td.Po.b_d = 2.0 * td.Po.p_r + q->gap / length_const;
+    td.Po.p_e = q->p_e;
+    td.Po.p_mu = q->p_mu;
+    td.Po.p_mur = q->p_mur;
+    td.Po.nuV = 1e-5;
+    td.Po.nuW = 1e-3;
+    td.Po.a_farcut = q->farcut_factor * td.Po.p_r;
+    td.C.a = 2.0 * td.Po.a_farcut;
+    td.Po.CalculateParameters();
+    const uint i = q->isample;
+    mpMDP.S[i].SetSpaceSizeSi(q->space_si[0], q->space_si[1], q->space_si[2]);
+    mpMDP.S[i].SetLSi(q->lsi[0], q->lsi[1], q->lsi[2], td.Po.p_r);
+    mpMDP.S[i].SetAxis(0.0, 0.0, 1.0);
+    mpMDP.S[i].CalculateParameters(td.C.a, td.Po.p_r);
+    std::string pt(part);
+    h_LoadCylinderSample(mpMDP, i, (char*)pt.c_str());
+    td.S = mpMDP.S[i];
+    td.P.N = mpMDP.PN[i];
+    td.Compress.VLoad = q->velocity_si / velocity_const;
+    if (brazil)
+      td.Compress.CalculateBParameters(td.S.size_real, td.S.center_real, td.Po, q->minstress_si / stress_const,
+                                       q->maxstrain, q->condfract);
+    else
+      td.Compress.CalculateUParameters(td.S.size_real, td.S.center_real, td.Po, q->minstress_si / stress_const,
+                                       q->maxstrain, q->condfract);
+    td.R.dNsave = q->dNsave;
+    td.R.fileN = q->fileN;
+    auto t0 = std::chrono::steady_clock::now();
+    if (brazil)
+      h_CalculationBrazilTest(td, mpMDP.h_R[i]);
+    else
+      h_CalculationUniaxialCompression(td, mpMDP.h_R[i]);
+    cudaDeviceSynchronize();
+    auto t1 = std::chrono::steady_clock::now();
+    out->FractureStress = td.Compress.FractureStress;
+    out->FractureStrain = td.Compress.FractureStrain;
+    out->LinearityDeviation = td.Compress.LinearityDeviation;
+    out->Destruction = td.R.Destruction;
+    out->Strain = td.Compress.Strain;
+    out->dt = td.Po.dt;
+    out->seconds = std::chrono::duration<double>(t1 - t0).count();
+    out->N = td.P.N;
+    out->stepsave = td.R.stepsave;
+    out->steps_hint = 0;
+  }
+  chk(cudaGetLastError());
+  if (chdir(cwd) != 0) return -3;
+  return g_err;
+}
+
+}  // extern "C"

@@ -1,0 +1,314 @@
+"""Benchmark of the bonded-particle DEM step (BPM + Hertz-Mindlin) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload brazilian_disc|uniaxial_cylinder]
+
+A step is one DEM time step of a loading test (pair forces, platens,
+integration, loading controller; contact-list rebuilds when needed) over the
+whole specimen.  The default workload is the Brazilian disc 40 mm x 20 mm
+with radii U[0.18, 0.30] mm (~245k spheres, seeded synthetic packing).
+Metric: particle-steps/s (particles x steps / device time, all ranks summed).
+
+Under torchrun every rank runs its own specimen (different seed) on its own
+GPU: the specimens are independent, so the work shards with no data-path
+collective (weak scaling); the timing barrier and max-over-ranks use
+torch.distributed.
+
+--impl reference times the CPU restatement of the reference step (oracle,
+all host threads) on a bounded number of steps of the same specimen.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BPM particle-steps/s"
+UNIT = "particle-steps/s"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    def __init__(self, ws):
+        self.ws = ws
+        self.pg = None
+        if ws > 1:
+            import datetime
+
+            import torch.distributed as td
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            td.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.td = td
+
+    def barrier(self):
+        if self.ws > 1:
+            self.td.barrier()
+
+    def max(self, v: float) -> float:
+        if self.ws == 1:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if self.ws == 1:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            self.td.destroy_process_group()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1].split()[0]))
+                mx.append(float(r[2].split()[0]))
+                for k, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_specimen(dem, workload: str, seed: int, device: int):
+    W = importlib.import_module("dem-rock-calibration_b200.workloads")
+    return getattr(W, workload)(seed=seed, pack_kw=dict(device=device))
+
+
+def algorithmic_bytes(n, bonds, touching, fp64=False):
+    """Per step: 60 N + 104 B + 28 C bytes (FP32), 120 N + 204 B + 52 C (FP64):
+    particle R,V,W read + F,M written; per undirected bond j, L0 and four
+    3-vector histories read and written; per touching contact j and the
+    tangential history read and written."""
+    if fp64:
+        return 120.0 * n + 204.0 * bonds + 52.0 * touching
+    return 60.0 * n + 104.0 * bonds + 28.0 * touching
+
+
+def cpu_baseline(spec, nsteps: int, threads: int):
+    """The oracle's full loop body (cells, interaction-list rebuild, BPM, HM,
+    platens, integration, escape parking, far-link deletion) on host cores."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle import lib as L
+    from oracle import params as prm
+    from oracle import sim
+
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    L.lib().orc_set_threads(threads)
+    n = spec.n
+    mat, ld = spec.material, spec.loading
+    r_mean = float(np.mean(spec.radii))
+    a_far = mat.farcut * mat.p_r
+    C_a = float(np.float32(2.0 * a_far))
+    B = [ld.space_center[d] + ld.space_half[d] + 1.01 * C_a for d in range(3)]
+    cells = prm.cells_for(2.0 * a_far, B)
+    st = sim.RefState.empty(n)
+    st.R[:] = spec.xyz
+    # per-particle constants as the engine derives them
+    rad = spec.radii.astype(np.float32)
+    r = rad.astype(np.float64)
+    mass = mat.rho * (4.0 * (1.0 / 3.0) * np.pi * r ** 3)
+    dt = mat.dt_rayleigh_factor * np.pi * r.min() * np.sqrt(2.0 * mat.rho * (1.0 + mat.nu)) / (
+        np.sqrt(mat.E) * (0.163 * mat.nu + 0.8766))
+    dtm = ((1.0 / mass) * dt).astype(np.float32)
+    dtI = (dt / (0.4 * mass * r * r)).astype(np.float32)
+    hmE = 0.5 * mat.E / (1 - mat.nu ** 2)
+    Gp = 0.5 * mat.E / (1 + mat.nu)
+    hmG = 0.5 * Gp / (2 - mat.nu)
+    le = np.log(mat.p_e)
+    pA = le / np.sqrt(np.pi ** 2 + le ** 2)
+    Eb = mat.E_bond
+    Gb = Eb / mat.kn_ks
+    sc = sim.Scalars(a=cells.a, inv_a=cells.inv_a, nx=cells.nx, ny=cells.ny, nz=cells.nz, IonP=32,
+                     il_aacut=prm.il_aacut(a_far), aa_farcut=prm.F(a_far * a_far), dt=prm.F(dt), m_E=prm.F(Eb),
+                     m_G=prm.F(Gb), b_r=0.0, m_Ec=prm.F(mat.Ec), m_Gc=prm.F(mat.Gc), hm_E=prm.F(hmE),
+                     hm_G=prm.F(hmG), p_A=prm.F(pA), p_mu=prm.F(mat.mu), p_mur=prm.F(mat.mur), p_m=0.0, p_r=r_mean,
+                     wall_E=prm.F(hmE), wall_G=prm.F(hmG), center=np.array(ld.center_real[:], np.float32),
+                     wall_RR=float(np.float32(0.5 * ld.size_real[0]) ** 2), wall_top=prm.F(ld.center_real[1] +
+                                                                                        0.5 * ld.size_real[1]),
+                     wall_bot=prm.F(ld.center_real[1] - 0.5 * ld.size_real[1]), wall_V=prm.F(ld.velocity),
+                     Zcut=prm.F(ld.zcut), dt_d_m=0.0, dt_d_I=0.0,
+                     s_center=np.array(ld.space_center[:], np.float32),
+                     s_spacesized2=np.array(ld.space_half[:], np.float32),
+                     hidenpoint=np.array(ld.hidden_point[:], np.float32), brazil=1)
+    sim.oracle_setup_bonds(st, sc, rad=rad, gap=mat.gap)
+    # per-slot bond radius and strengths (0.8 min r, mean strengths)
+    IL = st.IL.reshape(n, 32)
+    jj = np.where(IL == L.EMPTY, 0, IL)
+    slot_br = (0.8 * np.minimum(rad[:, None], rad[jj])).astype(np.float32).reshape(-1)
+    slot_sn = np.full(n * 32, prm.F(mat.Ec), np.float32)
+    slot_st = np.full(n * 32, prm.F(mat.Gc), np.float32)
+    kw = dict(rad=rad, mass=mass.astype(np.float32), slot_br=slot_br, slot_sn=slot_sn, slot_st=slot_st,
+              dtm_i=dtm, dtI_i=dtI)
+    sim.oracle_step(st, sc, **kw)  # warm caches / first-touch
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        sim.oracle_step(st, sc, **kw)
+    el = time.perf_counter() - t0
+    return n * nsteps / el, el, L.lib().orc_get_threads()
+
+
+def run_reference(args, ws, rank, local):
+    """--impl reference: the CPU restatement on host cores (rank 0 only)."""
+    if rank != 0:
+        return 0
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    spec = build_specimen(dem, args.workload, 1, local)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, args.ref_steps))
+    v, el, th = cpu_baseline(spec, steps, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded packing)",
+            "config": {"workload": f"{args.workload}: {spec.n} spheres", "particles": spec.n},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                             "sample": f"{steps} full loading steps of the {spec.n}-sphere specimen"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=300)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="brazilian_disc", choices=["brazilian_disc", "uniaxial_cylinder"])
+    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--ref-steps", type=int, default=6)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank, local)
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    D = Dist(ws)
+    spec = build_specimen(dem, args.workload, 1 + rank, local)
+    ctx = dem.Context(device=local, graph_steps=200)
+    sid = ctx.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
+    ctx.setup()
+    cnt = ctx.counts()
+    ctx.run_timed(args.warmup)
+    D.barrier()
+    clk = Clocks(local)
+    ms = ctx.run_timed(args.steps)
+    clocks = clk.stop()
+    D.barrier()
+    ms_max = D.max(ms)
+    n_total = D.sum(float(spec.n))
+    value = n_total * args.steps / (ms_max * 1e-3)
+    # per-kernel timing of the same pipeline (events around each launch)
+    prof = ctx.profile(min(args.steps, 300))
+    res = ctx.result(sid)
+    A = algorithmic_bytes(spec.n, res["bonds_now"], prof["touching"])
+    achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    state_mb = (spec.n * (5 * 16 + 16 + 8) + cnt["bonds"] * (8 + 4 * 16) + cnt["contacts"] * 24) / 1e6
+    # end to end through the public C ABI: host positions in, results and record out
+    ld = spec.loading
+    ld.max_steps = args.steps
+    t0 = time.perf_counter()
+    r_e2e, rec, rb = dem.calculation_test(spec.material, ld, spec.xyz, spec.radii, rec_cap=1 << 16)
+    t_e2e = time.perf_counter() - t0
+    e2e_val = D.sum(spec.n * args.steps / t_e2e) if ws > 1 else spec.n * args.steps / t_e2e
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, el, th = cpu_baseline(spec, args.cpu_steps, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+               "sample": f"{args.cpu_steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
+                         f"integration) of the {spec.n}-sphere specimen"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded packing, FIRE-relaxed)",
+        "config": {"workload": f"{args.workload}: {spec.n} spheres, radii U[0.18,0.30] mm, Brazilian platens"
+                               if args.workload == "brazilian_disc" else f"{args.workload}: {spec.n} spheres",
+                   "particles": spec.n, "bonds": res["bonds_now"], "contacts_listed": cnt["contacts"],
+                   "touching_contacts": prof["touching"], "parallelism": f"{ws} independent specimen(s)",
+                   "l2": f"state {state_mb:.0f} MB per GPU, larger than the 126 MB L2",
+                   "packing": spec.pack},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
+                     "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
+                     "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": (spec.xyz.nbytes + spec.radii.nbytes) /
+                args.steps, "d2h_bytes_per_step": (rec.nbytes + rb.nbytes + 160) / args.steps,
+                "seconds": t_e2e, "note": "dem_calculation_test: upload, set-up, steps, results"},
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    D.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,73 @@
+"""Build of the product library libb200dem.so (sm_100a) in place.
+
+    python dem-rock-calibration_b200/build.py
+
+nvcc compiles the CUDA kernels and host engine for sm_100a only.  -fmad=false
+keeps every a*b+c as two rounded operations (the arithmetic contract of the
+kernels); host code is built with -ffp-contract=off for the same reason.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+SRC = PKG / "csrc"
+OUT = PKG / "libb200dem.so"
+
+SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_capi.cpp"]
+HEADERS = ["dem_common.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
+           "dem_engine.h"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-std=c++17", "-lineinfo",
+    "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+    "-Xptxas", "-O3",
+    "-shared",
+]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and Path(c).exists():
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def stale() -> bool:
+    if not OUT.exists():
+        return True
+    t = OUT.stat().st_mtime
+    deps = [SRC / s for s in SOURCES + HEADERS] + [ROOT / "include" / "b200dem.h"]
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
+    if not force and not stale():
+        return OUT
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", str(ROOT / "include"), "-I", str(SRC),
+           *[str(SRC / s) for s in SOURCES], "-o", str(OUT) + ".tmp", "-lcuda"]
+    if verbose:
+        print(" ".join(cmd))
+    env = dict(os.environ)
+    # nvcc's host compiler: the system g++ (a wrapper in CXX may lack parts of the toolchain)
+    if Path("/usr/bin/g++").exists():
+        cmd[1:1] = ["-ccbin", "/usr/bin/g++"]
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("libb200dem build failed")
+    os.replace(str(OUT) + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    p = build(force="--force" in sys.argv, verbose=True,
+              extra=["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else [])
+    print(p)

@@ -1,0 +1,317 @@
+// Set-up and rebuild kernels of the B200 DEM engine: cell binning as a stable
+// counting sort, an exclusive scan, and a 27-cell pair search used for three
+// pair sets (the reference's interaction sets, the bond list, the contact
+// list).  They replace the reference's CellDistribution
+// (md_cell_distribution.cu:130-172 with CUB radix sort), its cell pointer scan
+// (md_calculate_cell.cu:43-75), d_ConstructInteractionList / the BPM rebuild
+// (md_interaction_list_construct.cu, md_interaction_list_reconstructbpm.cu) and
+// d_ConstructBoundInteractions (md_boundinteractions_construct.cu:35-106).
+#pragma once
+
+#include "dem_common.cuh"
+#include "dem_types.h"
+
+namespace dem {
+
+// Uniform cell grid of one sample: cell (ix,iy,iz) = floor((x - origin) / a),
+// global id = off + ix + iy*nx + iz*nx*ny.  With origin 0 and the reference's
+// edge this is the reference's cell numbering (md_calculate_cell.cu:24-35).
+template <class Real>
+struct Grid {
+  Real ox, oy, oz, inv_a;
+  uint32_t nx, ny, nz, off;
+};
+
+template <class Real>
+__device__ __forceinline__ uint32_t cell_coord(Real x, Real o, Real inv_a, uint32_t n) {
+  const Real f = floor((x - o) * inv_a);
+  if (!(f > Real(0))) return 0u;
+  const uint32_t u = (uint32_t)f;
+  return u < n ? u : n - 1u;
+}
+
+template <class Real>
+__global__ void k_cell_index(const typename RT<Real>::V4* __restrict__ pos, const uint32_t* __restrict__ sid,
+                             uint32_t np, const Grid<Real>* __restrict__ grids, uint32_t* __restrict__ cell_of,
+                             uint32_t* __restrict__ cell_count) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+    const auto x = ld4(pos + p);
+    const Grid<Real> g = grids[sid[p]];
+    const uint32_t ix = cell_coord<Real>(x.x, g.ox, g.inv_a, g.nx);
+    const uint32_t iy = cell_coord<Real>(x.y, g.oy, g.inv_a, g.ny);
+    const uint32_t iz = cell_coord<Real>(x.z, g.oz, g.inv_a, g.nz);
+    const uint32_t c = g.off + ix + iy * g.nx + iz * g.ny * g.nx;
+    cell_of[p] = c;
+    atomicAdd(cell_count + c, 1u);
+  }
+}
+
+// --- exclusive scan of uint32 (three passes, recursive over block sums)
+constexpr int kScanBlock = 1024;
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) >= (unsigned)o) v += t;
+  }
+  return v;
+}
+
+// each block scans kScanBlock elements; block totals go to sums[blockIdx]
+static __global__ void __launch_bounds__(kScanBlock) k_scan_block(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                          uint32_t n, uint32_t* __restrict__ sums) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  const uint32_t v = i < n ? in[i] : 0u;
+  const uint32_t inc = warp_incl_scan(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 31) warp_tot[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t t = warp_incl_scan(warp_tot[lane]);
+    warp_tot[lane] = t;
+  }
+  __syncthreads();
+  const uint32_t base = w > 0 ? warp_tot[w - 1] : 0u;
+  if (i < n) out[i] = base + inc - v;  // exclusive
+  if (threadIdx.x == kScanBlock - 1 && sums) sums[blockIdx.x] = base + inc;
+}
+
+static __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ offs) {
+  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  if (i < n && blockIdx.x > 0) out[i] += offs[blockIdx.x];
+}
+
+// out[n] receives the total
+static __global__ void k_scan_total(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[n] = (n ? out[n - 1] + in[n - 1] : 0u);
+}
+
+static __global__ void k_scatter_cells(const uint32_t* __restrict__ cell_of, uint32_t np, uint32_t* __restrict__ cursor,
+                                uint32_t* __restrict__ cell_list) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+    const uint32_t slot = atomicAdd(cursor + cell_of[p], 1u);
+    cell_list[slot] = p;
+  }
+}
+
+// Restore ascending particle order inside each cell, so the binning equals a
+// stable sort of (cell, particle) pairs (the reference's CUB radix sort).
+static __global__ void k_sort_cells(const uint32_t* __restrict__ cell_start, uint32_t ncell, uint32_t* __restrict__ cell_list) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    const uint32_t b = cell_start[c], e = cell_start[c + 1];
+    for (uint32_t k = b + 1; k < e; ++k) {
+      const uint32_t v = cell_list[k];
+      uint32_t q = k;
+      while (q > b && cell_list[q - 1] > v) {
+        cell_list[q] = cell_list[q - 1];
+        --q;
+      }
+      cell_list[q] = v;
+    }
+  }
+}
+
+// --- pair search over the 27 surrounding cells
+enum PairMode : int {
+  kModeRefSet = 0,  // reference interaction set: j != i, r^2 < add && !(r^2 > del) && !(r^2 < 1e-10)
+  kModeBond = 1,    // bonds: j > i, 1e-10 <= r^2 < (r_i + r_j + gap)^2
+  kModeContact = 2  // contacts: j > i, not bonded, 1e-10 < r^2 < (r_i + r_j + skin)^2
+};
+
+template <class Real>
+struct PairSearch {
+  using V4 = typename RT<Real>::V4;
+  const V4* pos;
+  const uint32_t* sid;
+  uint32_t np;
+  const Grid<Real>* grids;
+  const uint32_t* cell_start;  // ncell + 1
+  const uint32_t* cell_list;
+  int mode;
+  Real add_thr, del_thr;  // kModeRefSet thresholds (squared)
+  const double* gap;      // per sample: bond gap (kModeBond) or skin (kModeContact)
+  const uint32_t* b_row;  // kModeContact: bonds of i (CSR over i, j > i, sorted)
+  const uint2* b_ij;
+  uint32_t* count;        // count pass output (per particle)
+  const uint32_t* offset; // fill pass input (per particle)
+  uint32_t* out_j;        // fill: partner indices (kModeRefSet: np*cap slots)
+  uint32_t cap;           // max pairs per particle kept in registers / slots
+  uint32_t* overflow;     // number of particles whose pairs exceeded cap
+};
+
+template <class Real>
+__device__ __forceinline__ bool pair_pred(const PairSearch<Real>& S, uint32_t i, uint32_t j, const typename RT<Real>::V4& xi,
+                                          const typename RT<Real>::V4& xj, uint32_t s) {
+  const Real dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+  const Real rr = (dx * dx + dy * dy) + dz * dz;
+  if (S.mode == kModeRefSet) {
+    return j != i && rr < S.add_thr && !(rr > S.del_thr) && !(rr < Real(1e-10));
+  }
+  if (j <= i) return false;
+  if (S.mode == kModeBond) {
+    const double r = (double)xi.w + (double)xj.w + (double)S.gap[s];
+    return !(rr < Real(1e-10)) && rr < Real(r * r);
+  }
+  // contact: not bonded
+  const Real cut = xi.w + xj.w + (Real)S.gap[s];
+  if (!(rr > Real(1e-10) && rr < cut * cut)) return false;
+  for (uint32_t k = S.b_row[i], e = S.b_row[i + 1]; k < e; ++k)
+    if (S.b_ij[k].y == j) return false;
+  return true;
+}
+
+// One thread per particle; fill=false counts pairs, fill=true writes them in
+// ascending partner order at offset[i] (kModeRefSet: at i*cap).
+template <class Real, bool kFill>
+__global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
+  constexpr uint32_t kMax = 48;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.np; i += gridDim.x * blockDim.x) {
+    const auto xi = ld4(S.pos + i);
+    const uint32_t s = S.sid[i];
+    const Grid<Real> g = S.grids[s];
+    const int ix = (int)cell_coord<Real>(xi.x, g.ox, g.inv_a, g.nx);
+    const int iy = (int)cell_coord<Real>(xi.y, g.oy, g.inv_a, g.ny);
+    const int iz = (int)cell_coord<Real>(xi.z, g.oz, g.inv_a, g.nz);
+    uint32_t n = 0;
+    uint32_t buf[kMax];
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int cz = iz + dz;
+      if (cz < 0 || cz >= (int)g.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int cy = iy + dy;
+        if (cy < 0 || cy >= (int)g.ny) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int cx = ix + dx;
+          if (cx < 0 || cx >= (int)g.nx) continue;
+          const uint32_t c = g.off + (uint32_t)cx + (uint32_t)cy * g.nx + (uint32_t)cz * g.ny * g.nx;
+          for (uint32_t k = S.cell_start[c], e = S.cell_start[c + 1]; k < e; ++k) {
+            const uint32_t j = S.cell_list[k];
+            const auto xj = ld4(S.pos + j);
+            if (!pair_pred<Real>(S, i, j, xi, xj, s)) continue;
+            if (kFill && n < kMax && n < S.cap) buf[n] = j;
+            ++n;
+          }
+        }
+      }
+    }
+    if (!kFill) {
+      S.count[i] = n;
+      if (n > S.cap && S.overflow) atomicAdd(S.overflow, 1u);
+      continue;
+    }
+    const uint32_t m = n < S.cap ? (n < kMax ? n : kMax) : (S.cap < kMax ? S.cap : kMax);
+    // insertion sort by partner index
+    for (uint32_t a = 1; a < m; ++a) {
+      const uint32_t v = buf[a];
+      uint32_t q = a;
+      while (q > 0 && buf[q - 1] > v) {
+        buf[q] = buf[q - 1];
+        --q;
+      }
+      buf[q] = v;
+    }
+    if (S.mode == kModeRefSet) {
+      uint32_t* o = S.out_j + (size_t)i * S.cap;
+      for (uint32_t a = 0; a < S.cap; ++a) o[a] = a < m ? buf[a] : kEmpty;
+    } else {
+      uint32_t* o = S.out_j + S.offset[i];
+      for (uint32_t a = 0; a < m; ++a) o[a] = buf[a];
+    }
+  }
+}
+
+// Expand per-particle partner lists (CSR by i) into (i, j) pairs.
+static __global__ void k_expand_pairs(const uint32_t* __restrict__ offset, uint32_t np, const uint32_t* __restrict__ js,
+                               uint2* __restrict__ ij) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x)
+    for (uint32_t k = offset[i], e = offset[i + 1]; k < e; ++k) ij[k] = make_uint2(i, js[k]);
+}
+
+// Bond state at creation (d_ConstructBoundInteractions, md_boundinteractions_construct.cu:57-98):
+// 1/L0 = rsqrt(r^2) with r^2 rounded as the reference rounds it, all histories
+// zero (the reference zeroes the previous direction too), radius and
+// strengths from the sample's law.
+template <class Real>
+struct BondLaw {
+  Real br_abs;      // > 0: absolute bond radius (reference b_r)
+  Real br_factor;   // otherwise b_r = factor * min(r_i, r_j)
+  Real sn_mean, sn_sd, st_mean, st_sd;  // normal / shear strength distribution
+  uint64_t seed;
+};
+
+template <class Real>
+__global__ void k_bond_init(const uint2* __restrict__ ij, uint32_t nb, const typename RT<Real>::V4* __restrict__ pos,
+                            const uint32_t* __restrict__ sid, const uint32_t* __restrict__ orig,
+                            const BondLaw<Real>* __restrict__ law, typename RT<Real>::V4* __restrict__ s0,
+                            typename RT<Real>::V4* __restrict__ s1, typename RT<Real>::V4* __restrict__ s2,
+                            typename RT<Real>::V4* __restrict__ par, int32_t* __restrict__ per_sample_count) {
+  using T = RT<Real>;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const uint2 e = ij[b];
+    const auto xi = ld4(pos + e.x), xj = ld4(pos + e.y);
+    const Real rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
+    const Real rm2 = (rx * rx + ry * ry) + rz * rz;
+    const uint32_t s = sid[e.x];
+    const BondLaw<Real> L = law[s];
+    const Real br = L.br_abs > Real(0) ? L.br_abs : L.br_factor * (xi.w < xj.w ? xi.w : xj.w);
+    const uint32_t oa = orig[e.x], ob = orig[e.y];
+    const uint32_t lo = oa < ob ? oa : ob, hi = oa < ob ? ob : oa;
+    Real sn = L.sn_mean, st = L.st_mean;
+    if (L.sn_sd > Real(0)) sn = Real((double)L.sn_mean + (double)L.sn_sd * normal_from(L.seed, lo, hi, 1));
+    if (L.st_sd > Real(0)) st = Real((double)L.st_mean + (double)L.st_sd * normal_from(L.seed, lo, hi, 2));
+    if (sn < Real(0)) sn = Real(0);
+    if (st < Real(0)) st = Real(0);
+    const Real z = Real(0);
+    s0[b] = mk4(z, z, z, z);
+    s1[b] = mk4(z, z, z, z);
+    s2[b] = mk4(z, z, z, z);
+    par[b] = mk4(T::rsqrt_rn(rm2), sn, st, br);
+    atomicAdd(per_sample_count + s, 1);
+  }
+}
+
+// History carry-over after a contact-list rebuild: a pair present before keeps
+// its tangential history (bit 31 of j marks non-zero history).
+template <class Real>
+__global__ void k_contact_carry(uint2* __restrict__ ij, uint32_t nc_new, typename RT<Real>::V4* __restrict__ o_new,
+                                const uint2* __restrict__ ij_old, const typename RT<Real>::V4* __restrict__ o_old,
+                                const uint32_t* __restrict__ row_old) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc_new; c += gridDim.x * blockDim.x) {
+    const uint2 e = ij[c];
+    uint32_t lo = row_old[e.x], hi = row_old[e.x + 1];
+    auto ov = mk4(Real(0), Real(0), Real(0), Real(0));
+    uint32_t flag = 0;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      const uint32_t jm = ij_old[mid].y & 0x7FFFFFFFu;
+      if (jm < e.y)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < row_old[e.x + 1] && (ij_old[lo].y & 0x7FFFFFFFu) == e.y && (ij_old[lo].y >> 31)) {
+      ov = ld4(o_old + lo);
+      flag = 0x80000000u;
+    }
+    o_new[c] = ov;
+    ij[c] = make_uint2(e.x, e.y | flag);
+  }
+}
+
+template <class Real>
+__global__ void k_copy_pos(const typename RT<Real>::V4* __restrict__ pos, typename RT<Real>::V4* __restrict__ ref,
+                           uint32_t np) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) ref[p] = pos[p];
+}
+
+// CSR row pointer of a pair list sorted by i: row[i] = first pair with first index >= i
+static __global__ void k_rows_from_pairs(const uint2* __restrict__ ij, uint32_t n, uint32_t np, uint32_t* __restrict__ row) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= n; k += gridDim.x * blockDim.x) {
+    const uint32_t a = k > 0 ? ij[k - 1].x + 1 : 0u;
+    const uint32_t b = k < n ? ij[k].x : np;
+    for (uint32_t i = a; i <= b && i <= np; ++i) row[i] = k;
+  }
+}
+
+}  // namespace dem

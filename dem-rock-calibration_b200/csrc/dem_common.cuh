@@ -1,0 +1,111 @@
+// Device-side building blocks shared by the B200 DEM kernels.
+//
+// Arithmetic contract: this library is compiled with -fmad=false, so every
+// a*b+c below is two correctly rounded operations, exactly as written; the
+// float path uses the correctly rounded intrinsics __frcp_rn/__fsqrt_rn/
+// __frsqrt_rn (the ones the reference kernels use), the double path uses IEEE
+// division and sqrt.  Evaluation order follows the reference kernels
+// (md_calculateforcesdem3.cu, md_compression_hm.cu), so per-bond results are
+// reproducible bit for bit by a CPU restatement with the same order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dem {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+template <class Real>
+struct RT;
+
+template <>
+struct RT<float> {
+  using V4 = float4;
+  static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+  static __device__ __forceinline__ float sqrt_rn(float x) { return __fsqrt_rn(x); }
+  static __device__ __forceinline__ float rsqrt_rn(float x) { return __frsqrt_rn(x); }
+  static __device__ __forceinline__ float fabs_(float x) { return fabsf(x); }
+  static constexpr float kPi = 3.14159265358979f;    // value of the reference's float pi
+  static constexpr float kTwoThirds = 0.6666666667f;  // value of the reference's float 2/3
+  static constexpr float kDamp = -1.8257f;
+};
+
+template <>
+struct RT<double> {
+  using V4 = double4;
+  static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+  static __device__ __forceinline__ double sqrt_rn(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double rsqrt_rn(double x) { return 1.0 / sqrt(x); }
+  static __device__ __forceinline__ double fabs_(double x) { return fabs(x); }
+  static constexpr double kPi = 3.1415926535897932384626433832795;
+  static constexpr double kTwoThirds = 2.0 / 3.0;
+  static constexpr double kDamp = -1.8257;
+};
+
+template <class Real>
+struct Vec3 {
+  Real x, y, z;
+};
+
+// Euclidean norm of a pair vector.  float: the squares are exact in double, so
+// the double sum and square root rounded once to float give the correctly
+// rounded norm (the reference's norm3df is within a few ulp of it); double:
+// sqrt of the rounded sum of squares.  A CPU evaluation of the same
+// expression gives the same bits.
+__device__ __forceinline__ float norm3(float x, float y, float z) {
+  const double dx = x, dy = y, dz = z;
+  return __double2float_rn(sqrt((dx * dx + dy * dy) + dz * dz));
+}
+__device__ __forceinline__ double norm3(double x, double y, double z) { return sqrt((x * x + y * y) + z * z); }
+
+// 128-bit (float) / 256-bit (double) vector loads and stores through the
+// read-only / default paths.
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ld4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld4_rw(const float4* p) { return *p; }
+__device__ __forceinline__ double4 ld4_rw(const double4* p) { return *p; }
+
+__device__ __forceinline__ float4 mk4(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+__device__ __forceinline__ double4 mk4(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
+
+// Accumulation of per-pair contributions into particle force/moment.
+// float: one 128-bit vector reduction (sm_90+); double: three scalar atomics.
+__device__ __forceinline__ void acc3(float4* p, float x, float y, float z) {
+  atomicAdd(p, make_float4(x, y, z, 0.0f));
+}
+__device__ __forceinline__ void acc3(double4* p, double x, double y, double z) {
+  double* q = reinterpret_cast<double*>(p);
+  atomicAdd(q + 0, x);
+  atomicAdd(q + 1, y);
+  atomicAdd(q + 2, z);
+}
+
+// Counter-based normal deviates for per-bond properties: splitmix64 mixing of
+// (seed, a, b, stream) into two uniforms, then Box-Muller.  Keyed by the
+// original particle indices of the bond, so the draw does not depend on the
+// thread or storage order.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ double u01_from(uint64_t h) {
+  // 53 random bits -> (0,1)
+  return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+__host__ __device__ __forceinline__ double normal_from(uint64_t seed, uint64_t a, uint64_t b, uint64_t stream) {
+  uint64_t k = splitmix64(seed ^ splitmix64(a * 0x100000001B3ull + b) ^ (stream * 0xD6E8FEB86659FD93ull));
+  double u1 = u01_from(splitmix64(k));
+  double u2 = u01_from(splitmix64(k ^ 0x5851F42D4C957F2Dull));
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586476925286766559 * u2);
+}
+
+}  // namespace dem

@@ -1,0 +1,1294 @@
+// B200 DEM engine: device memory, set-up, the per-step pipeline (two kernels
+// per step, replayed from a captured CUDA graph), contact-list rebuilds and
+// state export.  The C ABI (include/b200dem.h) is a thin layer over
+// dem::EngineBase in dem_capi.cpp.
+#include "dem_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "dem_build.cuh"
+#include "dem_params.h"
+#include "dem_step.cuh"
+
+namespace dem {
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) {                   \
+      last_cuda_ = e_;                         \
+      return DEM_ERR_CUDA;                     \
+    }                                          \
+  } while (0)
+#define RC(x)                \
+  do {                       \
+    int r_ = (x);            \
+    if (r_ != DEM_OK) return r_; \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t cnt) {
+    release();
+    n = cnt;
+    if (cnt == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)&p, cnt * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+      return e;
+    }
+    return cudaMemset(p, 0, cnt * sizeof(T));
+  }
+  cudaError_t upload(const T* h, size_t cnt) { return cudaMemcpy(p, h, cnt * sizeof(T), cudaMemcpyHostToDevice); }
+  cudaError_t download(T* h, size_t cnt) const { return cudaMemcpy(h, p, cnt * sizeof(T), cudaMemcpyDeviceToHost); }
+};
+
+static uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// 30-bit Morton interleave of three 10-bit coordinates
+static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1FFFFF;
+    v = (v | v << 32) & 0x1F00000000FFFFull;
+    v = (v | v << 16) & 0x1F0000FF0000FFull;
+    v = (v | v << 8) & 0x100F00F00F00F00Full;
+    v = (v | v << 4) & 0x10C30C30C30C30C3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+struct SampleHost {
+  dem_material mat{};
+  dem_loading load{};
+  uint32_t n = 0;
+  std::vector<float> xyz, rad;     // caller order
+  std::vector<uint32_t> perm;      // storage position k -> caller index
+  std::vector<uint32_t> inv;       // caller index -> storage position
+  uint32_t p_begin = 0;
+  double rmin = 0, rmax = 0, rmean = 0;
+  Potential pot{};
+  double dt = 0;
+  double E_b = 0, G_b = 0, hm_E = 0, hm_G = 0;
+  int32_t bonds_initial = 0;
+};
+
+template <class Real>
+class Engine final : public EngineBase {
+ public:
+  using V4 = typename RT<Real>::V4;
+
+  explicit Engine(const dem_options& o) : opt_(o) {}
+  ~Engine() override {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  int precision() const override { return sizeof(Real) == 8 ? 1 : 0; }
+
+  int init() {
+    CK(cudaSetDevice(opt_.device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    int dev = opt_.device;
+    CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    if (!opt_.pair_block || opt_.pair_block > 256) opt_.pair_block = 256;
+    if (!opt_.pair_grid) opt_.pair_grid = (uint32_t)num_sms_ * 8;
+    if (!opt_.particle_block) opt_.particle_block = 256;
+    if (!opt_.graph_steps) opt_.graph_steps = 100;
+    if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.25;
+    return DEM_OK;
+  }
+
+  int add_sample(const dem_material* mat, const dem_loading* load, const float* xyz, const float* radii, uint32_t n,
+                 int32_t* id) override {
+    if (setup_done_) return DEM_ERR_STATE;
+    if (!mat || !load || !xyz || n == 0) return DEM_ERR_ARG;
+    SampleHost s;
+    s.mat = *mat;
+    s.load = *load;
+    s.n = n;
+    s.xyz.assign(xyz, xyz + 3 * (size_t)n);
+    if (radii)
+      s.rad.assign(radii, radii + n);
+    else
+      s.rad.assign(n, (float)mat->p_r);
+    for (float r : s.rad)
+      if (!(r > 0)) return DEM_ERR_ARG;
+    samples_.push_back(std::move(s));
+    if (id) *id = (int32_t)samples_.size() - 1;
+    return DEM_OK;
+  }
+
+  // ---------------------------------------------------------------- set-up
+  int setup() override {
+    if (setup_done_) return DEM_ERR_STATE;
+    if (samples_.empty()) return DEM_ERR_STATE;
+    CK(cudaSetDevice(opt_.device));
+    const uint32_t S = (uint32_t)samples_.size();
+    np_ = 0;
+    for (auto& s : samples_) {
+      s.p_begin = np_;
+      np_ += s.n;
+      derive(s);
+      morton_order(s);
+    }
+    // per-particle host arrays in storage order
+    std::vector<V4> hpos(np_), hvel(np_), homg(np_);
+    std::vector<Real> hmass(np_);
+    std::vector<uint32_t> hsid(np_), horig(np_);
+    for (uint32_t si = 0; si < S; ++si) {
+      const SampleHost& s = samples_[si];
+      for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t q = s.perm[k];
+        const uint32_t p = s.p_begin + k;
+        const double r = s.rad[q];
+        double m, dtm, dtI;
+        particle_constants(r, s.pot.m_ro, s.dt, m, dtm, dtI);
+        hpos[p] = make4((Real)s.xyz[q], (Real)s.xyz[s.n + q], (Real)s.xyz[2 * s.n + q], (Real)s.rad[q]);
+        hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
+        homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
+        hmass[p] = (Real)m;
+        hsid[p] = si;
+        horig[p] = q;
+      }
+    }
+    CK(pos_.alloc(np_));
+    CK(vel_.alloc(np_));
+    CK(omg_.alloc(np_));
+    CK(frc_.alloc(np_));
+    CK(mom_.alloc(np_));
+    CK(wallO_.alloc(np_));
+    CK(pos_ref_.alloc(np_));
+    CK(mass_.alloc(np_));
+    CK(sid_.alloc(np_));
+    CK(orig_.alloc(np_));
+    CK(pos_.upload(hpos.data(), np_));
+    CK(vel_.upload(hvel.data(), np_));
+    CK(omg_.upload(homg.data(), np_));
+    CK(mass_.upload(hmass.data(), np_));
+    CK(sid_.upload(hsid.data(), np_));
+    CK(orig_.upload(horig.data(), np_));
+    // per-sample constants and controllers
+    RC(upload_params());
+    // contact grids
+    RC(make_grids());
+    // bonds
+    RC(build_bonds());
+    // contact list
+    RC(build_contacts(true));
+    RC(init_controllers());
+    CK(blocks_done_.alloc(1));
+    CK(cudaDeviceSynchronize());
+    setup_done_ = true;
+    return DEM_OK;
+  }
+
+  void derive(SampleHost& s) {
+    const dem_material& m = s.mat;
+    s.rmin = 1e300;
+    s.rmax = 0;
+    double sum = 0;
+    for (float r : s.rad) {
+      s.rmin = std::min(s.rmin, (double)r);
+      s.rmax = std::max(s.rmax, (double)r);
+      sum += r;
+    }
+    s.rmean = sum / s.n;
+    Potential& P = s.pot;
+    P.m_E = m.E;
+    P.m_nu = m.nu;
+    P.m_Ec = m.Ec;
+    P.m_Gc = m.Gc;
+    P.b_r = m.b_r > 0 ? m.b_r : m.bond_radius_factor * s.rmin;
+    // monodisperse specimens use the reference's p_r; polydisperse ones the
+    // smallest radius, which bounds the stable time step
+    P.p_r = (s.rmin == s.rmax) ? (double)s.rmin : s.rmin;
+    if (m.p_r > 0 && s.rmin == s.rmax && (float)m.p_r == (float)s.rmin) P.p_r = m.p_r;
+    P.b_d = 2.0 * P.p_r + m.gap;
+    P.m_ro = m.rho;
+    P.p_e = m.p_e;
+    P.p_mu = m.mu;
+    P.p_mur = m.mur;
+    P.a_farcut = m.farcut * (m.p_r > 0 ? m.p_r : s.rmean);
+    P.calculate();
+    s.dt = P.dt;
+    if (m.dt_rayleigh_factor > 0) s.dt = m.dt_rayleigh_factor * rayleigh_time(s.rmin, m.rho, m.E, m.nu);
+    if (m.dt > 0) s.dt = m.dt;
+    s.E_b = m.E_bond > 0 ? m.E_bond : m.E;
+    s.G_b = m.kn_ks > 0 ? s.E_b / m.kn_ks : 0.5 * s.E_b / (1.0 + m.nu);
+    s.hm_E = P.hm_E;
+    s.hm_G = P.hm_G;
+  }
+
+  void morton_order(SampleHost& s) {
+    const double q = std::max(s.rmin, 1e-6);
+    double lo[3] = {1e300, 1e300, 1e300};
+    for (uint32_t i = 0; i < s.n; ++i)
+      for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], (double)s.xyz[d * s.n + i]);
+    std::vector<std::pair<uint64_t, uint32_t>> key(s.n);
+    for (uint32_t i = 0; i < s.n; ++i) {
+      uint32_t c[3];
+      for (int d = 0; d < 3; ++d) {
+        double v = ((double)s.xyz[d * s.n + i] - lo[d]) / q;
+        c[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
+      }
+      key[i] = {morton3(c[0], c[1], c[2]), i};
+    }
+    std::stable_sort(key.begin(), key.end());
+    s.perm.resize(s.n);
+    s.inv.resize(s.n);
+    for (uint32_t k = 0; k < s.n; ++k) {
+      s.perm[k] = key[k].second;
+      s.inv[key[k].second] = k;
+    }
+  }
+
+  static V4 make4(Real a, Real b, Real c, Real d) {
+    V4 v;
+    v.x = a;
+    v.y = b;
+    v.z = c;
+    v.w = d;
+    return v;
+  }
+
+  int upload_params() {
+    const uint32_t S = (uint32_t)samples_.size();
+    std::vector<SampleParams<Real>> hp(S);
+    std::vector<BondLaw<Real>> hl(S);
+    std::vector<double> hgap(S), hskin(S);
+    for (uint32_t si = 0; si < S; ++si) {
+      const SampleHost& s = samples_[si];
+      const dem_material& m = s.mat;
+      const dem_loading& L = s.load;
+      SampleParams<Real>& p = hp[si];
+      p.dt = (Real)s.dt;
+      p.E = (Real)s.E_b;
+      p.G = (Real)s.G_b;
+      p.hmE = (Real)s.hm_E;
+      p.hmG = (Real)s.hm_G;
+      const bool brazil = L.test == DEM_TEST_BRAZIL;
+      p.wallE = brazil ? (Real)s.hm_E : (Real)(2.0 * s.hm_E);
+      p.wallG = brazil ? (Real)s.hm_G : (Real)(2.0 * s.hm_G);
+      p.pA = (Real)s.pot.p_A;
+      p.mu = (Real)m.mu;
+      p.mur = (Real)m.mur;
+      p.aa_far = (Real)s.pot.aa_farcut;
+      const double skin = opt_.skin_factor * s.rmin;
+      p.skin_half2 = (Real)(0.25 * skin * skin);
+      for (int d = 0; d < 3; ++d) {
+        p.space_c[d] = (Real)(float)L.space_center[d];
+        p.space_h[d] = (Real)(float)L.space_half[d];
+        p.hide[d] = (Real)(float)L.hidden_point[d];
+        p.wall_c[d] = (float)L.center_real[d];
+      }
+      p.axis = L.test == DEM_TEST_UNIAXIAL ? 2 : (brazil ? 1 : -1);
+      p.zcut = (float)L.zcut;
+      // lateral radius of the platen zone (compression_data::Calculate{U,B}Parameters)
+      const float sx2 = (float)(0.5 * L.size_real[0]), sz2 = (float)(0.5 * L.size_real[2]);
+      float Rw = brazil ? ((sx2 > sz2) ? sx2 : (float)(1.05 * sz2)) : (float)(1.5 * sx2);
+      p.wall_RR = Rw * Rw;
+      p.nobreak = m.nobreak;
+      p.p_begin = s.p_begin;
+      p.p_end = s.p_begin + s.n;
+      BondLaw<Real>& l = hl[si];
+      l.br_abs = m.b_r > 0 ? (Real)s.pot.b_r : Real(0);
+      l.br_factor = (Real)m.bond_radius_factor;
+      l.sn_mean = (Real)m.Ec;
+      l.sn_sd = (Real)m.Ec_sd;
+      l.st_mean = (Real)m.Gc;
+      l.st_sd = (Real)m.Gc_sd;
+      l.seed = m.seed;
+      hgap[si] = m.gap;
+      hskin[si] = skin;
+    }
+    CK(sp_.alloc(S));
+    CK(sp_.upload(hp.data(), S));
+    CK(law_.alloc(S));
+    CK(law_.upload(hl.data(), S));
+    CK(gap_.alloc(S));
+    CK(gap_.upload(hgap.data(), S));
+    CK(skin_.alloc(S));
+    CK(skin_.upload(hskin.data(), S));
+    hparams_ = hp;
+    return DEM_OK;
+  }
+
+  int make_grids() {
+    const uint32_t S = (uint32_t)samples_.size();
+    std::vector<Grid<Real>> hg(S);
+    uint32_t off = 0;
+    for (uint32_t si = 0; si < S; ++si) {
+      const SampleHost& s = samples_[si];
+      const double skin = opt_.skin_factor * s.rmin;
+      double a = 2.0 * s.rmax + skin;
+      const double bond_reach = 2.0 * s.rmax + std::max(0.0, s.pot.b_d - 2.0 * s.pot.p_r);
+      a = std::max(a, bond_reach) * 1.0001;
+      Grid<Real>& g = hg[si];
+      double lo[3], hi[3];
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = s.load.space_center[d] - s.load.space_half[d];
+        hi[d] = s.load.space_center[d] + s.load.space_half[d];
+        if (s.load.space_half[d] <= 0) {  // no escape box: use the particle extent
+          lo[d] = 1e300;
+          hi[d] = -1e300;
+          for (uint32_t i = 0; i < s.n; ++i) {
+            lo[d] = std::min(lo[d], (double)s.xyz[d * s.n + i]);
+            hi[d] = std::max(hi[d], (double)s.xyz[d * s.n + i]);
+          }
+        }
+        lo[d] -= a;
+        hi[d] += a;
+      }
+      g.ox = (Real)lo[0];
+      g.oy = (Real)lo[1];
+      g.oz = (Real)lo[2];
+      g.inv_a = (Real)(1.0 / a);
+      g.nx = (uint32_t)std::ceil((hi[0] - lo[0]) / a) + 1;
+      g.ny = (uint32_t)std::ceil((hi[1] - lo[1]) / a) + 1;
+      g.nz = (uint32_t)std::ceil((hi[2] - lo[2]) / a) + 1;
+      g.off = off;
+      off += g.nx * g.ny * g.nz;
+    }
+    ncell_ = off;
+    CK(grids_.alloc(S));
+    CK(grids_.upload(hg.data(), S));
+    CK(cell_of_.alloc(np_));
+    CK(cell_count_.alloc(ncell_ + 1));
+    CK(cell_start_.alloc(ncell_ + 1));
+    CK(cell_cursor_.alloc(ncell_ + 1));
+    CK(cell_list_.alloc(np_));
+    CK(cnt_.alloc(np_ + 1));
+    CK(offs_.alloc(np_ + 1));
+    CK(ovf_.alloc(1));
+    return DEM_OK;
+  }
+
+  // exclusive scan of n values into out[0..n], out[n] = total
+  int scan(const uint32_t* in, uint32_t* out, uint32_t n) {
+    const uint32_t nb = ceil_div(n, kScanBlock);
+    std::vector<std::pair<uint32_t*, uint32_t>> levels;
+    if (scan_tmp_.n < 2 * (size_t)nb + 2048) CK(scan_tmp_.alloc(2 * (size_t)nb + 2048));
+    uint32_t* sums = scan_tmp_.p;
+    uint32_t* sums_scan = scan_tmp_.p + nb + 1024;
+    k_scan_block<<<std::max(nb, 1u), kScanBlock, 0, stream_>>>(in, out, n, sums);
+    if (nb > 1) {
+      if (nb > kScanBlock) {
+        // second level recursively (rare: more than ~1M elements)
+        DBuf<uint32_t> s2;
+        CK(s2.alloc(nb + 1));
+        RC(scan(sums, s2.p, nb));
+        CK(cudaMemcpyAsync(sums_scan, s2.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+      } else {
+        k_scan_block<<<1, kScanBlock, 0, stream_>>>(sums, sums_scan, nb, nullptr);
+      }
+      k_scan_add<<<nb, kScanBlock, 0, stream_>>>(out, n, sums_scan);
+    }
+    k_scan_total<<<1, 1, 0, stream_>>>(in, out, n);
+    CK(cudaGetLastError());
+    return DEM_OK;
+  }
+
+  int bin_cells() {
+    const uint32_t g = grid1(np_);
+    CK(cudaMemsetAsync(cell_count_.p, 0, (ncell_ + 1) * sizeof(uint32_t), stream_));
+    k_cell_index<Real><<<g, 256, 0, stream_>>>(pos_.p, sid_.p, np_, grids_.p, cell_of_.p, cell_count_.p);
+    RC(scan(cell_count_.p, cell_start_.p, ncell_));
+    CK(cudaMemcpyAsync(cell_cursor_.p, cell_start_.p, (ncell_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                       stream_));
+    k_scatter_cells<<<g, 256, 0, stream_>>>(cell_of_.p, np_, cell_cursor_.p, cell_list_.p);
+    k_sort_cells<<<grid1(ncell_), 256, 0, stream_>>>(cell_start_.p, ncell_, cell_list_.p);
+    CK(cudaGetLastError());
+    return DEM_OK;
+  }
+
+  uint32_t grid1(uint64_t n) const {
+    return std::max(1u, std::min(ceil_div(n, 256), (uint32_t)num_sms_ * 16));
+  }
+
+  PairSearch<Real> search_args(int mode) {
+    PairSearch<Real> S{};
+    S.pos = pos_.p;
+    S.sid = sid_.p;
+    S.np = np_;
+    S.grids = grids_.p;
+    S.cell_start = cell_start_.p;
+    S.cell_list = cell_list_.p;
+    S.mode = mode;
+    S.count = cnt_.p;
+    S.offset = offs_.p;
+    S.cap = 48;
+    S.overflow = ovf_.p;
+    return S;
+  }
+
+  int build_bonds() {
+    RC(bin_cells());
+    PairSearch<Real> S = search_args(kModeBond);
+    S.gap = gap_.p;
+    CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
+    k_pair_search<Real, false><<<grid1(np_), 128, 0, stream_>>>(S);
+    RC(scan(cnt_.p, offs_.p, np_));
+    uint32_t nb = 0, ovf = 0;
+    CK(cudaMemcpyAsync(&nb, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(&ovf, ovf_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    if (ovf) return DEM_ERR_CAPACITY;
+    nb_ = nb;
+    DBuf<uint32_t> js;
+    CK(js.alloc(std::max(nb, 1u)));
+    S.out_j = js.p;
+    k_pair_search<Real, true><<<grid1(np_), 128, 0, stream_>>>(S);
+    CK(b_ij_.alloc(std::max(nb, 1u)));
+    CK(b_s0_.alloc(std::max(nb, 1u)));
+    CK(b_s1_.alloc(std::max(nb, 1u)));
+    CK(b_s2_.alloc(std::max(nb, 1u)));
+    CK(b_par_.alloc(std::max(nb, 1u)));
+    CK(b_row_.alloc(np_ + 1));
+    const uint32_t S_ = (uint32_t)samples_.size();
+    DBuf<int32_t> counts;
+    CK(counts.alloc(S_));
+    k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, js.p, b_ij_.p);
+    CK(cudaMemcpyAsync(b_row_.p, offs_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+    if (nb)
+      k_bond_init<Real><<<grid1(nb), 256, 0, stream_>>>(b_ij_.p, nb, pos_.p, sid_.p, orig_.p, law_.p, b_s0_.p,
+                                                       b_s1_.p, b_s2_.p, b_par_.p, counts.p);
+    CK(cudaGetLastError());
+    std::vector<int32_t> hc(S_);
+    CK(cudaMemcpyAsync(hc.data(), counts.p, S_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    for (uint32_t si = 0; si < S_; ++si) samples_[si].bonds_initial = hc[si];
+    return DEM_OK;
+  }
+
+  // Rebuilds the contact list from the current positions; pairs that existed
+  // keep their tangential history.
+  int build_contacts(bool first) {
+    RC(bin_cells());
+    PairSearch<Real> S = search_args(kModeContact);
+    S.gap = skin_.p;
+    S.b_row = b_row_.p;
+    S.b_ij = b_ij_.p;
+    CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
+    k_pair_search<Real, false><<<grid1(np_), 128, 0, stream_>>>(S);
+    RC(scan(cnt_.p, offs_.p, np_));
+    uint32_t nc = 0, ovf = 0;
+    CK(cudaMemcpyAsync(&nc, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(&ovf, ovf_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    if (ovf) return DEM_ERR_CAPACITY;
+    const size_t need = std::max<size_t>(nc, 1);
+    if (first || need > c_ij_.n) {
+      const size_t cap = std::max<size_t>(need + need / 2, (size_t)np_ * 2 + 1024);
+      // keep the old list for the carry-over
+      DBuf<uint2> old_ij;
+      DBuf<V4> old_o;
+      DBuf<uint32_t> old_row;
+      const uint32_t old_nc = nc_host_;
+      if (!first) {
+        CK(old_ij.alloc(std::max<size_t>(old_nc, 1)));
+        CK(old_o.alloc(std::max<size_t>(old_nc, 1)));
+        CK(old_row.alloc(np_ + 1));
+        CK(cudaMemcpyAsync(old_ij.p, c_ij_.p, old_nc * sizeof(uint2), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(old_o.p, c_o_.p, old_nc * sizeof(V4), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(old_row.p, c_row_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+      }
+      CK(cudaStreamSynchronize(stream_));
+      CK(c_ij_.alloc(cap));
+      CK(c_o_.alloc(cap));
+      CK(c_ij_new_.alloc(cap));
+      CK(c_o_new_.alloc(cap));
+      CK(c_js_.alloc(cap));
+      CK(c_row_.alloc(np_ + 1));
+      CK(nc_dev_.alloc(1));
+      invalidate_graph();
+      if (!first) {
+        CK(cudaMemcpyAsync(c_ij_.p, old_ij.p, old_nc * sizeof(uint2), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(c_o_.p, old_o.p, old_nc * sizeof(V4), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(c_row_.p, old_row.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+      }
+    }
+    S.out_j = c_js_.p;
+    k_pair_search<Real, true><<<grid1(np_), 128, 0, stream_>>>(S);
+    k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_js_.p, c_ij_new_.p);
+    if (nc) {
+      if (first)
+        CK(cudaMemsetAsync(c_row_.p, 0, (np_ + 1) * sizeof(uint32_t), stream_));
+      k_contact_carry<Real><<<grid1(nc), 256, 0, stream_>>>(c_ij_new_.p, nc, c_o_new_.p, c_ij_.p, c_o_.p, c_row_.p);
+      CK(cudaMemcpyAsync(c_ij_.p, c_ij_new_.p, nc * sizeof(uint2), cudaMemcpyDeviceToDevice, stream_));
+      CK(cudaMemcpyAsync(c_o_.p, c_o_new_.p, nc * sizeof(V4), cudaMemcpyDeviceToDevice, stream_));
+    }
+    CK(cudaMemcpyAsync(c_row_.p, offs_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+    CK(cudaMemcpyAsync(nc_dev_.p, &nc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+    k_copy_pos<Real><<<grid1(np_), 256, 0, stream_>>>(pos_.p, pos_ref_.p, np_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    nc_host_ = nc;
+    ++rebuilds_;
+    return DEM_OK;
+  }
+
+  int init_controllers() {
+    const uint32_t S = (uint32_t)samples_.size();
+    std::vector<SampleCtl> hc(S);
+    rec_.resize(S);
+    rec_bonds_.resize(S);
+    for (uint32_t si = 0; si < S; ++si) {
+      const SampleHost& s = samples_[si];
+      const dem_loading& L = s.load;
+      SampleCtl& C = hc[si];
+      std::memset(&C, 0, sizeof(C));
+      const bool brazil = L.test == DEM_TEST_BRAZIL;
+      const int ax = brazil ? 1 : 2;
+      C.brazil = brazil ? 1 : 0;
+      for (int d = 0; d < 3; ++d) C.size_d[d] = L.size_real[d];
+      const double pr = L.p_r_platen > 0 ? L.p_r_platen : (s.mat.p_r > 0 ? s.mat.p_r : s.rmean);
+      C.p_r = pr;
+      C.Size0 = C.size_d[ax];
+      C.Bottom = L.center_real[ax] - 0.5 * C.size_d[ax];
+      C.Top = L.center_real[ax] + 0.5 * C.size_d[ax];
+      const float sx2 = (float)(0.5 * C.size_d[0]);
+      const float sizez = (float)C.size_d[2];
+      float area;
+      if (!brazil) {
+        area = (float)(kPiD * (sx2 + pr) * (sx2 + pr));
+        C.ZeroStress = 0.33 * L.min_stress;
+      } else {
+        area = (float)(0.5 * 2 * kPiD * (sx2) * (sizez));
+        C.ZeroStress = 0.5 * L.min_stress;
+      }
+      C.inv_Area = (float)(1.0 / area);
+      C.sz0 = (double)(float)C.size_d[ax];
+      C.MinStress = L.min_stress;
+      C.MaxStrain = L.test == DEM_TEST_NONE ? 1e300 : L.max_strain;
+      C.ConditionFracture = L.cond_fracture;
+      C.VLoad = L.velocity;
+      C.V = 0;
+      C.dt = s.dt;
+      C.max_steps = L.max_steps ? L.max_steps : ~0ull;
+      C.bonds = s.bonds_initial;
+      C.dNsave = L.dNsave;
+      uint64_t nsave = 16;
+      if (L.test != DEM_TEST_NONE && L.dNsave && std::fabs(L.velocity) > 0) {
+        double v = 1.5 * L.max_strain * C.size_d[ax] / (std::fabs(L.velocity) * s.dt * L.dNsave);
+        nsave = (uint64_t)std::min(v, 4.0e7);
+      }
+      if (L.max_steps && L.dNsave) nsave = std::min<uint64_t>(nsave, L.max_steps / L.dNsave + 2);
+      C.Nsave = (uint32_t)std::max<uint64_t>(nsave, 4);
+      RC(alloc_rec(si, C.Nsave));
+      C.rec = rec_[si]->p;
+      C.rec_bonds = rec_bonds_[si]->p;
+    }
+    CK(ctl_.alloc(S));
+    CK(ctl_.upload(hc.data(), S));
+    return DEM_OK;
+  }
+
+  int alloc_rec(uint32_t si, uint32_t nsave) {
+    rec_[si].reset(new DBuf<double>());
+    rec_bonds_[si].reset(new DBuf<uint32_t>());
+    CK(rec_[si]->alloc(3 * ((size_t)nsave + 2)));
+    CK(rec_bonds_[si]->alloc((size_t)nsave + 2));
+    return DEM_OK;
+  }
+
+  // ---------------------------------------------------------------- stepping
+  StepArgs<Real> args() {
+    StepArgs<Real> A{};
+    A.pos = pos_.p;
+    A.vel = vel_.p;
+    A.omg = omg_.p;
+    A.frc = frc_.p;
+    A.mom = mom_.p;
+    A.wallO = wallO_.p;
+    A.pos_ref = pos_ref_.p;
+    A.mass = mass_.p;
+    A.sid = sid_.p;
+    A.np = np_;
+    A.b_ij = b_ij_.p;
+    A.b_s0 = b_s0_.p;
+    A.b_s1 = b_s1_.p;
+    A.b_s2 = b_s2_.p;
+    A.b_par = b_par_.p;
+    A.nb = nb_;
+    A.c_ij = c_ij_.p;
+    A.c_o = c_o_.p;
+    A.nc = nc_dev_.p;
+    A.sp = sp_.p;
+    A.ctl = ctl_.p;
+    A.nsamples = (uint32_t)samples_.size();
+    A.blocks_done = blocks_done_.p;
+    A.keep_forces = 0;
+    A.touching = nullptr;
+    return A;
+  }
+
+  void launch_step(const StepArgs<Real>& A, int stages) {
+    if (stages & 1) k_pairs<Real><<<opt_.pair_grid, opt_.pair_block, 0, stream_>>>(A);
+    if (stages & 2) {
+      const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
+      k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
+    }
+  }
+
+  void invalidate_graph() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+  }
+
+  int capture_graph() {
+    invalidate_graph();
+    cudaGraph_t g = nullptr;
+    StepArgs<Real> A = args();
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t k = 0; k < opt_.graph_steps; ++k) launch_step(A, 3);
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e != cudaSuccess) {
+      last_cuda_ = e;
+      return DEM_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&graph_exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      last_cuda_ = e;
+      graph_exec_ = nullptr;
+      return DEM_ERR_CUDA;
+    }
+    return DEM_OK;
+  }
+
+  struct Flags {
+    uint32_t done, rebuild, stale;
+  };
+
+  int read_flags(Flags& f) {
+    const uint32_t S = (uint32_t)samples_.size();
+    hctl_.resize(S);
+    CK(cudaMemcpyAsync(hctl_.data(), ctl_.p, S * sizeof(SampleCtl), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    f = {1, 0, 0};
+    for (auto& c : hctl_) {
+      f.done &= c.done ? 1u : 0u;
+      f.rebuild |= c.rebuild;
+      f.stale |= c.stale;
+    }
+    return DEM_OK;
+  }
+
+  int clear_rebuild_flags() {
+    // clear rebuild on the device copy (host copy is fresh from read_flags)
+    for (uint32_t si = 0; si < hctl_.size(); ++si) {
+      uint32_t z = 0;
+      CK(cudaMemcpyAsync(&ctl_.p[si].rebuild, &z, sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+    }
+    CK(cudaStreamSynchronize(stream_));
+    return DEM_OK;
+  }
+
+  int prepare() {
+    if (!setup_done_) return DEM_ERR_STATE;
+    if (forces_dirty_) {
+      CK(cudaMemsetAsync(frc_.p, 0, np_ * sizeof(V4), stream_));
+      CK(cudaMemsetAsync(mom_.p, 0, np_ * sizeof(V4), stream_));
+      forces_dirty_ = false;
+    }
+    if (contacts_dirty_) {
+      RC(build_contacts(false));
+      contacts_dirty_ = false;
+    }
+    return DEM_OK;
+  }
+
+  int run(uint64_t max_steps, uint64_t* done_steps, bool stop_when_done) {
+    RC(prepare());
+    uint64_t steps = 0;
+    Flags f{};
+    RC(read_flags(f));
+    if (f.rebuild) {
+      RC(build_contacts(false));
+      RC(clear_rebuild_flags());
+    }
+    while (steps < max_steps) {
+      if (stop_when_done && f.done) break;
+      const uint64_t left = max_steps - steps;
+      if (left >= opt_.graph_steps) {
+        if (!graph_exec_) RC(capture_graph());
+        CK(cudaGraphLaunch(graph_exec_, stream_));
+        steps += opt_.graph_steps;
+      } else {
+        StepArgs<Real> A = args();
+        for (uint64_t k = 0; k < left; ++k) launch_step(A, 3);
+        steps += left;
+      }
+      CK(cudaGetLastError());
+      RC(read_flags(f));
+      if (f.stale) {
+        stale_ = true;
+        break;
+      }
+      if (f.rebuild) {
+        RC(build_contacts(false));
+        RC(clear_rebuild_flags());
+      }
+    }
+    total_steps_ += steps;
+    if (done_steps) *done_steps = steps;
+    return stale_ ? DEM_ERR_STALE : DEM_OK;
+  }
+
+  int run_until_done(uint64_t max_steps, uint64_t* done) override { return run(max_steps, done, true); }
+  int step(uint32_t n) override { return run(n, nullptr, false); }
+
+  int step_stages(int stages) override {
+    RC(prepare());
+    StepArgs<Real> A = args();
+    A.keep_forces = (stages & 4) ? 1 : 0;
+    launch_step(A, stages & 3);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    if (stages & 4) forces_dirty_ = true;
+    if ((stages & 1) && !(stages & 2)) forces_dirty_ = true;
+    return DEM_OK;
+  }
+
+  int sync() override {
+    CK(cudaStreamSynchronize(stream_));
+    return DEM_OK;
+  }
+
+  // ---------------------------------------------------------------- queries
+  int counts(uint32_t* p, uint32_t* b, uint32_t* c, uint32_t* s) override {
+    if (p) *p = np_;
+    if (b) *b = nb_;
+    if (c) *c = nc_host_;
+    if (s) *s = (uint32_t)samples_.size();
+    return DEM_OK;
+  }
+
+  int result(int32_t si, dem_result* out) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !out) return DEM_ERR_ARG;
+    if (!setup_done_) return DEM_ERR_STATE;
+    SampleCtl C;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&C, ctl_.p + si, sizeof(C), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->FractureStress = C.FractureStress;
+    out->FractureStrain = C.FractureStrain;
+    out->Strain = C.Strain;
+    out->Stress = C.Stress;
+    out->dt = C.dt;
+    out->platen_top = C.Top;
+    out->platen_bottom = C.Bottom;
+    out->platen_velocity = C.V;
+    out->steps = C.step;
+    out->stepsave = C.stepsave;
+    out->bonds_initial = (uint32_t)samples_[si].bonds_initial;
+    out->bonds_now = (uint32_t)std::max(C.bonds, 0);
+    out->fracture = (int)C.Fracture;
+    out->done = (int)C.done;
+    out->stale = C.stale ? 1 : 0;
+    // host post-processing of the record (CalculateLinearityDeviation, CalculateDestruction)
+    std::vector<double> rec;
+    std::vector<uint32_t> rb;
+    RC(record(si, rec, rb));
+    const uint32_t ns = C.stepsave;
+    if (ns > 0 && rb.size() >= ns && rb[0] > 0) out->Destruction = rb[ns - 1] / (double)rb[0];
+    if (!C.brazil && ns > 0 && C.FractureStrain != 0 && C.FractureStress != 0)
+      out->LinearityDeviation = linearity_deviation(rec, ns, C.FractureStress, C.FractureStrain);
+    return DEM_OK;
+  }
+
+  // md_results.cu:147-166 (the record holds two extra zero entries so the
+  // look-ahead stays inside it)
+  static double linearity_deviation(const std::vector<double>& h, uint32_t stepsave, double FS, double Fe) {
+    double l_eps = 0, l_deps = 0, l_A = FS / Fe, l_dS = 0, LD = 0;
+    uint32_t i = 0;
+    do {
+      LD += l_deps * l_dS * l_dS;
+      ++i;
+      if (3 * (size_t)(i + 1) + 2 >= h.size()) break;
+      l_eps = -h[3 * i];
+      l_deps = -0.5 * (h[3 * (i + 1)] - h[3 * (i - 1)]);
+      l_dS = (l_A * l_eps - 0.5 * (h[3 * i + 2] - h[3 * i + 1]));
+    } while (l_eps < Fe - 2 * l_deps && i < stepsave);
+    LD /= (Fe * FS * FS);
+    return LD + 1.0;
+  }
+
+  int record(int32_t si, std::vector<double>& rec, std::vector<uint32_t>& rb) {
+    const size_t n = rec_[si]->n / 3;
+    rec.resize(3 * n);
+    rb.resize(rec_bonds_[si]->n);
+    CK(rec_[si]->download(rec.data(), 3 * n));
+    CK(rec_bonds_[si]->download(rb.data(), rb.size()));
+    return DEM_OK;
+  }
+
+  int get_record(int32_t si, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n) override {
+    if (si < 0 || (size_t)si >= samples_.size()) return DEM_ERR_ARG;
+    SampleCtl C;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&C, ctl_.p + si, sizeof(C), cudaMemcpyDeviceToHost));
+    std::vector<double> r;
+    std::vector<uint32_t> b;
+    RC(record(si, r, b));
+    const uint32_t m = std::min<uint32_t>(C.stepsave, cap);
+    if (rec) std::memcpy(rec, r.data(), 3 * (size_t)m * sizeof(double));
+    if (bonds) std::memcpy(bonds, b.data(), (size_t)m * sizeof(uint32_t));
+    if (n) *n = C.stepsave;
+    return DEM_OK;
+  }
+
+  template <class Out>
+  int get_particles_t(int32_t si, Out* R, Out* V, Out* W, Out* F, Out* M, Out* O) {
+    if (si < 0 || (size_t)si >= samples_.size()) return DEM_ERR_ARG;
+    const SampleHost& s = samples_[si];
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<V4> h(s.n);
+    auto fetch = [&](DBuf<V4>& b, Out* dst) -> int {
+      if (!dst) return DEM_OK;
+      CK(cudaMemcpy(h.data(), b.p + s.p_begin, s.n * sizeof(V4), cudaMemcpyDeviceToHost));
+      for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t q = s.perm[k];
+        dst[q] = (Out)h[k].x;
+        dst[s.n + q] = (Out)h[k].y;
+        dst[2 * s.n + q] = (Out)h[k].z;
+      }
+      return DEM_OK;
+    };
+    RC(fetch(pos_, R));
+    RC(fetch(vel_, V));
+    RC(fetch(omg_, W));
+    RC(fetch(frc_, F));
+    RC(fetch(mom_, M));
+    RC(fetch(wallO_, O));
+    return DEM_OK;
+  }
+  int get_particles(int32_t si, float* R, float* V, float* W, float* F, float* M, float* O) override {
+    return get_particles_t<float>(si, R, V, W, F, M, O);
+  }
+  int get_particles_d(int32_t si, double* R, double* V, double* W, double* F, double* M, double* O) override {
+    return get_particles_t<double>(si, R, V, W, F, M, O);
+  }
+
+  int set_particles(int32_t si, const float* R, const float* V, const float* W, const float* O) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
+    const SampleHost& s = samples_[si];
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<V4> h(s.n);
+    auto put = [&](DBuf<V4>& b, const float* src) -> int {
+      if (!src) return DEM_OK;
+      CK(cudaMemcpy(h.data(), b.p + s.p_begin, s.n * sizeof(V4), cudaMemcpyDeviceToHost));
+      for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t q = s.perm[k];
+        h[k].x = (Real)src[q];
+        h[k].y = (Real)src[s.n + q];
+        h[k].z = (Real)src[2 * s.n + q];
+      }
+      CK(cudaMemcpy(b.p + s.p_begin, h.data(), s.n * sizeof(V4), cudaMemcpyHostToDevice));
+      return DEM_OK;
+    };
+    RC(put(pos_, R));
+    RC(put(vel_, V));
+    RC(put(omg_, W));
+    RC(put(wallO_, O));
+    if (R) contacts_dirty_ = true;
+    return DEM_OK;
+  }
+
+  // pair record: 16 values (1/L0, prev-dir xyz, Ot xyz, Mn xyz, Mt xyz, sigma_c, tau_c, b_r)
+  int get_pairs(int32_t si, uint32_t cap, uint32_t* oi, uint32_t* oj, uint32_t* kind, float* st, uint32_t* n) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
+    RC(prepare());
+    const SampleHost& s = samples_[si];
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<uint2> bij(nb_), cij(nc_host_);
+    std::vector<V4> s0(nb_), s1(nb_), s2(nb_), par(nb_), co(nc_host_);
+    if (nb_) {
+      CK(b_ij_.download(bij.data(), nb_));
+      CK(b_s0_.download(s0.data(), nb_));
+      CK(b_s1_.download(s1.data(), nb_));
+      CK(b_s2_.download(s2.data(), nb_));
+      CK(b_par_.download(par.data(), nb_));
+    }
+    if (nc_host_) {
+      CK(c_ij_.download(cij.data(), nc_host_));
+      CK(c_o_.download(co.data(), nc_host_));
+    }
+    uint32_t m = 0;
+    const uint32_t lo = s.p_begin, hi = s.p_begin + s.n;
+    auto emit = [&](uint32_t a, uint32_t b, uint32_t k, const float v[16]) {
+      if (m < cap) {
+        uint32_t ia = s.perm[a - lo], ib = s.perm[b - lo];
+        float w[16];
+        std::memcpy(w, v, sizeof(w));
+        if (ia > ib) {  // express in the direction i -> j with i < j: mirror the vectors
+          std::swap(ia, ib);
+          for (int d = 1; d < 13; ++d) w[d] = -w[d];
+        }
+        if (oi) oi[m] = ia;
+        if (oj) oj[m] = ib;
+        if (kind) kind[m] = k;
+        if (st) std::memcpy(st + 16 * (size_t)m, w, sizeof(w));
+      }
+      ++m;
+    };
+    for (uint32_t b = 0; b < nb_; ++b) {
+      if (bij[b].x < lo || bij[b].x >= hi) continue;
+      const bool intact = par[b].x > 0;
+      const float v[16] = {(float)(intact ? par[b].x : -par[b].x),
+                           (float)s0[b].x, (float)s0[b].y, (float)s0[b].z,
+                           (float)s0[b].w, (float)s1[b].x, (float)s1[b].y,
+                           (float)s1[b].z, (float)s1[b].w, (float)s2[b].x,
+                           (float)s2[b].y, (float)s2[b].z, (float)s2[b].w,
+                           (float)par[b].y, (float)par[b].z, (float)par[b].w};
+      emit(bij[b].x, bij[b].y, intact ? 1u : 2u, v);
+    }
+    for (uint32_t c = 0; c < nc_host_; ++c) {
+      if (cij[c].x < lo || cij[c].x >= hi) continue;
+      const float v[16] = {0, 0, 0, 0, (float)co[c].x, (float)co[c].y, (float)co[c].z, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+      emit(cij[c].x, cij[c].y & 0x7FFFFFFFu, 3u, v);
+    }
+    if (n) *n = m;
+    return DEM_OK;
+  }
+
+  int set_pairs(int32_t si, uint32_t cnt, const uint32_t* ii, const uint32_t* jj, const uint32_t* kind,
+                const float* st) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
+    RC(prepare());
+    const SampleHost& s = samples_[si];
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<uint2> bij(nb_), cij(nc_host_);
+    std::vector<V4> s0(nb_), s1(nb_), s2(nb_), par(nb_), co(nc_host_);
+    if (nb_) {
+      CK(b_ij_.download(bij.data(), nb_));
+      CK(b_s0_.download(s0.data(), nb_));
+      CK(b_s1_.download(s1.data(), nb_));
+      CK(b_s2_.download(s2.data(), nb_));
+      CK(b_par_.download(par.data(), nb_));
+    }
+    if (nc_host_) {
+      CK(c_ij_.download(cij.data(), nc_host_));
+      CK(c_o_.download(co.data(), nc_host_));
+    }
+    std::vector<int32_t> delta(samples_.size(), 0);
+    for (uint32_t k = 0; k < cnt; ++k) {
+      uint32_t a = s.inv[ii[k]] + s.p_begin, b = s.inv[jj[k]] + s.p_begin;
+      float v[13];
+      std::memcpy(v, st + 13 * (size_t)k, sizeof(v));  // set_pairs takes the 13-value state
+      if (a > b) {
+        std::swap(a, b);
+        for (int d = 1; d < 13; ++d) v[d] = -v[d];
+      }
+      // bonds: search the row of a
+      bool found = false;
+      auto it = std::lower_bound(bij.begin(), bij.end(), make_uint2(a, b),
+                                 [](const uint2& x, const uint2& y) { return x.x < y.x || (x.x == y.x && x.y < y.y); });
+      if (it != bij.end() && it->x == a && it->y == b) {
+        const size_t q = it - bij.begin();
+        const bool was = par[q].x > 0;
+        const bool now = kind[k] == 1;
+        const Real il = (Real)std::fabs(v[0]) > 0 ? (Real)std::fabs(v[0]) : std::fabs(par[q].x);
+        par[q].x = now ? il : -il;
+        if (was != now) delta[si] += now ? 1 : -1;
+        s0[q] = make4(v[1], v[2], v[3], v[4]);
+        s1[q] = make4(v[5], v[6], v[7], v[8]);
+        s2[q] = make4(v[9], v[10], v[11], v[12]);
+        found = true;
+      }
+      if (!found) {
+        for (uint32_t c = 0; c < nc_host_; ++c) {
+          if (cij[c].x == a && (cij[c].y & 0x7FFFFFFFu) == b) {
+            co[c] = make4(v[4], v[5], v[6], Real(0));
+            const bool nz = v[4] != 0 || v[5] != 0 || v[6] != 0;
+            cij[c].y = b | (nz ? 0x80000000u : 0u);
+            found = true;
+            break;
+          }
+        }
+      }
+      if (!found) return DEM_ERR_ARG;
+    }
+    if (nb_) {
+      CK(b_s0_.upload(s0.data(), nb_));
+      CK(b_s1_.upload(s1.data(), nb_));
+      CK(b_s2_.upload(s2.data(), nb_));
+      CK(b_par_.upload(par.data(), nb_));
+    }
+    if (nc_host_) {
+      CK(c_ij_.upload(cij.data(), nc_host_));
+      CK(c_o_.upload(co.data(), nc_host_));
+    }
+    if (delta[si]) {
+      int32_t cur;
+      CK(cudaMemcpy(&cur, &ctl_.p[si].bonds, sizeof(int32_t), cudaMemcpyDeviceToHost));
+      cur += delta[si];
+      CK(cudaMemcpy(&ctl_.p[si].bonds, &cur, sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+    return DEM_OK;
+  }
+
+  int set_platens(int32_t si, double top, double bottom, double v) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
+    CK(cudaStreamSynchronize(stream_));
+    SampleCtl C;
+    CK(cudaMemcpy(&C, ctl_.p + si, sizeof(C), cudaMemcpyDeviceToHost));
+    C.Top = top;
+    C.Bottom = bottom;
+    C.V = v;
+    CK(cudaMemcpy(ctl_.p + si, &C, sizeof(C), cudaMemcpyHostToDevice));
+    return DEM_OK;
+  }
+
+  int rebuild_contacts() override {
+    if (!setup_done_) return DEM_ERR_STATE;
+    return build_contacts(false);
+  }
+
+  cudaError_t last_cuda() const override { return last_cuda_; }
+  uint64_t rebuilds() const override { return rebuilds_; }
+  uint32_t num_sms() const override { return (uint32_t)num_sms_; }
+
+  // device pointers of the step kernel for external timing
+  void launch_raw(int stages) override {
+    StepArgs<Real> A = args();
+    launch_step(A, stages);
+  }
+  void* stream() override { return (void*)stream_; }
+
+  int run_timed(uint64_t nsteps, double* ms) override {
+    RC(prepare());
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, stream_));
+    uint64_t done = 0;
+    int rc = run(nsteps, &done, false);
+    CK(cudaEventRecord(b, stream_));
+    CK(cudaEventSynchronize(b));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms) *ms = t;
+    return rc;
+  }
+
+  int profile(uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching) override {
+    RC(prepare());
+    if (nsteps == 0) return DEM_ERR_ARG;
+    std::vector<cudaEvent_t> ev(4 * (size_t)nsteps);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    DBuf<unsigned long long> cnt;
+    CK(cnt.alloc(1));
+    StepArgs<Real> A = args();
+    A.touching = cnt.p;
+    const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
+    for (uint32_t k = 0; k < nsteps; ++k) {
+      CK(cudaEventRecord(ev[4 * k], stream_));
+      k_pairs<Real><<<opt_.pair_grid, opt_.pair_block, 0, stream_>>>(A);
+      CK(cudaEventRecord(ev[4 * k + 1], stream_));
+      CK(cudaEventRecord(ev[4 * k + 2], stream_));
+      k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
+      CK(cudaEventRecord(ev[4 * k + 3], stream_));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    double sp = 0, sq = 0;
+    for (uint32_t k = 0; k < nsteps; ++k) {
+      float t1 = 0, t2 = 0;
+      CK(cudaEventElapsedTime(&t1, ev[4 * k], ev[4 * k + 1]));
+      CK(cudaEventElapsedTime(&t2, ev[4 * k + 2], ev[4 * k + 3]));
+      sp += t1;
+      sq += t2;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    unsigned long long tc = 0;
+    CK(cnt.download(&tc, 1));
+    if (pair_ms) *pair_ms = sp / nsteps;
+    if (particle_ms) *particle_ms = sq / nsteps;
+    if (touching) *touching = (double)tc / nsteps;
+    Flags f{};
+    RC(read_flags(f));
+    if (f.rebuild) {
+      RC(build_contacts(false));
+      RC(clear_rebuild_flags());
+    }
+    total_steps_ += nsteps;
+    return f.stale ? DEM_ERR_STALE : DEM_OK;
+  }
+
+ private:
+  dem_options opt_;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int num_sms_ = 148;
+  bool setup_done_ = false, forces_dirty_ = false, contacts_dirty_ = false, stale_ = false;
+  cudaError_t last_cuda_ = cudaSuccess;
+  uint64_t total_steps_ = 0, rebuilds_ = 0;
+
+  std::vector<SampleHost> samples_;
+  std::vector<SampleParams<Real>> hparams_;
+  std::vector<SampleCtl> hctl_;
+  uint32_t np_ = 0, nb_ = 0, nc_host_ = 0, ncell_ = 0;
+
+  DBuf<V4> pos_, vel_, omg_, frc_, mom_, wallO_, pos_ref_;
+  DBuf<Real> mass_;
+  DBuf<uint32_t> sid_, orig_;
+  DBuf<uint2> b_ij_;
+  DBuf<V4> b_s0_, b_s1_, b_s2_, b_par_;
+  DBuf<uint32_t> b_row_;
+  DBuf<uint2> c_ij_, c_ij_new_;
+  DBuf<V4> c_o_, c_o_new_;
+  DBuf<uint32_t> c_js_, c_row_, nc_dev_;
+  DBuf<SampleParams<Real>> sp_;
+  DBuf<BondLaw<Real>> law_;
+  DBuf<double> gap_, skin_;
+  DBuf<SampleCtl> ctl_;
+  DBuf<Grid<Real>> grids_;
+  DBuf<uint32_t> cell_of_, cell_count_, cell_start_, cell_cursor_, cell_list_, cnt_, offs_, ovf_, scan_tmp_;
+  DBuf<unsigned int> blocks_done_;
+  std::vector<std::unique_ptr<DBuf<double>>> rec_;
+  std::vector<std::unique_ptr<DBuf<uint32_t>>> rec_bonds_;
+};
+
+EngineBase* make_engine(const dem_options& o, int* err) {
+  EngineBase* e = nullptr;
+  int rc = DEM_OK;
+  if (o.precision == 1) {
+    auto* x = new Engine<double>(o);
+    rc = x->init();
+    e = x;
+  } else {
+    auto* x = new Engine<float>(o);
+    rc = x->init();
+    e = x;
+  }
+  if (rc != DEM_OK) {
+    delete e;
+    e = nullptr;
+  }
+  if (err) *err = rc;
+  return e;
+}
+
+// ------------------------------------------------------------------ reference-layout parity exports
+namespace {
+int ref_grid_bin(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, DBuf<float4>& pos,
+                 DBuf<uint32_t>& sid, DBuf<Grid<float>>& grid, DBuf<uint32_t>& cell_of, DBuf<uint32_t>& cstart,
+                 DBuf<uint32_t>& clist, uint32_t& ncell) {
+  std::vector<float4> h(n);
+  for (uint32_t i = 0; i < n; ++i) h[i] = make_float4(xyz[i], xyz[n + i], xyz[2 * n + i], 0.f);
+  ncell = nx * ny * nz;
+  Grid<float> g{0.f, 0.f, 0.f, (float)(1.0 / (double)a), nx, ny, nz, 0};
+  if (pos.alloc(n) || sid.alloc(n) || grid.alloc(1) || cell_of.alloc(n) || cstart.alloc(ncell + 1) || clist.alloc(n))
+    return DEM_ERR_CUDA;
+  if (pos.upload(h.data(), n) || grid.upload(&g, 1)) return DEM_ERR_CUDA;
+  DBuf<uint32_t> count, cursor, tmp1, tmp2;
+  if (count.alloc(ncell + 1) || cursor.alloc(ncell + 1)) return DEM_ERR_CUDA;
+  const uint32_t gb = std::max(1u, ceil_div(n, 256));
+  k_cell_index<float><<<gb, 256>>>(pos.p, sid.p, n, grid.p, cell_of.p, count.p);
+  // scan (host-side simple three-level, sizes here are small)
+  const uint32_t nb = ceil_div(ncell, kScanBlock);
+  if (tmp1.alloc(nb + 1) || tmp2.alloc(nb + 1)) return DEM_ERR_CUDA;
+  k_scan_block<<<nb, kScanBlock>>>(count.p, cstart.p, ncell, tmp1.p);
+  if (nb > 1) {
+    if (nb > kScanBlock) return DEM_ERR_CAPACITY;
+    k_scan_block<<<1, kScanBlock>>>(tmp1.p, tmp2.p, nb, nullptr);
+    k_scan_add<<<nb, kScanBlock>>>(cstart.p, ncell, tmp2.p);
+  }
+  k_scan_total<<<1, 1>>>(count.p, cstart.p, ncell);
+  if (cudaMemcpy(cursor.p, cstart.p, (ncell + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice)) return DEM_ERR_CUDA;
+  k_scatter_cells<<<gb, 256>>>(cell_of.p, n, cursor.p, clist.p);
+  k_sort_cells<<<std::max(1u, ceil_div(ncell, 256)), 256>>>(cstart.p, ncell, clist.p);
+  if (cudaDeviceSynchronize()) return DEM_ERR_CUDA;
+  return DEM_OK;
+}
+}  // namespace
+
+int ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
+              uint32_t* CIs, uint32_t* pnC) {
+  DBuf<float4> pos;
+  DBuf<uint32_t> sid, cell_of, cstart, clist;
+  DBuf<Grid<float>> grid;
+  uint32_t ncell = 0;
+  int rc = ref_grid_bin(xyz, n, a, nx, ny, nz, pos, sid, grid, cell_of, cstart, clist, ncell);
+  if (rc) return rc;
+  std::vector<uint32_t> co(n), cs(ncell + 1), cl(n);
+  if (cell_of.download(co.data(), n) || cstart.download(cs.data(), ncell + 1) || clist.download(cl.data(), n))
+    return DEM_ERR_CUDA;
+  if (CI) std::memcpy(CI, co.data(), n * sizeof(uint32_t));
+  if (CIs)
+    for (uint32_t k = 0; k < n; ++k) {
+      CIs[k] = co[cl[k]];
+      CIs[n + k] = cl[k];
+    }
+  if (pnC) {
+    std::memset(pnC, 0, 2 * (size_t)ncell * sizeof(uint32_t));
+    for (uint32_t c = 0; c < ncell; ++c)
+      if (cs[c + 1] > cs[c]) {
+        pnC[c] = cs[c];
+        pnC[ncell + c] = cs[c + 1] - cs[c];
+      }
+  }
+  return DEM_OK;
+}
+
+int ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, float add_thr,
+                      float del_thr, uint32_t cap, uint32_t* sets, uint32_t* overflow) {
+  DBuf<float4> pos;
+  DBuf<uint32_t> sid, cell_of, cstart, clist;
+  DBuf<Grid<float>> grid;
+  uint32_t ncell = 0;
+  int rc = ref_grid_bin(xyz, n, a, nx, ny, nz, pos, sid, grid, cell_of, cstart, clist, ncell);
+  if (rc) return rc;
+  DBuf<uint32_t> out, cnt, ovf;
+  if (out.alloc((size_t)n * cap) || cnt.alloc(n) || ovf.alloc(1)) return DEM_ERR_CUDA;
+  PairSearch<float> S{};
+  S.pos = pos.p;
+  S.sid = sid.p;
+  S.np = n;
+  S.grids = grid.p;
+  S.cell_start = cstart.p;
+  S.cell_list = clist.p;
+  S.mode = kModeRefSet;
+  S.add_thr = add_thr;
+  S.del_thr = del_thr;
+  S.count = cnt.p;
+  S.out_j = out.p;
+  S.cap = cap;
+  S.overflow = ovf.p;
+  const uint32_t gb = std::max(1u, ceil_div(n, 128));
+  k_pair_search<float, false><<<gb, 128>>>(S);
+  k_pair_search<float, true><<<gb, 128>>>(S);
+  if (cudaDeviceSynchronize()) return DEM_ERR_CUDA;
+  if (out.download(sets, (size_t)n * cap)) return DEM_ERR_CUDA;
+  uint32_t o = 0;
+  if (ovf.download(&o, 1)) return DEM_ERR_CUDA;
+  if (overflow) *overflow = o;
+  return DEM_OK;
+}
+
+}  // namespace dem

@@ -1,0 +1,624 @@
+// Per-step kernels of the B200 DEM engine:
+//
+//   k_pairs     one thread per bond or contact pair: BPM bond force/moment with
+//               break test, Hertz-Mindlin contact for broken bonds and unbonded
+//               pairs; contributions scattered to both particles with 128-bit
+//               vector reductions.  Replaces the reference's d_CalculateForcesDEM_22
+//               + d_CalculateForcesDEM_21 (md_calculateforcesdem3.cu:341-486), which
+//               compute every pair twice, once per direction.
+//   k_particles one thread per particle: platen contacts (d_UniaxialCompression_hm /
+//               d_BrazilCompression_hm, md_compression_hm.cu:156-449), integration
+//               (d_CalculateIncrementsDEM, md_calculateincrementsdem.cu:128-158), escape
+//               parking (d_ParallelepipedCutRestriction, md_parallelepipedrestriction.cu:254),
+//               accumulator reset, neighbour-list validity, platen force sums; the
+//               last block to finish runs the loading controller of every sample
+//               (SumForces{U,B}Loading + Compress{U,B}_S3, md_results.cu:56-145,
+//               md_data_types.h:347-494) on the device, so a step needs no host sync.
+#pragma once
+
+#include "dem_common.cuh"
+#include "dem_types.h"
+
+namespace dem {
+
+template <class Real>
+struct StepArgs {
+  using V4 = typename RT<Real>::V4;
+  V4* pos;
+  V4* vel;
+  V4* omg;
+  V4* frc;
+  V4* mom;
+  V4* wallO;
+  V4* pos_ref;
+  const Real* mass;
+  const uint32_t* sid;
+  uint32_t np;
+  // bonds
+  const uint2* b_ij;
+  V4* b_s0;
+  V4* b_s1;
+  V4* b_s2;
+  V4* b_par;
+  uint32_t nb;
+  // contacts
+  uint2* c_ij;
+  V4* c_o;
+  const uint32_t* nc;  // device count
+  // samples
+  const SampleParams<Real>* sp;
+  SampleCtl* ctl;
+  uint32_t nsamples;
+  unsigned int* blocks_done;
+  int keep_forces;  // 1: leave the step's total force/moment in frc/mom (parity checks)
+  unsigned long long* touching;  // non-null: count touching contacts (algorithmic-byte accounting)
+};
+
+// Hertz-Mindlin contact of pair (i, j) seen from i (n points from i to j), in
+// the polydisperse form that reduces bit for bit to dd_Calculate_fijn_ppHM_2 /
+// dd_Calculate_fijtmijt_ppHM_2 / dd_Calculate_mijroll_ppHM_2
+// (md_calculateforcesdem3.cu:202-339) when r_i = r_j is a power of two and the
+// masses are equal.  Updates the tangential history o and returns the force on
+// i and the moments on i and j (the reference drops the whole contact moment of
+// a particle whose spin satisfies |w|^2 <= 1e-18, see md_calculateforcesdem3.cu:333-338).
+template <class Real>
+__device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, Real ry, Real rz, Real rijm, Real ri,
+                                        Real rj, Real mi, Real mj, const typename RT<Real>::V4& vi,
+                                        const typename RT<Real>::V4& vj, const typename RT<Real>::V4& wi,
+                                        const typename RT<Real>::V4& wj, Real& ox, Real& oy, Real& oz, Real f[3],
+                                        Real mI[3], Real mJ[3], bool& dropI, bool& dropJ) {
+  using T = RT<Real>;
+  const Real half = Real(0.5);
+  const Real sumr = ri + rj;
+  const Real rinv = T::rcp(rijm);
+  const Real n0 = rx * rinv, n1 = ry * rinv, n2 = rz * rinv;
+  const Real reff = ri * rj / sumr;
+  Real cef1 = T::sqrt_rn(reff * (sumr - rijm));
+  const Real Kn = Real(2) * sp.hmE * cef1;
+  const Real Kt = Real(8) * sp.hmG * cef1;
+  const Real rbar = half * sumr, rdif = half * (rj - ri);
+  const Real sw0 = wj.x + wi.x, sw1 = wj.y + wi.y, sw2 = wj.z + wi.z;
+  const Real dw0 = wj.x - wi.x, dw1 = wj.y - wi.y, dw2 = wj.z - wi.z;
+  const Real v0 = vj.x - vi.x + rbar * (n1 * sw2 - n2 * sw1) + rdif * (n1 * dw2 - n2 * dw1);
+  const Real v1 = vj.y - vi.y + rbar * (n2 * sw0 - n0 * sw2) + rdif * (n2 * dw0 - n0 * dw2);
+  const Real v2 = vj.z - vi.z + rbar * (n0 * sw1 - n1 * sw0) + rdif * (n0 * dw1 - n1 * dw0);
+  const Real vn = n0 * v0 + n1 * v1 + n2 * v2;
+  const Real fijnm = (rijm - sumr) * Kn * T::kTwoThirds;
+  const Real m2 = mi * ((mj + mj) / (mi + mj));
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * half * m2);
+  const Real fn0 = n0 * (fijnm + cef1), fn1 = n1 * (fijnm + cef1), fn2 = n2 * (fijnm + cef1);
+  const Real vt0 = v0 - n0 * vn, vt1 = v1 - n1 * vn, vt2 = v2 - n2 * vn;
+  // rotate the old tangential overlap into the new tangent plane, keep its length
+  cef1 = n0 * ox + n1 * oy + n2 * oz;
+  Real t0 = ox - n0 * cef1, t1 = oy - n1 * cef1, t2 = oz - n2 * cef1;
+  cef1 = (t0 * t0 + t1 * t1) + t2 * t2;
+  if (cef1 > Real(1e-18)) {
+    cef1 = T::rcp(cef1);
+    cef1 *= (ox * ox + oy * oy) + oz * oz;
+    cef1 = T::sqrt_rn(cef1);
+    t0 *= cef1;
+    t1 *= cef1;
+    t2 *= cef1;
+  }
+  const Real dt = sp.dt;
+  t0 += vt0 * dt;
+  t1 += vt1 * dt;
+  t2 += vt2 * dt;
+  Real ft0 = t0 * Kt, ft1 = t1 * Kt, ft2 = t2 * Kt;
+  const Real ftmm = (ft0 * ft0 + ft1 * ft1) + ft2 * ft2;
+  if (ftmm > sp.mu * sp.mu * fijnm * fijnm) {
+    cef1 = sp.mu * T::fabs_(fijnm) * T::rsqrt_rn(ftmm);
+    ft0 *= cef1;
+    ft1 *= cef1;
+    ft2 *= cef1;
+    cef1 = T::rcp(Kt);
+    t0 = ft0 * cef1;
+    t1 = ft1 * cef1;
+    t2 = ft2 * cef1;
+  } else {
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * half * m2);
+    ft0 += vt0 * cef1;
+    ft1 += vt1 * cef1;
+    ft2 += vt2 * cef1;
+  }
+  ox = t0;
+  oy = t1;
+  oz = t2;
+  f[0] = fn0 + ft0;
+  f[1] = fn1 + ft1;
+  f[2] = fn2 + ft2;
+  const Real c0 = n1 * ft2 - n2 * ft1, c1 = n2 * ft0 - n0 * ft2, c2 = n0 * ft1 - n1 * ft0;
+  mI[0] = c0 * ri;
+  mI[1] = c1 * ri;
+  mI[2] = c2 * ri;
+  mJ[0] = c0 * rj;
+  mJ[1] = c1 * rj;
+  mJ[2] = c2 * rj;
+  const Real afn = T::fabs_(fijnm);
+  const Real wim = (wi.x * wi.x + wi.y * wi.y) + wi.z * wi.z;
+  const Real wjm = (wj.x * wj.x + wj.y * wj.y) + wj.z * wj.z;
+  dropI = !(wim > Real(1e-18));
+  dropJ = !(wjm > Real(1e-18));
+  if (!dropI) {
+    const Real c = -sp.mur * afn * T::rsqrt_rn(wim);
+    mI[0] += wi.x * c;
+    mI[1] += wi.y * c;
+    mI[2] += wi.z * c;
+  }
+  if (!dropJ) {
+    const Real c = -sp.mur * afn * T::rsqrt_rn(wjm);
+    mJ[0] += wj.x * c;
+    mJ[1] += wj.y * c;
+    mJ[2] += wj.z * c;
+  }
+}
+
+template <class Real>
+__device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i, uint32_t j, const Real f[3],
+                                             const Real mI[3], const Real mJ[3], bool dropI, bool dropJ) {
+  acc3(A.frc + i, f[0], f[1], f[2]);
+  acc3(A.frc + j, -f[0], -f[1], -f[2]);
+  if (!dropI) acc3(A.mom + i, mI[0], mI[1], mI[2]);
+  if (!dropJ) acc3(A.mom + j, mJ[0], mJ[1], mJ[2]);
+}
+
+// One bond (i < j).  The arithmetic is that of d_CalculateForcesDEM_22 for the
+// slot i->j (md_calculateforcesdem3.cu:41-200, 427-486); the slot j->i of the
+// reference is its exact mirror (all vectors negated, the unsymmetric moment
+// equal), so j receives -F, -(Mn + Mt) terms and the same unsymmetric moment.
+template <class Real>
+__device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
+  using T = RT<Real>;
+  using V4 = typename T::V4;
+  const uint2 ij = A.b_ij[b];
+  const uint32_t i = ij.x, j = ij.y;
+  const uint32_t s = A.sid[i];
+  if (A.ctl[s].done) return;
+  const SampleParams<Real>& sp = A.sp[s];
+  V4 par = ld4_rw(A.b_par + b);
+  const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
+  const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
+  const Real rr = (rx * rx + ry * ry) + rz * rz;
+  bool intact = par.x > Real(0);
+  if (intact && (rr > sp.aa_far || rr < Real(1e-10))) {
+    // d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:169-181): the slot is
+    // emptied with all histories; the pair later interacts only by contact.
+    par.x = -par.x;
+    A.b_par[b] = par;
+    const Real z = Real(0);
+    A.b_s0[b] = mk4(z, z, z, z);
+    A.b_s1[b] = mk4(z, z, z, z);
+    A.b_s2[b] = mk4(z, z, z, z);
+    atomicSub(&A.ctl[s].bonds, 1);
+    return;
+  }
+  const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
+  const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
+  V4 s0 = ld4_rw(A.b_s0 + b), s1 = ld4_rw(A.b_s1 + b), s2 = ld4_rw(A.b_s2 + b);
+  const Real rijm = norm3(rx, ry, rz);
+  Real ox = s0.w, oy = s1.x, oz = s1.y;
+  if (intact) {
+    const Real one = Real(1), half = Real(0.5), dt = sp.dt, E = sp.E, G = sp.G, pi_ = T::kPi;
+    const Real il = par.x, br = par.w;
+    const Real rinv = T::rcp(rijm);
+    const Real n0 = rx * rinv, n1 = ry * rinv, n2 = rz * rinv;
+    // normal force (dd_Calculate_fijn_bpm_2)
+    Real cef = E * (rijm - T::rcp(il)) * il;
+    Real Sc = cef;
+    cef *= br * br * pi_;
+    const Real fn0 = n0 * cef, fn1 = n1 * cef, fn2 = n2 * cef;
+    // incremental rotation (dd_Calculate_M123_bpm_2)
+    const Real tp0 = s0.y * n2 - s0.z * n1, tp1 = s0.z * n0 - s0.x * n2, tp2 = s0.x * n1 - s0.y * n0;
+    cef = ((wj.x + wi.x) * n0 + (wj.y + wi.y) * n1 + (wj.z + wi.z) * n2) * dt * half;
+    const Real ph0 = n0 * cef, ph1 = n1 * cef, ph2 = n2 * cef;
+    s0.x = n0;
+    s0.y = n1;
+    s0.z = n2;
+    const Real M10 = one + tp2 * ph2 + tp1 * ph1;
+    const Real M11 = ph2 - tp2 - tp1 * ph0;
+    const Real M12 = -ph1 - tp2 * ph0 + tp1;
+    const Real M20 = tp2 - ph2 - tp0 * ph1;
+    const Real M21 = tp2 * ph2 + one + tp0 * ph0;
+    const Real M22 = -tp2 * ph1 + ph0 - tp0;
+    const Real M30 = -tp1 - tp0 * ph2 + ph1;
+    const Real M31 = -tp1 * ph2 + tp0 - ph0;
+    const Real M32 = tp1 * ph1 + tp0 * ph0 + one;
+    // twisting moment (dd_Calculate_mijn_bpm_2)
+    const Real dwx = wj.x - wi.x, dwy = wj.y - wi.y, dwz = wj.z - wi.z;
+    const Real wn = n0 * dwx + n1 * dwy + n2 * dwz;
+    Real cef1 = wn * (dt * half * G * il);
+    const Real Nx = s1.z, Ny = s1.w, Nz = s2.x;
+    const Real mn0 = M10 * Nx + M11 * Ny + M12 * Nz + n0 * cef1;
+    const Real mn1 = M20 * Nx + M21 * Ny + M22 * Nz + n1 * cef1;
+    const Real mn2 = M30 * Nx + M31 * Ny + M32 * Nz + n2 * cef1;
+    cef1 = pi_ * br * br * br * br;
+    const Real tn0 = mn0 * cef1, tn1 = mn1 * cef1, tn2 = mn2 * cef1;
+    // bending moment (dd_Calculate_mijt_bpm_2)
+    Real cef2 = dt * Real(0.25) * E * il;
+    const Real Tx = s2.y, Ty = s2.z, Tz = s2.w;
+    const Real mt0 = M10 * Tx + M11 * Ty + M12 * Tz + (dwx - n0 * wn) * cef2;
+    const Real mt1 = M20 * Tx + M21 * Ty + M22 * Tz + (dwy - n1 * wn) * cef2;
+    const Real mt2 = M30 * Tx + M31 * Ty + M32 * Tz + (dwz - n2 * wn) * cef2;
+    cef2 *= pi_ * br * br * br * br;
+    const Real tt0 = mt0 * cef2, tt1 = mt1 * cef2, tt2 = mt2 * cef2;
+    // shear force and unsymmetric moment (dd_Calculate_fijt_mijunsym_bpm_2)
+    const Real ws0 = half * (wj.x + wi.x), ws1 = half * (wj.y + wi.y), ws2 = half * (wj.z + wi.z);
+    const Real v0 = vj.x - vi.x - ws1 * rz + ws2 * ry;
+    const Real v1 = vj.y - vi.y - ws2 * rx + ws0 * rz;
+    const Real v2 = vj.z - vi.z - ws0 * ry + ws1 * rx;
+    cef = n0 * v0 + n1 * v1 + n2 * v2;
+    const Real ot0 = (M10 * ox + M11 * oy + M12 * oz) + (v0 - n0 * cef) * dt;
+    const Real ot1 = (M20 * ox + M21 * oy + M22 * oz) + (v1 - n1 * cef) * dt;
+    const Real ot2 = (M30 * ox + M31 * oy + M32 * oz) + (v2 - n2 * cef) * dt;
+    cef = G * il;
+    Real Mc = cef;
+    cef *= br * br * pi_;
+    const Real ft0 = ot0 * cef, ft1 = ot1 * cef, ft2 = ot2 * cef;
+    const Real mu0 = half * (ry * ot2 - rz * ot1) * cef;
+    const Real mu1 = half * (rz * ot0 - rx * ot2) * cef;
+    const Real mu2 = half * (rx * ot1 - ry * ot0) * cef;
+    // contributions: i gets (F, Mn+Mt+Mu), j gets (-F, -(Mn+Mt)+Mu)
+    acc3(A.frc + i, fn0 + ft0, fn1 + ft1, fn2 + ft2);
+    acc3(A.frc + j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2));
+    acc3(A.mom + i, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1, (tn2 + tt2) + mu2);
+    acc3(A.mom + j, mu0 - (tn0 + tt0), mu1 - (tn1 + tt1), mu2 - (tn2 + tt2));
+    // break test (dd_CheckBreakConditionDEM_2)
+    bool broke = false;
+    if (!sp.nobreak) {
+      Mc *= norm3(ot0, ot1, ot2);
+      Sc += norm3(mt0, mt1, mt2) * Real(4) * br;
+      Mc += norm3(mn0, mn1, mn2) * Real(2) * br;
+      broke = (Sc > par.y) || (Mc > par.z);
+    }
+    if (!broke) {
+      s0.w = ot0;
+      s1 = mk4(ot1, ot2, mn0, mn1);
+      s2 = mk4(mn2, mt0, mt1, mt2);
+      A.b_s0[b] = s0;
+      A.b_s1[b] = s1;
+      A.b_s2[b] = s2;
+      return;
+    }
+    // broken: histories cleared; the pair is a contact from now on and, as in the
+    // reference (DEM_21 runs after DEM_22 in the same step), already this step.
+    par.x = -par.x;
+    A.b_par[b] = par;
+    atomicSub(&A.ctl[s].bonds, 1);
+    ox = oy = oz = Real(0);
+    const Real z = Real(0);
+    s1.z = z;
+    s1.w = z;
+    s2 = mk4(z, z, z, z);
+  }
+  // Hertz-Mindlin contact of a broken bond
+  const Real ri = pi.w, rj = pj.w;
+  if (rr > Real(1e-10) && rijm < ri + rj) {
+    Real f[3], mI[3], mJ[3];
+    bool dI, dJ;
+    hm_pair<Real>(sp, rx, ry, rz, rijm, ri, rj, A.mass[i], A.mass[j], vi, vj, wi, wj, ox, oy, oz, f, mI, mJ, dI, dJ);
+    scatter_pair<Real>(A, i, j, f, mI, mJ, dI, dJ);
+    if (A.touching) atomicAdd(A.touching, 1ull);
+  } else {
+    ox = oy = oz = Real(0);
+  }
+  s0.w = ox;
+  s1.x = oy;
+  s1.y = oz;
+  A.b_s0[b] = s0;
+  A.b_s1[b] = s1;
+  if (intact) A.b_s2[b] = s2;
+}
+
+// One unbonded contact-list pair (i < j).  Bit 31 of j flags a non-zero
+// tangential history, so separated pairs cost only the position gathers.
+template <class Real>
+__device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) {
+  using T = RT<Real>;
+  using V4 = typename T::V4;
+  uint2 ij = A.c_ij[c];
+  const uint32_t i = ij.x, j = ij.y & 0x7FFFFFFFu;
+  const bool has_hist = (ij.y >> 31) != 0;
+  const uint32_t s = A.sid[i];
+  if (A.ctl[s].done) return;
+  const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
+  const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
+  const Real rr = (rx * rx + ry * ry) + rz * rz;
+  const Real ri = pi.w, rj = pj.w;
+  const Real rijm = norm3(rx, ry, rz);
+  if (!(rr > Real(1e-10) && rijm < ri + rj)) {
+    if (has_hist) {
+      const Real z = Real(0);
+      A.c_o[c] = mk4(z, z, z, z);
+      A.c_ij[c] = make_uint2(i, j);
+    }
+    return;
+  }
+  const SampleParams<Real>& sp = A.sp[s];
+  V4 o = has_hist ? ld4_rw(A.c_o + c) : mk4(Real(0), Real(0), Real(0), Real(0));
+  const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
+  const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
+  Real f[3], mI[3], mJ[3];
+  bool dI, dJ;
+  Real ox = o.x, oy = o.y, oz = o.z;
+  hm_pair<Real>(sp, rx, ry, rz, rijm, ri, rj, A.mass[i], A.mass[j], vi, vj, wi, wj, ox, oy, oz, f, mI, mJ, dI, dJ);
+  scatter_pair<Real>(A, i, j, f, mI, mJ, dI, dJ);
+  if (A.touching) atomicAdd(A.touching, 1ull);
+  A.c_o[c] = mk4(ox, oy, oz, Real(0));
+  if (!has_hist) A.c_ij[c] = make_uint2(i, j | 0x80000000u);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(256) k_pairs(StepArgs<Real> A) {
+  const uint32_t nb = A.nb;
+  const uint32_t total = nb + *A.nc;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    if (t < nb)
+      do_bond<Real>(A, t);
+    else
+      do_contact<Real>(A, t - nb);
+  }
+}
+
+// Particle-platen contact (dd_Calculate_fijn_pwHM_2 + dd_Calculate_fijtmijt_pwHM_2,
+// md_compression_hm.cu:20-154) with radius ri and mass mi.  Returns the normal
+// force component along the platen axis.
+template <class Real>
+__device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int axis, Real sgn, Real wallvel,
+                                             Real riwm, Real ri, Real mi, const typename RT<Real>::V4& v,
+                                             const typename RT<Real>::V4& w, Real o[3], Real F[3], Real M[3]) {
+  using T = RT<Real>;
+  Real niw[3] = {0, 0, 0}, wv[3] = {0, 0, 0};
+  niw[axis] = sgn;
+  wv[axis] = wallvel;
+  Real cef1 = T::sqrt_rn(ri * T::fabs_(ri - riwm));
+  const Real Kn = Real(2) * sp.wallE * cef1;
+  const Real Kt = Real(8) * sp.wallG * cef1;
+  Real viw[3];
+  viw[0] = wv[0] - v.x + ri * (niw[1] * w.z - niw[2] * w.y);
+  viw[1] = wv[1] - v.y + ri * (niw[2] * w.x - niw[0] * w.z);
+  viw[2] = wv[2] - v.z + ri * (niw[0] * w.y - niw[1] * w.x);
+  const Real vn = niw[0] * viw[0] + niw[1] * viw[1] + niw[2] * viw[2];
+  const Real fiwnm = (riwm - ri) * Kn * T::kTwoThirds;
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * mi);
+  const Real fiwn[3] = {niw[0] * (fiwnm + cef1), niw[1] * (fiwnm + cef1), niw[2] * (fiwnm + cef1)};
+  const Real vt[3] = {viw[0] - niw[0] * vn, viw[1] - niw[1] * vn, viw[2] - niw[2] * vn};
+  cef1 = niw[0] * o[0] + niw[1] * o[1] + niw[2] * o[2];
+  Real ot[3] = {o[0] - niw[0] * cef1, o[1] - niw[1] * cef1, o[2] - niw[2] * cef1};
+  cef1 = (ot[0] * ot[0] + ot[1] * ot[1]) + ot[2] * ot[2];
+  if (cef1 > Real(1e-18)) {
+    cef1 = T::rcp(cef1);
+    // md_compression_hm.cu:91 multiplies the x and y components in the first term
+    cef1 *= (o[0] * o[1] + o[1] * o[1]) + o[2] * o[2];
+    cef1 = T::sqrt_rn(cef1);
+    ot[0] *= cef1;
+    ot[1] *= cef1;
+    ot[2] *= cef1;
+  }
+  const Real dt = sp.dt;
+  ot[0] += vt[0] * dt;
+  ot[1] += vt[1] * dt;
+  ot[2] += vt[2] * dt;
+  Real ft[3] = {ot[0] * Kt, ot[1] * Kt, ot[2] * Kt};
+  const Real ftmm = (ft[0] * ft[0] + ft[1] * ft[1]) + ft[2] * ft[2];
+  if (ftmm > sp.mu * sp.mu * fiwnm * fiwnm) {
+    cef1 = sp.mu * T::fabs_(fiwnm) * T::rsqrt_rn(ftmm);
+    ft[0] *= cef1;
+    ft[1] *= cef1;
+    ft[2] *= cef1;
+    cef1 = T::rcp(Kt);
+    ot[0] = ft[0] * cef1;
+    ot[1] = ft[1] * cef1;
+    ot[2] = ft[2] * cef1;
+  } else {
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * mi);
+    ft[0] += vt[0] * cef1;
+    ft[1] += vt[1] * cef1;
+    ft[2] += vt[2] * cef1;
+  }
+  o[0] = ot[0];
+  o[1] = ot[1];
+  o[2] = ot[2];
+  const Real mt[3] = {(niw[1] * ft[2] - niw[2] * ft[1]) * ri, (niw[2] * ft[0] - niw[0] * ft[2]) * ri,
+                      (niw[0] * ft[1] - niw[1] * ft[0]) * ri};
+  const Real wim = (w.x * w.x + w.y * w.y) + w.z * w.z;
+  Real madd[3] = {0, 0, 0};
+  if (wim > Real(1e-18)) {
+    cef1 = -sp.mur * T::fabs_(fiwnm) * T::rsqrt_rn(wim);
+    madd[0] = w.x * cef1;
+    madd[1] = w.y * cef1;
+    madd[2] = w.z * cef1;
+  }
+  F[0] += fiwn[0] + ft[0];
+  F[1] += fiwn[1] + ft[1];
+  F[2] += fiwn[2] + ft[2];
+  M[0] += mt[0] + madd[0];
+  M[1] += mt[1] + madd[1];
+  M[2] += mt[2] + madd[2];
+  return fiwn[axis];
+}
+
+// Loading controller of one sample after its platen force sums are complete:
+// SumInteractions + SumForces{U,B}Loading + Compress{U,B}_S3.
+__device__ inline void controller_step(SampleCtl& C) {
+  const int ax = C.brazil ? 1 : 2;
+  const unsigned long long n = C.step;
+  const double sF0 = C.sFL[0], sF1 = C.sFL[1];
+  const bool save = C.dNsave && (n % C.dNsave == 0);
+  // SumInteractions (md_results.cu:198-203): bonded directed slots
+  if (save && C.stepsave < C.Nsave) C.rec_bonds[C.stepsave] = 2u * (uint32_t)max(C.bonds, 0);
+  // SumForces{U,B}Loading (md_results.cu:56-145)
+  if (save && C.stepsave < C.Nsave) {
+    C.rec[3 * C.stepsave] = (C.size_d[ax] - C.sz0) / C.sz0;
+    C.rec[3 * C.stepsave + 1] = sF0 * C.inv_Area;
+    C.rec[3 * C.stepsave + 2] = sF1 * C.inv_Area;
+    if (fabs(C.V) > 1e-9) ++C.stepsave;
+  }
+  C.Stress = 0.5 * (fabs(sF0) + fabs(sF1)) * C.inv_Area;
+  if (!C.Loading && C.Stress > C.MinStress) C.Loading = 1;
+  if (!C.brazil) {
+    if (C.FractureStress < C.Stress) {
+      C.FractureStress = C.Stress;
+      C.FractureStrain = (C.sz0 - C.size_d[ax]) / C.sz0;
+    }
+    if (C.Loading && (C.Stress < C.ZeroStress || C.Stress < C.ConditionFracture * C.FractureStress)) C.Fracture = 1;
+  } else {
+    if (C.FractureStress < C.Stress || C.Stress < C.ConditionFracture * C.FractureStress) {
+      C.FractureStress = C.Stress;
+      C.FractureStrain = (C.sz0 - C.size_d[ax]) / C.sz0;
+    }
+    if (C.Loading && C.Stress < C.ZeroStress) C.Fracture = 1;
+  }
+  // Compress{U,B}_S3 (md_data_types.h:347-379, 462-494)
+  const double pS = C.brazil ? 0.5 * (-sF0 + sF1) : 0.5 * fabs(-sF0 + sF1);
+  const double pD = fabs(sF0 + sF1);
+  if (pS * C.inv_Area < 1e-9) {
+    C.V = 10.0 * C.VLoad;
+  } else if (pD > 0.20 * pS && pS * C.inv_Area > 2.0e+6 / 1e9) {
+    if (fabs(C.V) > 1e-15) C.StepsStop = 0;
+    C.V = 0;
+    ++C.StepsStop;
+    if (C.StepsStop > 30000) C.Fracture = 1;
+  } else {
+    C.V = C.VLoad;
+  }
+  C.size_d[ax] += C.V * C.dt;
+  C.Top += 0.5 * C.V * C.dt;
+  C.Bottom -= 0.5 * C.V * C.dt;
+  C.Strain = (C.size_d[ax] - C.Size0) / C.Size0;
+  C.sFL[0] = 0.0;
+  C.sFL[1] = 0.0;
+  ++C.step;
+  // loop condition of h_Calculation{UniaxialCompression,BrazilTest}
+  if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps) C.done = 1;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
+  using T = RT<Real>;
+  using V4 = typename T::V4;
+  __shared__ int s_last;
+  // platen force partial sums of this block are kept per sample in registers and
+  // flushed with one double atomic per (sample, warp) run
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
+    const uint32_t s = A.sid[p];
+    SampleCtl& C = A.ctl[s];
+    double sb = 0.0, st = 0.0;
+    if (!C.done) {
+      const SampleParams<Real>& sp = A.sp[s];
+      V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
+      V4 f = A.frc[p], m = A.mom[p];
+      Real F[3] = {f.x, f.y, f.z}, M[3] = {m.x, m.y, m.z};
+      if (sp.axis >= 0) {
+        // d_UniaxialCompression_hm / d_BrazilCompression_hm (md_compression_hm.cu:167-239)
+        const int ax = sp.axis;
+        Real r[3];
+        r[0] = x.x - Real(sp.wall_c[0]);
+        if (ax == 2) {
+          r[1] = x.y - Real(sp.wall_c[1]);
+          r[2] = x.z;
+        } else {
+          r[1] = x.y;
+          r[2] = x.z - Real(sp.wall_c[2]);
+        }
+        const Real lat = (ax == 2) ? (r[0] * r[0] + r[1] * r[1]) : (r[0] * r[0] + r[2] * r[2]);
+        if (lat < Real(sp.wall_RR) && r[2] < Real(sp.zcut)) {
+          const Real wtop = Real((float)C.Top), wbot = Real((float)C.Bottom), wvel = Real((float)C.V);
+          V4 o4 = A.wallO[p];
+          Real o[3] = {o4.x, o4.y, o4.z};
+          const Real ri = x.w, mi = A.mass[p];
+          if (wtop - r[ax] < ri) {
+            st = -(double)wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
+          } else {
+            o[0] = o[1] = o[2] = Real(0);
+          }
+          if (r[ax] - wbot < ri) {
+            sb = -(double)wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
+          } else {
+            o[0] = o[1] = o[2] = Real(0);
+          }
+          A.wallO[p] = mk4(o[0], o[1], o[2], Real(0));
+        }
+      }
+      // d_CalculateIncrementsDEM: v += F dt/m, x += v dt, w += M dt/I
+      const Real dtm = v.w, dtI = w.w, dt = sp.dt;
+      v.x += F[0] * dtm;
+      v.y += F[1] * dtm;
+      v.z += F[2] * dtm;
+      x.x += v.x * dt;
+      x.y += v.y * dt;
+      x.z += v.z * dt;
+      w.x += M[0] * dtI;
+      w.y += M[1] * dtI;
+      w.z += M[2] * dtI;
+      // d_ParallelepipedCutRestriction: park escaped particles at the hidden point
+      const Real d0 = x.x - sp.space_c[0], d1 = x.y - sp.space_c[1], d2 = x.z - sp.space_c[2];
+      bool parked = false;
+      if (d0 - sp.space_h[0] > Real(0) || d0 + sp.space_h[0] < Real(0) || d1 - sp.space_h[1] > Real(0) ||
+          d1 + sp.space_h[1] < Real(0) || d2 - sp.space_h[2] > Real(0) || d2 + sp.space_h[2] < Real(0)) {
+        x.x = sp.hide[0];
+        x.y = sp.hide[1];
+        x.z = sp.hide[2];
+        v.x = v.y = v.z = Real(0);
+        parked = true;
+      }
+      A.pos[p] = x;
+      A.vel[p] = v;
+      A.omg[p] = w;
+      const Real z = Real(0);
+      if (A.keep_forces) {
+        A.frc[p] = mk4(F[0], F[1], F[2], z);
+        A.mom[p] = mk4(M[0], M[1], M[2], z);
+      } else {
+        A.frc[p] = mk4(z, z, z, z);
+        A.mom[p] = mk4(z, z, z, z);
+      }
+      // neighbour-list validity: displacement since the last build.  A parked
+      // particle interacts with nothing (all parked particles coincide, and
+      // pairs closer than 1e-10 are ignored), so it restarts its reference.
+      if (parked) {
+        A.pos_ref[p] = x;
+      } else {
+        const V4 x0 = ld4_rw(A.pos_ref + p);
+        const Real e0 = x.x - x0.x, e1 = x.y - x0.y, e2 = x.z - x0.z;
+        const Real d2s = (e0 * e0 + e1 * e1) + e2 * e2;
+        if (d2s > Real(0.25) * sp.skin_half2) C.rebuild = 1;  // past a quarter of the skin: rebuild soon
+        if (d2s > sp.skin_half2) C.stale = 1;                 // past half the skin: the list is no longer valid
+      }
+    }
+    // per-sample double sums: a full warp of one sample reduces with shuffles and
+    // issues one atomic; otherwise each contributing lane adds its own value
+    const unsigned full = __activemask();
+    bool uniform = false;
+    if (full == 0xFFFFFFFFu) {
+      const uint32_t s0 = __shfl_sync(full, s, 0);
+      uniform = __all_sync(full, s == s0);
+    }
+    if (uniform) {
+      for (int off = 16; off > 0; off >>= 1) {
+        sb += __shfl_xor_sync(full, sb, off);
+        st += __shfl_xor_sync(full, st, off);
+      }
+      if ((threadIdx.x & 31) == 0 && (sb != 0.0 || st != 0.0)) {
+        atomicAdd(&A.ctl[s].sFL[0], sb);
+        atomicAdd(&A.ctl[s].sFL[1], st);
+      }
+    } else if (sb != 0.0 || st != 0.0) {
+      atomicAdd(&A.ctl[s].sFL[0], sb);
+      atomicAdd(&A.ctl[s].sFL[1], st);
+    }
+  }
+  // the last block to finish runs the controllers
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
+    SampleCtl& C = A.ctl[s];
+    if (!C.done) controller_step(C);
+  }
+  if (threadIdx.x == 0) *A.blocks_done = 0;
+}
+
+}  // namespace dem

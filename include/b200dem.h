@@ -1,0 +1,249 @@
+/*
+ * b200dem: C ABI of the B200-native bonded-particle DEM step for rock
+ * calibration (uniaxial compression and Brazilian tests).
+ *
+ * Units are the reference's (md_phys_constants.h:5-14): length mm, mass mg,
+ * time us, so stresses are in GPa, forces in kN, velocities in mm/us.
+ * Positions are SoA: x[0..n) y[n..2n) z[2n..3n), as the reference's h_R.
+ *
+ * Every function returns 0 or a negative DEM_ERR_* code (dem_strerror names
+ * it); no exception crosses the ABI.  A context owns all its device memory
+ * and one CUDA stream; a context is not thread-safe.
+ *
+ * Entry points and the reference interfaces they replace:
+ *   dem_calculation_test      h_CalculationUniaxialCompression(md_task_data&, float* h_R)
+ *                             md_calculationuniaxialcompression.cu:126-340 and
+ *                             h_CalculationBrazilTest(md_task_data&, float* h_R)
+ *                             md_calculationbraziltest.cu:116-265 (declared mp.h:21-22)
+ *   dem_create_cylinder_sample  h_CreateCylinderSample(mp_mdparameters_data&, md_task_data&, uint, char[])
+ *                             md_createcylindersample.cu:184-439 (mp.h:16)
+ *   dem_load_cylinder_sample  h_LoadCylinderSample(mp_mdparameters_data&, uint, char[])
+ *                             md_createcylindersample.cu:441-466 (mp.h:17)
+ *   dem_save_sum_forces_loading  SaveSumForcesLoading(result_data&, char*) md_results.cu:168-180
+ *   dem_create/dem_add_sample/dem_setup/dem_run/dem_step and the getters expose the
+ *   same step pipeline at finer grain (set-up, stepping, state export), which the
+ *   reference keeps inside its drivers (md_calculationuniaxialcompression.cu:143-324).
+ *   dem_ref_cells / dem_ref_neighbor_sets reproduce CellDistribution
+ *   (md_cell_distribution.cu:130-172) and the interaction sets of
+ *   InteractionListConstruct/ReConstructBPM (md_interaction_list_construction.cu:382-404)
+ *   for parity checks.
+ */
+#ifndef B200DEM_H
+#define B200DEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEM_OK 0
+#define DEM_ERR_ARG (-1)
+#define DEM_ERR_CUDA (-2)
+#define DEM_ERR_STATE (-3)
+#define DEM_ERR_CAPACITY (-4)
+#define DEM_ERR_STALE (-5)
+#define DEM_ERR_IO (-6)
+#define DEM_ERR_NOMEM (-7)
+#define DEM_ERR_NUMERIC (-8)
+#define DEM_ERR_TIMEOUT (-9)
+
+#define DEM_TEST_NONE 0
+#define DEM_TEST_UNIAXIAL 1
+#define DEM_TEST_BRAZIL 2
+
+#define DEM_EMPTY 0xFFFFFFFFu
+
+typedef struct dem_ctx dem_ctx;
+
+typedef struct {
+  int precision;          /* 0: FP32, 1: FP64 */
+  int device;             /* CUDA device ordinal */
+  uint32_t pair_block;    /* threads per block of the pair kernel (0: 256) */
+  uint32_t pair_grid;     /* blocks of the pair kernel (0: 8 per SM) */
+  uint32_t particle_block;/* threads per block of the particle kernel (0: 256) */
+  uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
+  double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.25) */
+} dem_options;
+
+/* Micro-parameters of one specimen.  The first block is the reference's
+ * parameter set (SetInitialParameters, mp_determineconjgradient.cu:15-47);
+ * the second block holds the extensions (zero keeps the reference rule). */
+typedef struct {
+  double E;       /* Young modulus of particles and (by default) bonds, GPa */
+  double nu;      /* Poisson ratio (reference 0.247) */
+  double Ec, Gc;  /* bond normal / shear strength, GPa */
+  double b_r;     /* bond radius, mm (<= 0: bond_radius_factor * min(r_i, r_j)) */
+  double gap;     /* bond creation gap, mm: bond if r < r_i + r_j + gap */
+  double rho;     /* density, mg/mm^3 (reference 2.61) */
+  double p_r;     /* particle radius, mm, when no per-particle radii are given */
+  double p_e;     /* restitution coefficient (reference 0.6) */
+  double mu;      /* sliding friction (reference 0.45) */
+  double mur;     /* rolling friction (reference 0.05) */
+  double farcut;  /* far cut-off as a multiple of p_r (reference 3.2) */
+  /* extensions */
+  double E_bond;             /* > 0: bond Young modulus, separate from particle E */
+  double kn_ks;              /* > 0: bond normal/shear stiffness ratio (G_bond = E_bond / kn_ks) */
+  double Ec_sd, Gc_sd;       /* > 0: per-bond strengths drawn from N(Ec, Ec_sd), N(Gc, Gc_sd) */
+  double bond_radius_factor; /* used when b_r <= 0 */
+  double dt;                 /* > 0: time step, us (else the reference rule 0.05*min(T_R, T_bond)) */
+  double dt_rayleigh_factor; /* > 0: dt = factor * Rayleigh time of the smallest particle */
+  uint64_t seed;             /* per-bond strength draws */
+  int nobreak;               /* 1: bonds never break (elastic stage, d_CalculateForcesDEM_22_ncb) */
+  int reserved;
+} dem_material;
+
+/* Loading set-up of one specimen: the reference's sample_data and
+ * compression_data inputs (md_data_types.h:79-124, 203-495). */
+typedef struct {
+  int test;                  /* DEM_TEST_* */
+  int reserved;
+  double space_center[3];    /* escape box centre (reference S.center) */
+  double space_half[3];      /* escape box half size (reference S.spacesized2) */
+  double hidden_point[3];    /* where escaped particles are parked (reference S.hidenpoint) */
+  double zcut;               /* platen zone cut (reference S.center.z + S.spacesized2.z) */
+  double size_real[3];       /* specimen extent incl. radius (reference S.size_real) */
+  double center_real[3];     /* specimen centre (reference S.center_real) */
+  double velocity;           /* platen speed VLoad, mm/us (negative compresses) */
+  double min_stress;         /* GPa (reference UMinStress/BMinStress) */
+  double max_strain;         /* stop strain (reference UMaxStrain/BMaxStrain) */
+  double cond_fracture;      /* stop when stress < cond_fracture * peak (reference ConditionFracture) */
+  double p_r_platen;         /* radius used by the platen-area formula (0: material p_r or mean radius) */
+  uint32_t dNsave;           /* record every dNsave steps (reference dNSaveU/dNSaveB) */
+  uint32_t reserved2;
+  uint64_t max_steps;        /* safety bound on the loading loop (0: unlimited) */
+} dem_loading;
+
+typedef struct {
+  double FractureStress;     /* peak stress, GPa */
+  double FractureStrain;     /* strain at peak */
+  double LinearityDeviation; /* reference CalculateLinearityDeviation (uniaxial) */
+  double Destruction;        /* surviving bond fraction (reference CalculateDestruction) */
+  double Strain, Stress, dt;
+  double platen_top, platen_bottom, platen_velocity;
+  uint64_t steps;
+  uint32_t stepsave;         /* number of records */
+  uint32_t bonds_initial, bonds_now;  /* intact undirected bonds */
+  int fracture, done, stale;
+} dem_result;
+
+/* --- context and specimens --- */
+int dem_create(const dem_options* opt, dem_ctx** out);
+void dem_destroy(dem_ctx* ctx);
+const char* dem_strerror(int code);
+int dem_device_count(int* n);
+
+/* Adds one specimen.  xyz: 3n floats (mm, SoA); radii: n floats or NULL
+ * (all mat->p_r).  All specimens of a context advance together (one launch
+ * per kernel for all of them).  Returns the specimen id in *sample. */
+int dem_add_sample(dem_ctx* ctx, const dem_material* mat, const dem_loading* load, const float* xyz,
+                   const float* radii, uint32_t n, int32_t* sample);
+/* Uploads, Morton-sorts, creates bonds and the contact list. */
+int dem_setup(dem_ctx* ctx);
+/* Advances until every specimen met its stop condition or max_steps steps ran. */
+int dem_run(dem_ctx* ctx, uint64_t max_steps, uint64_t* steps_done);
+/* Advances exactly nsteps steps (finished specimens stay frozen). */
+int dem_step(dem_ctx* ctx, uint32_t nsteps);
+/* Stage control for parity checks: bit 0 pair forces, bit 1 platens +
+ * integration; bit 2 keeps the total force/moment of the step readable by
+ * dem_get_particles instead of clearing the accumulators. */
+int dem_step_stages(dem_ctx* ctx, int stages);
+int dem_sync(dem_ctx* ctx);
+
+int dem_counts(dem_ctx* ctx, uint32_t* particles, uint32_t* bonds, uint32_t* contacts, uint32_t* samples);
+int dem_sample_result(dem_ctx* ctx, int32_t sample, dem_result* out);
+/* Loading record: 3 doubles per entry (strain, sigma_bottom, sigma_top in GPa)
+ * and bonded directed-slot counts, as the reference's h_sFL / h_sSI. */
+int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n);
+
+/* Particle state in the caller's original order, SoA (3n each, NULL skips). */
+int dem_get_particles(dem_ctx* ctx, int32_t sample, float* R, float* V, float* W, float* F, float* M,
+                      float* Oiwt);
+int dem_get_particles_d(dem_ctx* ctx, int32_t sample, double* R, double* V, double* W, double* F, double* M,
+                        double* Oiwt);
+int dem_set_particles(dem_ctx* ctx, int32_t sample, const float* R, const float* V, const float* W,
+                      const float* Oiwt);
+/* Pair state: for every bond and contact-list pair, original indices (i < j),
+ * kind (1 intact bond, 2 broken bond, 3 contact) and 16 floats
+ * (1/L0, prev-direction xyz, tangential xyz, twisting xyz, bending xyz,
+ * normal strength, shear strength, bond radius). */
+int dem_get_pairs(dem_ctx* ctx, int32_t sample, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind,
+                  float* state, uint32_t* n);
+/* Overwrites the state of listed pairs (the first 13 values of the record
+ * layout; kind 1/2 sets a bond intact/broken, contacts take only the
+ * tangential history). */
+int dem_set_pairs(dem_ctx* ctx, int32_t sample, uint32_t n, const uint32_t* i, const uint32_t* j,
+                  const uint32_t* kind, const float* state);
+/* Platen state of a specimen (top, bottom position in mm; velocity mm/us). */
+int dem_set_platens(dem_ctx* ctx, int32_t sample, double top, double bottom, double velocity);
+/* Rebuilds the contact list now (normally automatic). */
+int dem_rebuild_contacts(dem_ctx* ctx);
+/* Advances nsteps steps from the captured step graph; *ms = device time of
+ * the whole run (CUDA events on the context's stream, rebuilds included). */
+int dem_run_timed(dem_ctx* ctx, uint64_t nsteps, double* ms);
+/* Advances nsteps steps launching the two step kernels one by one with CUDA
+ * events around each: average per-launch times of the pair kernel and the
+ * particle kernel, and the mean number of touching contacts per step. */
+int dem_profile(dem_ctx* ctx, uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching);
+
+/* --- reference-layout parity exports (stateless, run on the current device) --- */
+/* CellDistribution: CI[n], CIs[2n] (sorted keys then particle indices), pnC[2*nx*ny*nz]. */
+int dem_ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
+                  uint32_t* CIs, uint32_t* pnC);
+/* Interaction sets: for each particle the sorted partners j != i with
+ * r^2 < add_thr, !(r^2 > del_thr), !(r^2 < 1e-10), padded with DEM_EMPTY to cap. */
+int dem_ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz,
+                          float add_thr, float del_thr, uint32_t cap, uint32_t* sets, uint32_t* overflow);
+
+/* --- reference entry points --- */
+/* One loading test of one specimen from host positions to macro results and
+ * the loading record (h_Calculation{UniaxialCompression,BrazilTest}). */
+int dem_calculation_test(const dem_options* opt, const dem_material* mat, const dem_loading* load,
+                         const float* h_R, const float* radii, uint32_t n, dem_result* out, double* rec,
+                         uint32_t* rec_bonds, uint32_t rec_cap, uint32_t* rec_n);
+/* Sample text file (first line n, then "x y z" in metres per line):
+ * LoadParticleDATAtxt / SaveParticleDATAtxt, md_createcylindersample.cu:144-182.
+ * dem_load_cylinder_sample also returns the bounding box of h_LoadCylinderSample
+ * (size_real incl. 2*p_r, center_real). */
+int dem_load_cylinder_sample(const char* path, double p_r, float* xyz, uint32_t cap, uint32_t* n,
+                             double size_real[3], double center_real[3]);
+int dem_save_cylinder_sample(const char* path, const float* xyz, uint32_t n, const double hidden_point[3]);
+/* "EpsZ StressZ_bottom StressZ_top" file of SaveSumForcesLoading (stresses in Pa). */
+int dem_save_sum_forces_loading(const char* path, const double* rec, uint32_t n);
+
+/* Seeded sample creation (the role of h_CreateCylinderSample): n spheres with
+ * radii uniform in [r_min, r_max] filled at random into a z-axis cylinder
+ * (a column for the uniaxial test, a disc for the Brazilian test), grown from
+ * 30% of the final packing fraction with damped soft-sphere relaxation, then
+ * FIRE-relaxed until the largest overlap / (r_i + r_j) is below overlap_tol. */
+typedef struct {
+  double center[3];          /* cylinder centre, mm */
+  double radius;             /* cylinder radius, mm */
+  double half_height;        /* cylinder half height, mm */
+  double r_min, r_max;       /* particle radii, mm */
+  double E, nu, rho;         /* particle material (GPa, -, mg/mm^3): stiffness and time step */
+  double overlap_tol;        /* target largest relative overlap */
+  uint32_t n;                /* number of particles */
+  uint32_t growth_stages;    /* radius increments */
+  uint32_t steps_per_stage;  /* relaxation steps after each increment */
+  uint32_t max_fire_steps;   /* FIRE steps at the final radii */
+  uint64_t seed;
+  int device;
+  int reserved;
+} dem_pack_params;
+
+typedef struct {
+  uint64_t steps;
+  double max_overlap;        /* largest relative overlap at the end */
+  double packing_fraction;   /* sphere volume / cylinder volume */
+  uint32_t rebuilds;
+  uint32_t reserved;
+} dem_pack_report;
+
+int dem_create_cylinder_sample(const dem_pack_params* p, float* xyz, float* radii, uint32_t cap, uint32_t* n,
+                               dem_pack_report* rep);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

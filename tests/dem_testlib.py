@@ -32,6 +32,7 @@ class RefCase:
     N: int
     lsi: tuple
     space: tuple
+    kw: dict = None
 
 
 def fcc_cylinder(center, radius: float, half_h: float, d: float, jitter: float, rng) -> np.ndarray:
@@ -70,7 +71,10 @@ def ref_case(seed: int = 1, lsi=(0.0045, 0.0045, 0.006), space=(0.009, 0.009, 0.
     cmp = prm.compress_for(brazil, size_real, center_real, pot.p_r, minstress_si / prm.STRESS, maxstrain,
                            condfract)
     sc = sim.scalars_from(pot, cells, smp, cmp, velocity_si / prm.VELOCITY)
-    return RefCase(pot=pot, cells=cells, smp=smp, cmp=cmp, sc=sc, R=R, N=N, lsi=lsi, space=space)
+    kw = dict(seed=seed, p_r_si=p_r_si, E=E, Ec=Ec, Gc=Gc, br_si=br_si, gap_si=gap_si, brazil=brazil,
+              velocity_si=velocity_si, minstress_si=minstress_si, maxstrain=maxstrain, condfract=condfract,
+              farcut=farcut)
+    return RefCase(pot=pot, cells=cells, smp=smp, cmp=cmp, sc=sc, R=R, N=N, lsi=lsi, space=space, kw=kw)
 
 
 def perturb(st: sim.RefState, rng, dx=0.004, v=2e-4, w=2e-3) -> None:

@@ -241,6 +241,8 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--specimens", type=int, default=2,
+                    help="specimens of the workload advanced together per GPU (2 discs: state above the L2)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
@@ -248,11 +250,13 @@ def main() -> int:
         return run_reference(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
-    spec = build_specimen(dem, args.workload, 1 + rank, local)
+    specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
+    spec = specs[0]
     ctx = dem.Context(device=local, graph_steps=200)
-    sid = ctx.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
+    sids = [ctx.add_sample(sp.material, sp.loading, sp.xyz, sp.radii) for sp in specs]
     ctx.setup()
     cnt = ctx.counts()
+    n_gpu = cnt["particles"]
     ctx.run_timed(args.warmup)
     D.barrier()
     clk = Clocks(local)
@@ -260,22 +264,43 @@ def main() -> int:
     clocks = clk.stop()
     D.barrier()
     ms_max = D.max(ms)
-    n_total = D.sum(float(spec.n))
+    n_total = D.sum(float(n_gpu))
     value = n_total * args.steps / (ms_max * 1e-3)
     # per-kernel timing of the same pipeline (events around each launch)
     prof = ctx.profile(min(args.steps, 300))
-    res = ctx.result(sid)
-    A = algorithmic_bytes(spec.n, res["bonds_now"], prof["touching"])
+    res = [ctx.result(s) for s in sids]
+    bonds = sum(r["bonds_now"] for r in res)
+    A = algorithmic_bytes(n_gpu, bonds, prof["touching"])
     achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    state_mb = (spec.n * (5 * 16 + 16 + 8) + cnt["bonds"] * (8 + 4 * 16) + cnt["contacts"] * 24) / 1e6
-    # end to end through the public C ABI: host positions in, results and record out
-    ld = spec.loading
-    ld.max_steps = args.steps
+    state_mb = (n_gpu * (7 * 16 + 8) + cnt["bonds"] * (8 + 4 * 16) + cnt["contacts"] * 24) / 1e6
+    stale = sum(r["stale"] for r in res)
+    ctx.close()
+    # the same pipeline on one specimen alone (state inside the L2), for reference
+    one = dem.Context(device=local, graph_steps=200)
+    one.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
+    one.setup()
+    one.run_timed(args.warmup)
+    ms1 = one.run_timed(args.steps)
+    prof1 = one.profile(min(args.steps, 300))
+    one.close()
+    # end to end through the public API with host buffers: positions uploaded,
+    # set-up (Morton sort, bonds, contact list), K steps, results and records read back
     t0 = time.perf_counter()
-    r_e2e, rec, rb = dem.calculation_test(spec.material, ld, spec.xyz, spec.radii, rec_cap=1 << 16)
+    e2 = dem.Context(device=local, graph_steps=200)
+    for sp in specs:
+        ld = dem.Loading.from_buffer_copy(sp.loading)
+        ld.max_steps = args.steps
+        e2.add_sample(sp.material, ld, sp.xyz, sp.radii)
+    e2.setup()
+    e2.run(args.steps)
+    recs = [e2.record(k) for k in range(len(specs))]
+    _ = [e2.result(k) for k in range(len(specs))]
+    e2.close()
     t_e2e = time.perf_counter() - t0
-    e2e_val = D.sum(spec.n * args.steps / t_e2e) if ws > 1 else spec.n * args.steps / t_e2e
+    e2e_val = D.sum(n_gpu * args.steps / t_e2e)
+    h2d = sum(sp.xyz.nbytes + sp.radii.nbytes for sp in specs)
+    d2h = sum(r.nbytes + b.nbytes for r, b in recs) + len(specs) * 160
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, el, th = cpu_baseline(spec, args.cpu_steps, os.cpu_count() or 1)
@@ -285,27 +310,31 @@ def main() -> int:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded packing, FIRE-relaxed)",
-        "config": {"workload": f"{args.workload}: {spec.n} spheres, radii U[0.18,0.30] mm, Brazilian platens"
-                               if args.workload == "brazilian_disc" else f"{args.workload}: {spec.n} spheres",
-                   "particles": spec.n, "bonds": res["bonds_now"], "contacts_listed": cnt["contacts"],
-                   "touching_contacts": prof["touching"], "parallelism": f"{ws} independent specimen(s)",
-                   "l2": f"state {state_mb:.0f} MB per GPU, larger than the 126 MB L2",
-                   "packing": spec.pack},
+        "dtype": "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
+        "config": {"workload": f"{args.specimens} x {args.workload} ({spec.n} spheres each, radii "
+                               f"U[0.18,0.30] mm, Brazilian platens at 0.02 m/s) advanced together"
+                               if args.workload == "brazilian_disc" else
+                               f"{args.specimens} x {args.workload} ({spec.n} spheres each)",
+                   "particles_per_gpu": n_gpu, "bonds": bonds, "contacts_listed": cnt["contacts"],
+                   "touching_contacts": prof["touching"], "parallelism": f"{ws} GPU(s), independent specimens",
+                   "l2": f"inputs larger than L2: state {state_mb:.0f} MB per GPU vs 126 MB L2, no flush",
+                   "packing": spec.pack, "stale_lists": stale,
+                   "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
+                                       "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
+                                       "note": "state inside the L2"}},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
                      "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
                      "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
-        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": (spec.xyz.nbytes + spec.radii.nbytes) /
-                args.steps, "d2h_bytes_per_step": (rec.nbytes + rb.nbytes + 160) / args.steps,
-                "seconds": t_e2e, "note": "dem_calculation_test: upload, set-up, steps, results"},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e,
+                "note": "public API from host positions: upload, set-up, steps, results and records read back"},
         "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
     D.close()
     return 0
 

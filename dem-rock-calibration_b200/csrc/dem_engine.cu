@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -197,6 +198,14 @@ class Engine final : public EngineBase {
     RC(build_contacts(true));
     RC(init_controllers());
     CK(blocks_done_.alloc(1));
+    CK(blk_stat_.alloc(2 * (size_t)num_sms_ * 8 + 64));
+    CK(stat_.alloc(2));
+    min_skin_ = 1e300;
+    max_dt_ = 0;
+    for (auto& s : samples_) {
+      min_skin_ = std::min(min_skin_, opt_.skin_factor * s.rmin);
+      max_dt_ = std::max(max_dt_, s.dt);
+    }
     CK(cudaDeviceSynchronize());
     setup_done_ = true;
     return DEM_OK;
@@ -641,6 +650,8 @@ class Engine final : public EngineBase {
     A.blocks_done = blocks_done_.p;
     A.keep_forces = 0;
     A.touching = nullptr;
+    A.blk_stat = blk_stat_.p;
+    A.stat = stat_.p;
     return A;
   }
 
@@ -680,14 +691,17 @@ class Engine final : public EngineBase {
 
   struct Flags {
     uint32_t done, rebuild, stale;
+    float v2max, d2max;
   };
 
   int read_flags(Flags& f) {
     const uint32_t S = (uint32_t)samples_.size();
     hctl_.resize(S);
+    float st[2] = {0.f, 0.f};
     CK(cudaMemcpyAsync(hctl_.data(), ctl_.p, S * sizeof(SampleCtl), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(st, stat_.p, 2 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
-    f = {1, 0, 0};
+    f = {1, 0, 0, st[0], st[1]};
     for (auto& c : hctl_) {
       f.done &= c.done ? 1u : 0u;
       f.rebuild |= c.rebuild;
@@ -696,14 +710,29 @@ class Engine final : public EngineBase {
     return DEM_OK;
   }
 
+  // after a rebuild: clear the per-sample rebuild/stale flags and the
+  // displacement maximum (positions are the new reference)
   int clear_rebuild_flags() {
-    // clear rebuild on the device copy (host copy is fresh from read_flags)
     for (uint32_t si = 0; si < hctl_.size(); ++si) {
-      uint32_t z = 0;
-      CK(cudaMemcpyAsync(&ctl_.p[si].rebuild, &z, sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+      const uint32_t z[2] = {0, 0};
+      static_assert(offsetof(SampleCtl, stale) == offsetof(SampleCtl, rebuild) + sizeof(uint32_t), "layout");
+      CK(cudaMemcpyAsync(&ctl_.p[si].rebuild, z, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
     }
+    CK(cudaMemsetAsync(stat_.p + 1, 0, sizeof(float), stream_));
     CK(cudaStreamSynchronize(stream_));
     return DEM_OK;
+  }
+
+  // Largest number of steps the next chunk may take: a particle may not move
+  // more than half the skin between list builds; with the speed of the last
+  // chunk and a safety factor of 2 on the remaining distance.
+  uint64_t chunk_steps(const Flags& f) const {
+    const double budget = 0.5 * min_skin_ - std::sqrt((double)f.d2max);
+    const double v = std::sqrt((double)f.v2max);
+    if (!(v > 0)) return opt_.graph_steps;
+    const double k = 0.5 * budget / (v * max_dt_);
+    if (!(k >= 1.0)) return 1;
+    return (uint64_t)std::min<double>(k, opt_.graph_steps);
   }
 
   int prepare() {
@@ -725,36 +754,31 @@ class Engine final : public EngineBase {
     uint64_t steps = 0;
     Flags f{};
     RC(read_flags(f));
-    if (f.rebuild) {
-      RC(build_contacts(false));
-      RC(clear_rebuild_flags());
-    }
-    while (steps < max_steps) {
-      if (stop_when_done && f.done) break;
-      const uint64_t left = max_steps - steps;
-      if (left >= opt_.graph_steps) {
-        if (!graph_exec_) RC(capture_graph());
-        CK(cudaGraphLaunch(graph_exec_, stream_));
-        steps += opt_.graph_steps;
-      } else {
-        StepArgs<Real> A = args();
-        for (uint64_t k = 0; k < left; ++k) launch_step(A, 3);
-        steps += left;
-      }
-      CK(cudaGetLastError());
-      RC(read_flags(f));
-      if (f.stale) {
-        stale_ = true;
-        break;
-      }
-      if (f.rebuild) {
+    while (true) {
+      if (f.stale) ++stale_events_;
+      if (f.rebuild || f.stale || (double)f.d2max > 0.0625 * min_skin_ * min_skin_) {
         RC(build_contacts(false));
         RC(clear_rebuild_flags());
+        f.d2max = 0.f;
       }
+      if (steps >= max_steps || (stop_when_done && f.done)) break;
+      const uint64_t left = max_steps - steps;
+      const uint64_t chunk = std::min(left, chunk_steps(f));
+      CK(cudaMemsetAsync(stat_.p, 0, sizeof(float), stream_));  // speed maximum of this chunk
+      if (chunk == opt_.graph_steps) {
+        if (!graph_exec_) RC(capture_graph());
+        CK(cudaGraphLaunch(graph_exec_, stream_));
+      } else {
+        StepArgs<Real> A = args();
+        for (uint64_t k = 0; k < chunk; ++k) launch_step(A, 3);
+      }
+      steps += chunk;
+      CK(cudaGetLastError());
+      RC(read_flags(f));
     }
     total_steps_ += steps;
     if (done_steps) *done_steps = steps;
-    return stale_ ? DEM_ERR_STALE : DEM_OK;
+    return DEM_OK;
   }
 
   int run_until_done(uint64_t max_steps, uint64_t* done) override { return run(max_steps, done, true); }
@@ -807,7 +831,7 @@ class Engine final : public EngineBase {
     out->bonds_now = (uint32_t)std::max(C.bonds, 0);
     out->fracture = (int)C.Fracture;
     out->done = (int)C.done;
-    out->stale = C.stale ? 1 : 0;
+    out->stale = (int)stale_events_;
     // host post-processing of the record (CalculateLinearityDeviation, CalculateDestruction)
     std::vector<double> rec;
     std::vector<uint32_t> rb;
@@ -1132,12 +1156,13 @@ class Engine final : public EngineBase {
     if (touching) *touching = (double)tc / nsteps;
     Flags f{};
     RC(read_flags(f));
-    if (f.rebuild) {
+    if (f.stale) ++stale_events_;
+    if (f.rebuild || f.stale) {
       RC(build_contacts(false));
       RC(clear_rebuild_flags());
     }
     total_steps_ += nsteps;
-    return f.stale ? DEM_ERR_STALE : DEM_OK;
+    return DEM_OK;
   }
 
  private:
@@ -1147,7 +1172,8 @@ class Engine final : public EngineBase {
   int num_sms_ = 148;
   bool setup_done_ = false, forces_dirty_ = false, contacts_dirty_ = false, stale_ = false;
   cudaError_t last_cuda_ = cudaSuccess;
-  uint64_t total_steps_ = 0, rebuilds_ = 0;
+  uint64_t total_steps_ = 0, rebuilds_ = 0, stale_events_ = 0;
+  double min_skin_ = 0, max_dt_ = 0;
 
   std::vector<SampleHost> samples_;
   std::vector<SampleParams<Real>> hparams_;
@@ -1170,6 +1196,7 @@ class Engine final : public EngineBase {
   DBuf<Grid<Real>> grids_;
   DBuf<uint32_t> cell_of_, cell_count_, cell_start_, cell_cursor_, cell_list_, cnt_, offs_, ovf_, scan_tmp_;
   DBuf<unsigned int> blocks_done_;
+  DBuf<float> blk_stat_, stat_;
   std::vector<std::unique_ptr<DBuf<double>>> rec_;
   std::vector<std::unique_ptr<DBuf<uint32_t>>> rec_bonds_;
 };

@@ -52,6 +52,8 @@ struct StepArgs {
   unsigned int* blocks_done;
   int keep_forces;  // 1: leave the step's total force/moment in frc/mom (parity checks)
   unsigned long long* touching;  // non-null: count touching contacts (algorithmic-byte accounting)
+  float* blk_stat;  // per block: max |v|^2 and max displacement^2 since the last list build
+  float* stat;      // running maxima over blocks and steps (reset by the host)
 };
 
 // Hertz-Mindlin contact of pair (i, j) seen from i (n points from i to j), in
@@ -499,6 +501,7 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   __shared__ int s_last;
   // platen force partial sums of this block are kept per sample in registers and
   // flushed with one double atomic per (sample, warp) run
+  float my_v2 = 0.f, my_d2 = 0.f;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
@@ -583,6 +586,8 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
         const Real d2s = (e0 * e0 + e1 * e1) + e2 * e2;
         if (d2s > Real(0.25) * sp.skin_half2) C.rebuild = 1;  // past a quarter of the skin: rebuild soon
         if (d2s > sp.skin_half2) C.stale = 1;                 // past half the skin: the list is no longer valid
+        my_d2 = fmaxf(my_d2, (float)d2s);
+        my_v2 = fmaxf(my_v2, (float)((v.x * v.x + v.y * v.y) + v.z * v.z));
       }
     }
     // per-sample double sums: a full warp of one sample reduces with shuffles and
@@ -607,6 +612,27 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       atomicAdd(&A.ctl[s].sFL[1], st);
     }
   }
+  // block maxima of speed and displacement (the host sizes the next chunk of
+  // steps from them so no particle outruns the contact-list skin)
+  __shared__ float s_v2[32], s_d2[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    my_v2 = fmaxf(my_v2, __shfl_xor_sync(0xFFFFFFFFu, my_v2, o));
+    my_d2 = fmaxf(my_d2, __shfl_xor_sync(0xFFFFFFFFu, my_d2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_v2[threadIdx.x >> 5] = my_v2;
+    s_d2[threadIdx.x >> 5] = my_d2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = 0.f, b = 0.f;
+    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; ++w) {
+      a = fmaxf(a, s_v2[w]);
+      b = fmaxf(b, s_d2[w]);
+    }
+    A.blk_stat[2 * blockIdx.x] = a;
+    A.blk_stat[2 * blockIdx.x + 1] = b;
+  }
   // the last block to finish runs the controllers
   __threadfence();
   __syncthreads();
@@ -618,7 +644,32 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
     SampleCtl& C = A.ctl[s];
     if (!C.done) controller_step(C);
   }
-  if (threadIdx.x == 0) *A.blocks_done = 0;
+  float a = 0.f, b = 0.f;
+  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    a = fmaxf(a, __ldcg(A.blk_stat + 2 * k));
+    b = fmaxf(b, __ldcg(A.blk_stat + 2 * k + 1));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmaxf(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
+    b = fmaxf(b, __shfl_xor_sync(0xFFFFFFFFu, b, o));
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    s_v2[threadIdx.x >> 5] = a;
+    s_d2[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = A.stat[0];
+    b = A.stat[1];
+    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; ++w) {
+      a = fmaxf(a, s_v2[w]);
+      b = fmaxf(b, s_d2[w]);
+    }
+    A.stat[0] = a;
+    A.stat[1] = b;
+    *A.blocks_done = 0;
+  }
 }
 
 }  // namespace dem

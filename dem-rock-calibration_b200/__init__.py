@@ -121,6 +121,7 @@ def _declare(L):
     L.dem_profile.argtypes = [_vp, _u32, P(C.c_double), P(C.c_double), P(C.c_double)]
     L.dem_create_cylinder_sample.argtypes = [P(PackParams), _vp, _vp, _u32, P(_u32), P(PackReport)]
     L.dem_ref_cells.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
+    L.dem_ref_cells_static.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_neighbor_sets.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, C.c_float, C.c_float, _u32, _vp,
                                         P(_u32)]
     L.dem_calculation_test.argtypes = [P(Options), P(Material), P(Loading), _vp, _vp, _u32, P(Result), _vp, _vp,
@@ -382,6 +383,17 @@ def ref_cells(xyz: np.ndarray, a: float, nx: int, ny: int, nz: int):
     CIs = np.zeros(2 * n, np.uint32)
     pnC = np.zeros(2 * nx * ny * nz, np.uint32)
     _ck(_lib().dem_ref_cells(_p(xyz), n, a, nx, ny, nz, _p(CI), _p(CIs), _p(pnC)), "dem_ref_cells")
+    return CI, CIs, pnC
+
+
+def ref_cells_static(xyz: np.ndarray, a: float, nx: int, ny: int, nz: int):
+    """ref_cells through dem_ref_cells_static (no allocation; limited sizes)."""
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    n = xyz.size // 3
+    CI = np.zeros(n, np.uint32)
+    CIs = np.zeros(2 * n, np.uint32)
+    pnC = np.zeros(2 * nx * ny * nz, np.uint32)
+    _ck(_lib().dem_ref_cells_static(_p(xyz), n, a, nx, ny, nz, _p(CI), _p(CIs), _p(pnC)), "dem_ref_cells_static")
     return CI, CIs, pnC
 
 

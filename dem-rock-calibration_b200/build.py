@@ -19,7 +19,7 @@ ROOT = PKG.parent
 SRC = PKG / "csrc"
 OUT = PKG / "libb200dem.so"
 
-SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_capi.cpp"]
+SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_noalloc.cu", "dem_capi.cpp"]
 HEADERS = ["dem_common.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
            "dem_engine.h"]
 

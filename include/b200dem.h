@@ -195,6 +195,21 @@ int dem_ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t n
 int dem_ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz,
                           float add_thr, float del_thr, uint32_t cap, uint32_t* sets, uint32_t* overflow);
 
+/* dem_ref_cells without any allocation (no counterpart in the reference: the
+ * reference's CellDistribution works on buffers its caller allocated).  Same
+ * arguments and outputs as dem_ref_cells; the device work runs out of one
+ * file-scope device array of DEM_STATIC_SCRATCH_BYTES per device, whose
+ * address is looked up once per device with cudaGetSymbolAddress.  Returns
+ * DEM_ERR_CAPACITY when n > DEM_STATIC_MAX_PARTICLES or nx*ny*nz >
+ * DEM_STATIC_MAX_CELLS.  Calls on the same device share that array: calls
+ * that overlap in time (several host threads) race on it and must be
+ * serialised by the caller. */
+#define DEM_STATIC_MAX_PARTICLES 65536u
+#define DEM_STATIC_MAX_CELLS 65536u
+#define DEM_STATIC_SCRATCH_BYTES 4718592u /* 4.5 MiB */
+int dem_ref_cells_static(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
+                         uint32_t* CIs, uint32_t* pnC);
+
 /* --- reference entry points --- */
 /* One loading test of one specimen from host positions to macro results and
  * the loading record (h_Calculation{UniaxialCompression,BrazilTest}). */

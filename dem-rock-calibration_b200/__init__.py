@@ -36,6 +36,8 @@ class DemError(RuntimeError):
     def __init__(self, code: int, where: str = ""):
         self.code = code
         msg = _lib().dem_strerror(code).decode() if _LIB else str(code)
+        if code == -2 and _LIB:
+            msg += ": " + _lib().dem_last_error_detail().decode()
         super().__init__(f"{where}: {msg} ({code})" if where else f"{msg} ({code})")
 
 
@@ -69,7 +71,7 @@ class PackParams(C.Structure):
                 ("r_min", C.c_double), ("r_max", C.c_double), ("E", C.c_double), ("nu", C.c_double),
                 ("rho", C.c_double), ("overlap_tol", C.c_double), ("n", C.c_uint32), ("growth_stages", C.c_uint32),
                 ("steps_per_stage", C.c_uint32), ("max_fire_steps", C.c_uint32), ("seed", C.c_uint64),
-                ("device", C.c_int), ("reserved", C.c_int)]
+                ("device", C.c_int), ("fire_variant", C.c_int)]
 
 
 class PackReport(C.Structure):
@@ -83,7 +85,8 @@ class Result(C.Structure):
                 ("Stress", C.c_double), ("dt", C.c_double), ("platen_top", C.c_double),
                 ("platen_bottom", C.c_double), ("platen_velocity", C.c_double), ("steps", C.c_uint64),
                 ("stepsave", C.c_uint32), ("bonds_initial", C.c_uint32), ("bonds_now", C.c_uint32),
-                ("fracture", C.c_int), ("done", C.c_int), ("stale", C.c_int)]
+                ("fracture", C.c_int), ("done", C.c_int), ("stale", C.c_int), ("reserved", C.c_int),
+                ("E_chord", C.c_double), ("nu", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -120,6 +123,9 @@ def _declare(L):
     L.dem_run_timed.argtypes = [_vp, _u64, P(C.c_double)]
     L.dem_profile.argtypes = [_vp, _u32, P(C.c_double), P(C.c_double), P(C.c_double)]
     L.dem_create_cylinder_sample.argtypes = [P(PackParams), _vp, _vp, _u32, P(_u32), P(PackReport)]
+    L.dem_last_error_detail.restype = C.c_char_p
+    L.dem_last_error_detail.argtypes = []
+    L.dem_get_lateral_record.argtypes = [_vp, C.c_int32, _vp, _u32, P(_u32)]
     L.dem_ref_cells.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_cells_static.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_neighbor_sets.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, C.c_float, C.c_float, _u32, _vp,
@@ -317,6 +323,14 @@ class Context:
         _ck(_lib().dem_sample_result(self._h, sample, C.byref(r)), "dem_sample_result")
         return r.as_dict()
 
+    def lateral_record(self, sample: int = 0) -> np.ndarray:
+        """Mean radial distance of the lateral surface particles per record entry."""
+        n = C.c_uint32()
+        _ck(_lib().dem_get_lateral_record(self._h, sample, None, 0, C.byref(n)), "dem_get_lateral_record")
+        out = np.zeros(max(n.value, 1), np.float64)
+        _ck(_lib().dem_get_lateral_record(self._h, sample, _p(out), n.value, C.byref(n)), "dem_get_lateral_record")
+        return out[:n.value]
+
     def record(self, sample: int = 0):
         n = C.c_uint32()
         _ck(_lib().dem_get_record(self._h, sample, None, None, 0, C.byref(n)), "dem_get_record")
@@ -428,11 +442,12 @@ def calculation_test(mat: Material, load: Loading, xyz: np.ndarray, radii=None, 
 def create_cylinder_sample(center, radius: float, half_height: float, n: int, r_min: float, r_max: float,
                            E: float = 50.0, nu: float = 0.25, rho: float = 2.65, overlap_tol: float = 1e-3,
                            growth_stages: int = 40, steps_per_stage: int = 200, max_fire_steps: int = 20000,
-                           seed: int = 1, device: int = 0):
-    """Seeded packed cylinder (h_CreateCylinderSample): returns xyz (SoA), radii, report."""
+                           seed: int = 1, device: int = 0, fire_variant: int = 0):
+    """Seeded packed cylinder (h_CreateCylinderSample): returns xyz (SoA), radii, report.
+    fire_variant 0 relaxes with inertial FIRE 2.0, 1 with the reference's FIRE update."""
     p = PackParams(radius=radius, half_height=half_height, r_min=r_min, r_max=r_max, E=E, nu=nu, rho=rho,
                    overlap_tol=overlap_tol, n=n, growth_stages=growth_stages, steps_per_stage=steps_per_stage,
-                   max_fire_steps=max_fire_steps, seed=seed, device=device)
+                   max_fire_steps=max_fire_steps, seed=seed, device=device, fire_variant=fire_variant)
     for d in range(3):
         p.center[d] = float(center[d])
     xyz = np.zeros(3 * n, np.float32)

@@ -42,6 +42,8 @@ const char* dem_strerror(int code) {
   }
 }
 
+const char* dem_last_error_detail(void) { return dem::last_error_detail(); }
+
 int dem_device_count(int* n) {
   int c = 0;
   if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;
@@ -96,6 +98,9 @@ int dem_counts(dem_ctx* ctx, uint32_t* p, uint32_t* b, uint32_t* c, uint32_t* s)
 int dem_sample_result(dem_ctx* ctx, int32_t sample, dem_result* out) { CTX_CALL(ctx->e->result(sample, out)); }
 int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n) {
   CTX_CALL(ctx->e->get_record(sample, rec, bonds, cap, n));
+}
+int dem_get_lateral_record(dem_ctx* ctx, int32_t sample, double* lat, uint32_t cap, uint32_t* n) {
+  CTX_CALL(ctx->e->get_lateral_record(sample, lat, cap, n));
 }
 int dem_get_particles(dem_ctx* ctx, int32_t s, float* R, float* V, float* W, float* F, float* M, float* O) {
   CTX_CALL(ctx->e->get_particles(s, R, V, W, F, M, O));

@@ -69,6 +69,20 @@ __device__ __forceinline__ double4 ld4(const double4* p) {
 }
 __device__ __forceinline__ float4 ld4_rw(const float4* p) { return *p; }
 __device__ __forceinline__ double4 ld4_rw(const double4* p) { return *p; }
+// Streamed pair state (read once and written once per step): evict-first, so
+// the particle arrays that every pair gathers stay in L2.
+__device__ __forceinline__ float4 ld4_cs(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ double4 ld4_cs(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldcs(q), b = __ldcs(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st4_cs(float4* p, const float4& v) { __stcs(p, v); }
+__device__ __forceinline__ void st4_cs(double4* p, const double4& v) {
+  double2* q = reinterpret_cast<double2*>(p);
+  __stcs(q, make_double2(v.x, v.y));
+  __stcs(q + 1, make_double2(v.z, v.w));
+}
 
 __device__ __forceinline__ float4 mk4(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
 __device__ __forceinline__ double4 mk4(double a, double b, double c, double d) { return make_double4(a, b, c, d); }

@@ -19,11 +19,24 @@
 
 namespace dem {
 
+namespace {
+thread_local char g_detail[192] = "";
+}  // namespace
+
+void note_cuda_error(cudaError_t e, const char* file, int line) {
+  const char* base = std::strrchr(file, '/');
+  std::snprintf(g_detail, sizeof g_detail, "%s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e),
+                base ? base + 1 : file, line);
+}
+
+const char* last_error_detail() { return g_detail; }
+
 #define CK(x)                                  \
   do {                                         \
     cudaError_t e_ = (x);                      \
     if (e_ != cudaSuccess) {                   \
       last_cuda_ = e_;                         \
+      note_cuda_error(e_, __FILE__, __LINE__); \
       return DEM_ERR_CUDA;                     \
     }                                          \
   } while (0)
@@ -91,6 +104,7 @@ struct SampleHost {
   double dt = 0;
   double E_b = 0, G_b = 0, hm_E = 0, hm_G = 0;
   int32_t bonds_initial = 0;
+  uint32_t lat_count = 0;   // lateral surface particles (uniaxial specimens)
 };
 
 template <class Real>
@@ -188,6 +202,7 @@ class Engine final : public EngineBase {
     CK(mass_.upload(hmass.data(), np_));
     CK(sid_.upload(hsid.data(), np_));
     CK(orig_.upload(horig.data(), np_));
+    RC(mark_lateral());
     // per-sample constants and controllers
     RC(upload_params());
     // contact grids
@@ -208,6 +223,37 @@ class Engine final : public EngineBase {
     }
     CK(cudaDeviceSynchronize());
     setup_done_ = true;
+    return DEM_OK;
+  }
+
+  // Uniaxial specimens: mark the particles of the lateral surface near
+  // mid-height (outer shell one mean diameter thick, |z - z_c| <= H/4), whose
+  // mean radial distance gives the lateral strain for the Poisson ratio.
+  int mark_lateral() {
+    std::vector<uint8_t> h(np_, 0);
+    bool any = false;
+    for (auto& s : samples_) {
+      s.lat_count = 0;
+      const dem_loading& L = s.load;
+      if (L.test != DEM_TEST_UNIAXIAL) continue;
+      const double cx = L.center_real[0], cy = L.center_real[1], cz = L.center_real[2];
+      const double hz = 0.25 * L.size_real[2];
+      double outer = 0;
+      for (uint32_t q = 0; q < s.n; ++q)
+        outer = std::max(outer, std::hypot(s.xyz[q] - cx, s.xyz[s.n + q] - cy) + s.rad[q]);
+      for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t q = s.perm[k];
+        const double rho = std::hypot(s.xyz[q] - cx, s.xyz[s.n + q] - cy);
+        if (rho + s.rad[q] >= outer - 2.0 * s.rmean && std::fabs(s.xyz[2 * s.n + q] - cz) <= hz) {
+          h[s.p_begin + k] = 1;
+          ++s.lat_count;
+        }
+      }
+      any = any || s.lat_count > 0;
+    }
+    if (!any) return DEM_OK;
+    CK(lat_.alloc(np_));
+    CK(lat_.upload(h.data(), np_));
     return DEM_OK;
   }
 
@@ -563,6 +609,7 @@ class Engine final : public EngineBase {
     std::vector<SampleCtl> hc(S);
     rec_.resize(S);
     rec_bonds_.resize(S);
+    rec_lat_.resize(S);
     for (uint32_t si = 0; si < S; ++si) {
       const SampleHost& s = samples_[si];
       const dem_loading& L = s.load;
@@ -608,6 +655,8 @@ class Engine final : public EngineBase {
       RC(alloc_rec(si, C.Nsave));
       C.rec = rec_[si]->p;
       C.rec_bonds = rec_bonds_[si]->p;
+      C.rec_lat = rec_lat_[si]->p;
+      C.lat_count = s.lat_count;
     }
     CK(ctl_.alloc(S));
     CK(ctl_.upload(hc.data(), S));
@@ -617,8 +666,10 @@ class Engine final : public EngineBase {
   int alloc_rec(uint32_t si, uint32_t nsave) {
     rec_[si].reset(new DBuf<double>());
     rec_bonds_[si].reset(new DBuf<uint32_t>());
+    rec_lat_[si].reset(new DBuf<double>());
     CK(rec_[si]->alloc(3 * ((size_t)nsave + 2)));
     CK(rec_bonds_[si]->alloc((size_t)nsave + 2));
+    CK(rec_lat_[si]->alloc((size_t)nsave + 2));
     return DEM_OK;
   }
 
@@ -652,6 +703,7 @@ class Engine final : public EngineBase {
     A.touching = nullptr;
     A.blk_stat = blk_stat_.p;
     A.stat = stat_.p;
+    A.lat = lat_.p;
     return A;
   }
 
@@ -840,7 +892,49 @@ class Engine final : public EngineBase {
     if (ns > 0 && rb.size() >= ns && rb[0] > 0) out->Destruction = rb[ns - 1] / (double)rb[0];
     if (!C.brazil && ns > 0 && C.FractureStrain != 0 && C.FractureStress != 0)
       out->LinearityDeviation = linearity_deviation(rec, ns, C.FractureStress, C.FractureStrain);
+    std::vector<double> lat;
+    if (C.lat_count) {
+      lat.resize(rec_lat_[si]->n);
+      CK(rec_lat_[si]->download(lat.data(), lat.size()));
+    }
+    chord_moduli(rec, lat, ns, out);
     return DEM_OK;
+  }
+
+  // Young's modulus as the chord slope of stress over axial strain between 10%
+  // and 50% of the peak stress on the rising branch of the record, and the
+  // Poisson ratio as lateral over axial strain increment between the same two
+  // points (lateral strain from the mean radial distance of the marked
+  // surface particles).  The reference computes neither.
+  static void chord_moduli(const std::vector<double>& rec, const std::vector<double>& lat, uint32_t ns,
+                           dem_result* out) {
+    out->E_chord = std::nan("");
+    out->nu = std::nan("");
+    if (ns < 3) return;
+    auto sig = [&](uint32_t k) { return 0.5 * (std::fabs(rec[3 * k + 1]) + std::fabs(rec[3 * k + 2])); };
+    auto eps = [&](uint32_t k) { return -rec[3 * k]; };
+    uint32_t kp = 0;
+    for (uint32_t k = 1; k < ns; ++k)
+      if (sig(k) > sig(kp)) kp = k;
+    const double sp = sig(kp);
+    if (!(sp > 0)) return;
+    // first crossing of level*sp at or before the peak, linearly interpolated
+    auto cross = [&](double level, double& e, double& l) -> bool {
+      const double t = level * sp;
+      for (uint32_t k = 1; k <= kp; ++k) {
+        if (sig(k) >= t && sig(k - 1) < t) {
+          const double w = (t - sig(k - 1)) / (sig(k) - sig(k - 1));
+          e = eps(k - 1) + w * (eps(k) - eps(k - 1));
+          l = lat.empty() ? 0.0 : lat[k - 1] + w * (lat[k] - lat[k - 1]);
+          return true;
+        }
+      }
+      return false;
+    };
+    double e1, l1, e5, l5;
+    if (!cross(0.1, e1, l1) || !cross(0.5, e5, l5) || !(e5 > e1)) return;
+    out->E_chord = 0.4 * sp / (e5 - e1);
+    if (!lat.empty() && lat[0] > 0) out->nu = ((l5 - l1) / lat[0]) / (e5 - e1);
   }
 
   // md_results.cu:147-166 (the record holds two extra zero entries so the
@@ -866,6 +960,18 @@ class Engine final : public EngineBase {
     rb.resize(rec_bonds_[si]->n);
     CK(rec_[si]->download(rec.data(), 3 * n));
     CK(rec_bonds_[si]->download(rb.data(), rb.size()));
+    return DEM_OK;
+  }
+
+  int get_lateral_record(int32_t si, double* out, uint32_t cap, uint32_t* n) override {
+    if (si < 0 || (size_t)si >= samples_.size()) return DEM_ERR_ARG;
+    if (!setup_done_) return DEM_ERR_STATE;
+    SampleCtl C;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&C, ctl_.p + si, sizeof(C), cudaMemcpyDeviceToHost));
+    const uint32_t m = std::min<uint32_t>(C.stepsave, cap);
+    if (out && m) CK(cudaMemcpy(out, rec_lat_[si]->p, m * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n) *n = C.lat_count ? C.stepsave : 0;
     return DEM_OK;
   }
 
@@ -1199,6 +1305,8 @@ class Engine final : public EngineBase {
   DBuf<float> blk_stat_, stat_;
   std::vector<std::unique_ptr<DBuf<double>>> rec_;
   std::vector<std::unique_ptr<DBuf<uint32_t>>> rec_bonds_;
+  std::vector<std::unique_ptr<DBuf<double>>> rec_lat_;
+  DBuf<uint8_t> lat_;
 };
 
 EngineBase* make_engine(const dem_options& o, int* err) {

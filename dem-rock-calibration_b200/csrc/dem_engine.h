@@ -9,6 +9,12 @@
 
 namespace dem {
 
+// Thread-local text of the last CUDA error seen by the library (name, message,
+// source location), for dem_last_error_detail.
+void note_cuda_error(cudaError_t e, const char* file, int line);
+const char* last_error_detail();
+
+
 class EngineBase {
  public:
   virtual ~EngineBase() = default;
@@ -23,6 +29,7 @@ class EngineBase {
   virtual int counts(uint32_t* p, uint32_t* b, uint32_t* c, uint32_t* s) = 0;
   virtual int result(int32_t sample, dem_result* out) = 0;
   virtual int get_record(int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n) = 0;
+  virtual int get_lateral_record(int32_t sample, double* lat, uint32_t cap, uint32_t* n) = 0;
   virtual int get_particles(int32_t s, float* R, float* V, float* W, float* F, float* M, float* O) = 0;
   virtual int get_particles_d(int32_t s, double* R, double* V, double* W, double* F, double* M, double* O) = 0;
   virtual int set_particles(int32_t s, const float* R, const float* V, const float* W, const float* O) = 0;

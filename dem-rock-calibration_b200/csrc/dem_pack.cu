@@ -12,6 +12,7 @@
 
 #include "b200dem.h"
 #include "dem_build.cuh"
+#include "dem_engine.h"
 #include "dem_pack.cuh"
 #include "dem_params.h"
 
@@ -36,10 +37,13 @@ struct Buf {
   }
 };
 
-#define CKP(x)                      \
-  do {                              \
-    cudaError_t e_ = (x);           \
-    if (e_ != cudaSuccess) return DEM_ERR_CUDA; \
+#define CKP(x)                                 \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) {                   \
+      note_cuda_error(e_, __FILE__, __LINE__); \
+      return DEM_ERR_CUDA;                     \
+    }                                          \
   } while (0)
 
 uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
@@ -138,14 +142,23 @@ class Packer {
     FireCtl F{};
     F.dt0 = dt0;
     F.dt = dt0;
-    F.dtmax = 100.0 * dt0;   // SetFIREData, md_firerelaxation.cu:74-86
-    F.dtmin = 0.001 * dt0;
     F.dtgrow = 1.1;
     F.dtshrink = 0.5;
-    F.alpha0 = 0.1;
-    F.alpha = 0.1;
     F.alphashrink = 0.99;
     F.Ndelay = 20;
+    F.variant = P.fire_variant == 1 ? 1u : 0u;
+    if (F.variant == 1) {
+      F.dtmax = 100.0 * dt0;  // SetFIREData, md_firerelaxation.cu:74-86
+      F.dtmin = 0.001 * dt0;
+      F.alpha0 = 0.1;
+    } else {
+      // FIRE 2.0 defaults scaled to this time step: dt0 is about a tenth of the
+      // stability limit of the stiffest particle, so dt stays within 4 dt0
+      F.dtmax = 4.0 * dt0;
+      F.dtmin = 0.02 * dt0;
+      F.alpha0 = 0.25;
+    }
+    F.alpha = F.alpha0;
     CKP(cudaMemcpy(fire.p, &F, sizeof(F), cudaMemcpyHostToDevice));
     // radius growth: from the scale whose packing fraction is 30% of the final
     // one to 1, with damped relaxation after every increment
@@ -251,13 +264,18 @@ class Packer {
     return DEM_OK;
   }
 
-  // relaxation loop: chunks of steps between contact-list rebuilds
+  // Relaxation loop.  The pair list holds every pair within r_i + r_j + skin
+  // of the final radii; it is rebuilt when a particle has moved more than a
+  // quarter of the skin since the last build.  Chunks of steps between host
+  // checks are sized so that the fastest particle of the previous chunk cannot
+  // use up the rest of that quarter.
   int relax(bool viscous, float vis, uint32_t max_steps, double tol, uint64_t& steps) {
     const uint32_t n = P.n;
     PackArgs<float> A{};
     A.pos = pos.p;
     A.vel = vel.p;
     A.frc = frc.p;
+    A.ref = ref.p;
     A.sid = sid.p;
     A.np = n;
     A.nc = nc_dev.p;
@@ -271,31 +289,51 @@ class Packer {
     A.viscous = viscous ? 1 : 0;
     A.vis = vis;
     const uint32_t gp = nsm * 8, gn = std::max(1u, std::min(cdiv(n, 256), nsm * 8));
-    // largest displacement allowed between rebuilds: a quarter of the skin
-    // per chunk of kChunk steps is bounded by rebuilding every chunk
-    const uint32_t kChunk = 10;
+    const double quarter = 0.25 * skin;
+    const uint32_t kMaxChunk = 50;
     uint32_t done = 0;
+    bool need_build = true;
+    FireCtl F{};
+    CKP(cudaMemcpyAsync(&F, fire.p, sizeof F, cudaMemcpyDeviceToHost, st));
+    CKP(cudaStreamSynchronize(st));
+    double vmax = 0.0, dmax = 0.0;
     while (done < max_steps) {
-      int rc = rebuild();
-      if (rc) return rc;
+      if (need_build || dmax > quarter) {
+        int rc = rebuild();
+        if (rc) return rc;
+        dmax = 0.0;
+        need_build = false;
+      }
       A.c_ij = cij.p;
-      float z = 0.f;
-      CKP(cudaMemcpyAsync(&fire.p->max_overlap, &z, sizeof(float), cudaMemcpyHostToDevice, st));
-      const uint32_t m = std::min(kChunk, max_steps - done);
+      const double dt_bound = viscous ? F.dt0 : F.dtmax;
+      uint32_t m = kMaxChunk;
+      if (vmax > 0.0) {
+        const double k = 0.5 * (quarter - dmax) / (vmax * dt_bound);
+        m = (uint32_t)std::max(1.0, std::min((double)kMaxChunk, std::floor(k)));
+      } else {
+        m = std::min<uint32_t>(10, kMaxChunk);
+      }
+      m = std::min(m, max_steps - done);
+      const float z = 0.f;
+      CKP(cudaMemcpyAsync(&fire.p->vmax2, &z, sizeof(float), cudaMemcpyHostToDevice, st));
       for (uint32_t k = 0; k < m; ++k) {
-        if (k == m - 1) CKP(cudaMemcpyAsync(&fire.p->max_overlap, &z, sizeof(float), cudaMemcpyHostToDevice, st));
+        if (k == m - 1) {
+          CKP(cudaMemcpyAsync(&fire.p->max_overlap, &z, sizeof(float), cudaMemcpyHostToDevice, st));
+          CKP(cudaMemcpyAsync(&fire.p->dmax2, &z, sizeof(float), cudaMemcpyHostToDevice, st));
+        }
         k_soft_pairs<float><<<gp, 256, 0, st>>>(A);
         if (!viscous) k_fire_power<float><<<gn, 256, 0, st>>>(A);
         k_fire_move<float><<<gn, 256, 0, st>>>(A);
       }
       CKP(cudaGetLastError());
-      float ov = 0.f;
-      CKP(cudaMemcpyAsync(&ov, &fire.p->max_overlap, sizeof(float), cudaMemcpyDeviceToHost, st));
+      CKP(cudaMemcpyAsync(&F, fire.p, sizeof F, cudaMemcpyDeviceToHost, st));
       CKP(cudaStreamSynchronize(st));
-      last_overlap = ov;
+      last_overlap = F.max_overlap;
+      vmax = std::sqrt((double)F.vmax2);
+      dmax = std::sqrt((double)F.dmax2);
       done += m;
       steps += m;
-      if (tol > 0 && ov < tol) break;
+      if (tol > 0 && F.max_overlap < tol) break;
     }
     return DEM_OK;
   }

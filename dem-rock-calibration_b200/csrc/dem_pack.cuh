@@ -5,13 +5,18 @@
 //   k_soft_pairs      pair force of d_CalculateForces (md_calculateforces.cu:20-67):
 //                     F_i += -D (a^2/r^2) (x_j - x_i) for r < a, a = s (r_i + r_j),
 //                     or a linear overlap spring (packing by radius growth)
-//   k_fire_power      P = sum F.v per sample (d_FdotVEntire, md_firerelaxation.cu:375-494);
-//                     the last block adapts dt and alpha on the device (the host
-//                     logic of md_createcylindersample.cu:368-397)
-//   k_fire_move       half step back on P <= 0 (d_CalculateDecrementsHalfStepFIRE),
-//                     FIRE velocity mix and move (d_CalculateIncrementsFIRE,
-//                     md_firerelaxation.cu:18-70), cylinder confinement
-//                     (d_CylinderRestrictionZ, md_cylinderrestriction.cu:190-234)
+//   k_fire_power      P = F.v, |v|^2, |F|^2 per sample, reduced per block
+//                     (d_FdotVEntire, md_firerelaxation.cu:375-494); the last block
+//                     adapts dt and alpha on the device (the host logic of
+//                     md_createcylindersample.cu:368-397)
+//   k_fire_move       one FIRE move and the cylinder confinement
+//                     (d_CylinderRestrictionZ, md_cylinderrestriction.cu:190-234).
+//                     Variant 0 is inertial FIRE 2.0 (Guenole et al., Comput. Mater.
+//                     Sci. 175 (2020) 109584: half step back and v = 0 on P <= 0,
+//                     semi-implicit Euler, velocity mixing); variant 1 is the
+//                     reference's update (d_CalculateDecrementsHalfStepFIRE +
+//                     d_CalculateIncrementsFIRE, md_firerelaxation.cu:18-70), which
+//                     rebuilds v from the current force alone each step.
 #pragma once
 
 #include "dem_common.cuh"
@@ -24,8 +29,11 @@ struct FireCtl {
   double dt0, dtmax, dtmin, dtgrow, dtshrink, alpha0, alphashrink;
   uint32_t Npos, Nneg, Ndelay, back;  // back: this step moves half a step back and zeroes v
   unsigned long long step;
+  double vv, ff;       // |v|^2 and |F|^2 of the current step (accumulated)
   float max_overlap;   // largest relative overlap seen by the pair kernel this step
-  float pad;
+  float vmax2;         // largest |v|^2 after a move (since the host reset it)
+  float dmax2;         // largest squared displacement since the last list build (last move)
+  uint32_t variant;    // 0: inertial FIRE 2.0, 1: the reference's force-only update
 };
 
 template <class Real>
@@ -34,6 +42,7 @@ struct PackArgs {
   V4* pos;        // x, y, z, target radius
   V4* vel;        // v, dt0/m (reference Po.dt_d_m)
   V4* frc;
+  const V4* ref;  // positions at the last list build
   const uint32_t* sid;
   uint32_t np;
   const uint2* c_ij;
@@ -84,51 +93,85 @@ __global__ void __launch_bounds__(256) k_soft_pairs(PackArgs<Real> A) {
     atomicMax(reinterpret_cast<int*>(&A.fire[0].max_overlap), __float_as_int(worst));
 }
 
+// Block sum of three doubles (256 threads); result valid in thread 0.
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c) {
+  __shared__ double sh[3][8];
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+    b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+    c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sh[0][w] = a;
+    sh[1][w] = b;
+    sh[2][w] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = c = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += sh[0][k];
+      b += sh[1][k];
+      c += sh[2][k];
+    }
+  }
+}
+
+// One sample (the packer relaxes one specimen per call).
 template <class Real>
 __global__ void __launch_bounds__(256) k_fire_power(PackArgs<Real> A) {
   using V4 = typename RT<Real>::V4;
   __shared__ int s_last;
+  double pw = 0.0, vv = 0.0, ff = 0.0;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     const V4 f = A.frc[p], v = A.vel[p];
-    const double pw = (double)((f.x * v.x + f.y * v.y) + f.z * v.z);
-    if (pw != 0.0) atomicAdd(&A.fire[A.sid[p]].P, pw);
+    pw += (double)((f.x * v.x + f.y * v.y) + f.z * v.z);
+    vv += (double)((v.x * v.x + v.y * v.y) + v.z * v.z);
+    ff += (double)((f.x * f.x + f.y * f.y) + f.z * f.z);
   }
-  __threadfence();
+  block_sum3(pw, vv, ff);
+  FireCtl& F = A.fire[0];
+  if (threadIdx.x == 0) {
+    if (pw != 0.0) atomicAdd(&F.P, pw);
+    if (vv != 0.0) atomicAdd(&F.vv, vv);
+    if (ff != 0.0) atomicAdd(&F.ff, ff);
+    __threadfence();
+    s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
+  }
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
+  if (!s_last || threadIdx.x != 0) return;
   __threadfence();
-  for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
-    FireCtl& F = A.fire[s];
-    // md_createcylindersample.cu:374-397
-    if (F.P > 0) {
-      ++F.Npos;
-      F.Nneg = 0;
-      if (F.Npos > F.Ndelay) {
-        F.dt = (F.dt * F.dtgrow < F.dtmax) ? F.dt * F.dtgrow : F.dtmax;
-        F.alpha *= F.alphashrink;
-      }
-      F.back = 0;
-    } else {
-      F.Npos = 0;
-      ++F.Nneg;
-      if (F.step > F.Ndelay) {
-        F.dt = (F.dt * F.dtshrink > F.dtmin) ? F.dt * F.dtshrink : F.dtmin;
-        F.alpha = F.alpha0;
-      }
-      F.back = 1;
+  // md_createcylindersample.cu:374-397 (the same adaptation drives FIRE 2.0)
+  if (F.P > 0) {
+    ++F.Npos;
+    F.Nneg = 0;
+    if (F.Npos > F.Ndelay) {
+      F.dt = (F.dt * F.dtgrow < F.dtmax) ? F.dt * F.dtgrow : F.dtmax;
+      F.alpha *= F.alphashrink;
     }
-    F.P = 0.0;
-    ++F.step;
+    F.back = 0;
+  } else {
+    F.Npos = 0;
+    ++F.Nneg;
+    if (F.step > F.Ndelay) {
+      F.dt = (F.dt * F.dtshrink > F.dtmin) ? F.dt * F.dtshrink : F.dtmin;
+      F.alpha = F.alpha0;
+    }
+    F.back = 1;
   }
-  if (threadIdx.x == 0) *A.blocks_done = 0;
+  F.P = 0.0;
+  F.vv = 0.0;
+  F.ff = 0.0;
+  ++F.step;
+  *A.blocks_done = 0;
 }
 
 template <class Real>
 __global__ void __launch_bounds__(256) k_fire_move(PackArgs<Real> A) {
   using T = RT<Real>;
   using V4 = typename T::V4;
+  float my_v2 = 0.f, my_d2 = 0.f;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     const uint32_t s = A.sid[p];
     V4 x = A.pos[p], v = A.vel[p], f = A.frc[p];
@@ -142,7 +185,7 @@ __global__ void __launch_bounds__(256) k_fire_move(PackArgs<Real> A) {
       x.x += v.x * dt;
       x.y += v.y * dt;
       x.z += v.z * dt;
-    } else {
+    } else if (A.fire[s].variant == 1) {
       const FireCtl& F = A.fire[s];
       const Real dt = (Real)F.dt, alpha = (Real)F.alpha;
       if (F.back) {
@@ -169,6 +212,33 @@ __global__ void __launch_bounds__(256) k_fire_move(PackArgs<Real> A) {
       x.x += vx * dt;
       x.y += vy * dt;
       x.z += vz * dt;
+    } else {
+      // FIRE 2.0: on P <= 0 half a step back and v = 0; then v += dt F/m,
+      // v = (1 - alpha) v + alpha |v| F/|F| (per particle), x += dt v
+      const FireCtl& F = A.fire[s];
+      const Real dt = (Real)F.dt, alpha = (Real)F.alpha;
+      if (F.back) {
+        const Real h = Real(0.5) * dt;
+        x.x -= v.x * h;
+        x.y -= v.y * h;
+        x.z -= v.z * h;
+        v.x = v.y = v.z = Real(0);
+      }
+      const Real k = dtm * (Real)(F.dt / F.dt0);  // dt / m
+      v.x += f.x * k;
+      v.y += f.y * k;
+      v.z += f.z * k;
+      const Real ff = (f.x * f.x + f.y * f.y) + f.z * f.z;
+      if (ff > Real(0)) {
+        const Real vn = T::sqrt_rn((v.x * v.x + v.y * v.y) + v.z * v.z);
+        const Real c = alpha * vn * T::rsqrt_rn(ff);
+        v.x = (Real(1) - alpha) * v.x + c * f.x;
+        v.y = (Real(1) - alpha) * v.y + c * f.y;
+        v.z = (Real(1) - alpha) * v.z + c * f.z;
+      }
+      x.x += v.x * dt;
+      x.y += v.y * dt;
+      x.z += v.z * dt;
     }
     // cylinder confinement of the particle centre (radius R - r_i, half height H - r_i)
     const Real* c = A.cyl + 5 * s;
@@ -193,6 +263,19 @@ __global__ void __launch_bounds__(256) k_fire_move(PackArgs<Real> A) {
     A.pos[p] = x;
     A.vel[p] = v;
     A.frc[p] = mk4(Real(0), Real(0), Real(0), Real(0));
+    const V4 r0 = A.ref[p];
+    const Real ex = x.x - r0.x, ey = x.y - r0.y, ez = x.z - r0.z;
+    my_v2 = fmaxf(my_v2, (float)((v.x * v.x + v.y * v.y) + v.z * v.z));
+    my_d2 = fmaxf(my_d2, (float)((ex * ex + ey * ey) + ez * ez));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    my_v2 = fmaxf(my_v2, __shfl_xor_sync(0xFFFFFFFFu, my_v2, o));
+    my_d2 = fmaxf(my_d2, __shfl_xor_sync(0xFFFFFFFFu, my_d2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    // non-negative floats order as their bit patterns
+    if (my_v2 > 0.f) atomicMax(reinterpret_cast<int*>(&A.fire[0].vmax2), __float_as_int(my_v2));
+    if (my_d2 > 0.f) atomicMax(reinterpret_cast<int*>(&A.fire[0].dmax2), __float_as_int(my_d2));
   }
 }
 

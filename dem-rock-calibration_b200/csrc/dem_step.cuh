@@ -54,6 +54,7 @@ struct StepArgs {
   unsigned long long* touching;  // non-null: count touching contacts (algorithmic-byte accounting)
   float* blk_stat;  // per block: max |v|^2 and max displacement^2 since the last list build
   float* stat;      // running maxima over blocks and steps (reset by the host)
+  const uint8_t* lat;  // per particle: 1 = on the lateral surface near mid-height (or null)
 };
 
 // Hertz-Mindlin contact of pair (i, j) seen from i (n points from i to j), in
@@ -172,13 +173,18 @@ template <class Real>
 __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
   using T = RT<Real>;
   using V4 = typename T::V4;
-  const uint2 ij = A.b_ij[b];
+  // every load is issued before the first branch: the bond's own state, then
+  // the gathers that depend only on (i, j)
+  const uint2 ij = __ldcs(A.b_ij + b);
+  V4 par = ld4_cs(A.b_par + b);
+  V4 s0 = ld4_cs(A.b_s0 + b), s1 = ld4_cs(A.b_s1 + b), s2 = ld4_cs(A.b_s2 + b);
   const uint32_t i = ij.x, j = ij.y;
+  const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
+  const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
+  const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
   const uint32_t s = A.sid[i];
   if (A.ctl[s].done) return;
   const SampleParams<Real>& sp = A.sp[s];
-  V4 par = ld4_rw(A.b_par + b);
-  const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
   const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
   const Real rr = (rx * rx + ry * ry) + rz * rz;
   bool intact = par.x > Real(0);
@@ -186,17 +192,14 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
     // d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:169-181): the slot is
     // emptied with all histories; the pair later interacts only by contact.
     par.x = -par.x;
-    A.b_par[b] = par;
+    st4_cs(A.b_par + b, par);
     const Real z = Real(0);
-    A.b_s0[b] = mk4(z, z, z, z);
-    A.b_s1[b] = mk4(z, z, z, z);
-    A.b_s2[b] = mk4(z, z, z, z);
+    st4_cs(A.b_s0 + b, mk4(z, z, z, z));
+    st4_cs(A.b_s1 + b, mk4(z, z, z, z));
+    st4_cs(A.b_s2 + b, mk4(z, z, z, z));
     atomicSub(&A.ctl[s].bonds, 1);
     return;
   }
-  const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
-  const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
-  V4 s0 = ld4_rw(A.b_s0 + b), s1 = ld4_rw(A.b_s1 + b), s2 = ld4_rw(A.b_s2 + b);
   const Real rijm = norm3(rx, ry, rz);
   Real ox = s0.w, oy = s1.x, oz = s1.y;
   if (intact) {
@@ -276,15 +279,15 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
       s0.w = ot0;
       s1 = mk4(ot1, ot2, mn0, mn1);
       s2 = mk4(mn2, mt0, mt1, mt2);
-      A.b_s0[b] = s0;
-      A.b_s1[b] = s1;
-      A.b_s2[b] = s2;
+      st4_cs(A.b_s0 + b, s0);
+      st4_cs(A.b_s1 + b, s1);
+      st4_cs(A.b_s2 + b, s2);
       return;
     }
     // broken: histories cleared; the pair is a contact from now on and, as in the
     // reference (DEM_21 runs after DEM_22 in the same step), already this step.
     par.x = -par.x;
-    A.b_par[b] = par;
+    st4_cs(A.b_par + b, par);
     atomicSub(&A.ctl[s].bonds, 1);
     ox = oy = oz = Real(0);
     const Real z = Real(0);
@@ -306,9 +309,9 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
   s0.w = ox;
   s1.x = oy;
   s1.y = oz;
-  A.b_s0[b] = s0;
-  A.b_s1[b] = s1;
-  if (intact) A.b_s2[b] = s2;
+  st4_cs(A.b_s0 + b, s0);
+  st4_cs(A.b_s1 + b, s1);
+  if (intact) st4_cs(A.b_s2 + b, s2);
 }
 
 // One unbonded contact-list pair (i < j).  Bit 31 of j flags a non-zero
@@ -350,7 +353,7 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
 }
 
 template <class Real>
-__global__ void __launch_bounds__(256) k_pairs(StepArgs<Real> A) {
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2) k_pairs(StepArgs<Real> A) {
   const uint32_t nb = A.nb;
   const uint32_t total = nb + *A.nc;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
@@ -453,6 +456,7 @@ __device__ inline void controller_step(SampleCtl& C) {
     C.rec[3 * C.stepsave] = (C.size_d[ax] - C.sz0) / C.sz0;
     C.rec[3 * C.stepsave + 1] = sF0 * C.inv_Area;
     C.rec[3 * C.stepsave + 2] = sF1 * C.inv_Area;
+    if (C.rec_lat) C.rec_lat[C.stepsave] = C.lat_count ? C.lat_sum / C.lat_count : 0.0;
     if (fabs(C.V) > 1e-9) ++C.stepsave;
   }
   C.Stress = 0.5 * (fabs(sF0) + fabs(sF1)) * C.inv_Area;
@@ -489,6 +493,7 @@ __device__ inline void controller_step(SampleCtl& C) {
   C.Strain = (C.size_d[ax] - C.Size0) / C.Size0;
   C.sFL[0] = 0.0;
   C.sFL[1] = 0.0;
+  C.lat_sum = 0.0;
   ++C.step;
   // loop condition of h_Calculation{UniaxialCompression,BrazilTest}
   if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps) C.done = 1;
@@ -505,7 +510,7 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
-    double sb = 0.0, st = 0.0;
+    double sb = 0.0, st = 0.0, sl = 0.0;
     if (!C.done) {
       const SampleParams<Real>& sp = A.sp[s];
       V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
@@ -578,6 +583,11 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       // neighbour-list validity: displacement since the last build.  A parked
       // particle interacts with nothing (all parked particles coincide, and
       // pairs closer than 1e-10 are ignored), so it restarts its reference.
+      // lateral surface particles on record steps: radial distance from the axis
+      if (A.lat && A.lat[p] && !parked && C.dNsave && C.step % C.dNsave == 0) {
+        const double ex = (double)x.x - sp.wall_c[0], ey = (double)x.y - sp.wall_c[1];
+        sl = sqrt(ex * ex + ey * ey);
+      }
       if (parked) {
         A.pos_ref[p] = x;
       } else {
@@ -602,14 +612,21 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       for (int off = 16; off > 0; off >>= 1) {
         sb += __shfl_xor_sync(full, sb, off);
         st += __shfl_xor_sync(full, st, off);
+        sl += __shfl_xor_sync(full, sl, off);
       }
-      if ((threadIdx.x & 31) == 0 && (sb != 0.0 || st != 0.0)) {
+      if ((threadIdx.x & 31) == 0) {
+        if (sb != 0.0 || st != 0.0) {
+          atomicAdd(&A.ctl[s].sFL[0], sb);
+          atomicAdd(&A.ctl[s].sFL[1], st);
+        }
+        if (sl != 0.0) atomicAdd(&A.ctl[s].lat_sum, sl);
+      }
+    } else {
+      if (sb != 0.0 || st != 0.0) {
         atomicAdd(&A.ctl[s].sFL[0], sb);
         atomicAdd(&A.ctl[s].sFL[1], st);
       }
-    } else if (sb != 0.0 || st != 0.0) {
-      atomicAdd(&A.ctl[s].sFL[0], sb);
-      atomicAdd(&A.ctl[s].sFL[1], st);
+      if (sl != 0.0) atomicAdd(&A.ctl[s].lat_sum, sl);
     }
   }
   // block maxima of speed and displacement (the host sizes the next chunk of

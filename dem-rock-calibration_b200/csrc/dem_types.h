@@ -61,6 +61,12 @@ struct SampleCtl {
   uint32_t stale;           // a particle moved more than the skin allows: list was stale
   double* rec;              // 3*Nsave: strain, sigma_bottom, sigma_top (reference h_sFL)
   uint32_t* rec_bonds;      // Nsave: bonded directed slots (reference h_sSI)
+  // lateral surface of a uniaxial specimen (Poisson ratio): sum of the radial
+  // distances of the marked particles on record steps, and its record
+  double lat_sum;
+  double* rec_lat;          // Nsave: mean radial distance of the marked particles
+  uint32_t lat_count;       // marked particles (0: no lateral record)
+  uint32_t lat_pad;
 };
 
 }  // namespace dem

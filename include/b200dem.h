@@ -125,12 +125,20 @@ typedef struct {
   uint32_t stepsave;         /* number of records */
   uint32_t bonds_initial, bonds_now;  /* intact undirected bonds */
   int fracture, done, stale;
+  int reserved;
+  /* extensions (the reference outputs neither): chord Young modulus (GPa)
+   * between 10% and 50% of the peak stress, and the Poisson ratio over the
+   * same interval from the lateral record; NaN when undefined */
+  double E_chord, nu;
 } dem_result;
 
 /* --- context and specimens --- */
 int dem_create(const dem_options* opt, dem_ctx** out);
 void dem_destroy(dem_ctx* ctx);
 const char* dem_strerror(int code);
+/* Text of the last CUDA error the library saw on this host thread (error name,
+ * message, source location), "" if none; kept until the next CUDA error. */
+const char* dem_last_error_detail(void);
 int dem_device_count(int* n);
 
 /* Adds one specimen.  xyz: 3n floats (mm, SoA); radii: n floats or NULL
@@ -155,6 +163,10 @@ int dem_sample_result(dem_ctx* ctx, int32_t sample, dem_result* out);
 /* Loading record: 3 doubles per entry (strain, sigma_bottom, sigma_top in GPa)
  * and bonded directed-slot counts, as the reference's h_sFL / h_sSI. */
 int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n);
+/* Lateral record of a uniaxial specimen (no counterpart in the reference): per
+ * loading-record entry the mean radial distance (mm) of the particles on the
+ * lateral surface near mid-height; *n = 0 for specimens without one. */
+int dem_get_lateral_record(dem_ctx* ctx, int32_t sample, double* lat, uint32_t cap, uint32_t* n);
 
 /* Particle state in the caller's original order, SoA (3n each, NULL skips). */
 int dem_get_particles(dem_ctx* ctx, int32_t sample, float* R, float* V, float* W, float* F, float* M,
@@ -230,7 +242,9 @@ int dem_save_sum_forces_loading(const char* path, const double* rec, uint32_t n)
  * radii uniform in [r_min, r_max] filled at random into a z-axis cylinder
  * (a column for the uniaxial test, a disc for the Brazilian test), grown from
  * 30% of the final packing fraction with damped soft-sphere relaxation, then
- * FIRE-relaxed until the largest overlap / (r_i + r_j) is below overlap_tol. */
+ * FIRE-relaxed until the largest overlap / (r_i + r_j) is below overlap_tol.
+ * fire_variant 0: inertial FIRE 2.0; 1: the reference's FIRE update
+ * (md_firerelaxation.cu:18-70, velocity rebuilt from the force each step). */
 typedef struct {
   double center[3];          /* cylinder centre, mm */
   double radius;             /* cylinder radius, mm */
@@ -244,7 +258,7 @@ typedef struct {
   uint32_t max_fire_steps;   /* FIRE steps at the final radii */
   uint64_t seed;
   int device;
-  int reserved;
+  int fire_variant;
 } dem_pack_params;
 
 typedef struct {

@@ -54,16 +54,26 @@ def fcc_cylinder(center, radius: float, half_h: float, d: float, jitter: float, 
 
 def ref_case(seed: int = 1, lsi=(0.0045, 0.0045, 0.006), space=(0.009, 0.009, 0.012), p_r_si=0.25e-3,
              E=30e9, Ec=40e6, Gc=40e6, br_si=0.2e-3, gap_si=0.025e-3, jitter_frac=0.03, brazil=False,
-             velocity_si=-0.1, minstress_si=10e6, maxstrain=0.01, condfract=0.1, farcut=3.2) -> RefCase:
-    """A reference-mode specimen (equal radii, scalar micro-parameters)."""
+             velocity_si=-0.1, minstress_si=10e6, maxstrain=0.01, condfract=0.1, farcut=3.2,
+             lattice_gap=0.0) -> RefCase:
+    """A reference-mode specimen (equal radii, scalar micro-parameters).
+
+    lattice_gap > 0: nearest-neighbour spacing 2 p_r + lattice_gap * gap and the
+    jitter given in units of gap (jitter_frac * gap), so that no two spheres
+    overlap and every nearest pair is inside the bond distance."""
     pot = prm.initial_potential(E, Ec, Gc, br_si, gap_si, p_r_si=p_r_si, farcut=farcut)
     C_a = prm.F(2.0 * pot.a_farcut)
     smp = prm.sample_for(space, lsi, C_a, pot.p_r)
     cells = prm.cells_for(2.0 * pot.a_farcut, smp.B)
     rng = np.random.default_rng(seed)
-    d = 2.0 * pot.p_r
-    pts = fcc_cylinder(smp.center.astype(np.float64), 0.5 * float(smp.L[0]), 0.5 * float(smp.L[2]), d,
-                       jitter_frac * d, rng)
+    if lattice_gap > 0:
+        gap_mm = gap_si / prm.LENGTH
+        d = 2.0 * pot.p_r + lattice_gap * gap_mm
+        jitter = jitter_frac * gap_mm
+    else:
+        d = 2.0 * pot.p_r
+        jitter = jitter_frac * d
+    pts = fcc_cylinder(smp.center.astype(np.float64), 0.5 * float(smp.L[0]), 0.5 * float(smp.L[2]), d, jitter, rng)
     N = pts.shape[0]
     R = np.ascontiguousarray(pts.T.reshape(-1).astype(np.float32))
     size_real, center_real = prm.bounding_box(R, N, pot.p_r)
@@ -73,7 +83,7 @@ def ref_case(seed: int = 1, lsi=(0.0045, 0.0045, 0.006), space=(0.009, 0.009, 0.
     sc = sim.scalars_from(pot, cells, smp, cmp, velocity_si / prm.VELOCITY)
     kw = dict(seed=seed, p_r_si=p_r_si, E=E, Ec=Ec, Gc=Gc, br_si=br_si, gap_si=gap_si, brazil=brazil,
               velocity_si=velocity_si, minstress_si=minstress_si, maxstrain=maxstrain, condfract=condfract,
-              farcut=farcut)
+              farcut=farcut, lattice_gap=lattice_gap)
     return RefCase(pot=pot, cells=cells, smp=smp, cmp=cmp, sc=sc, R=R, N=N, lsi=lsi, space=space, kw=kw)
 
 

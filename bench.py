@@ -231,13 +231,80 @@ def run_reference(args, ws, rank, local):
     return 0
 
 
+def sweep_sizes(k: int, seed: int = 11) -> list[int]:
+    """k cylinder sizes, particle counts spread over [5k, 60k] (seeded, shuffled)."""
+    rng = np.random.default_rng(seed)
+    return [int(v) for v in rng.permutation(np.linspace(5000, 60000, k).round())]
+
+
+def run_sweep(args, ws, rank, local):
+    """Batched calibration sweep: `cases` Latin-hypercube parameter sets over 16
+    packed cylinders (5k-60k spheres) in one context, against the same cases
+    one context at a time.  Every rank runs its own sweep (weak scaling)."""
+    sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
+    D = Dist(ws)
+    sw = sweep.build_sweep(args.cases, sweep_sizes(16, 11 + rank), seed=1 + rank, device=local)
+    n = sw.particles
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks)
+    for c in sw.cases:
+        ctx.add_sample(c.material, c.loading, c.xyz, c.radii)
+    ctx.setup()
+    ctx.run_timed(args.warmup)
+    D.barrier()
+    clk = Clocks(local)
+    ms = ctx.run_timed(args.steps)
+    clocks = clk.stop()
+    D.barrier()
+    ms_max = D.max(ms)
+    value = D.sum(float(n)) * args.steps / (ms_max * 1e-3)
+    prof = ctx.profile(min(args.steps, 200))
+    res = [ctx.result(i) for i in range(len(sw.cases))]
+    ctx.close()
+    # the same cases one context at a time, a bounded sample of them
+    k_seq = min(len(sw.cases), 32)
+    sub = sweep.Sweep(cases=sw.cases[:k_seq])
+    seq = sweep.run_sequential(sub, args.steps, device=local)
+    n_sub = sub.particles
+    seq_rate = n_sub * args.steps / (seq["device_ms"] * 1e-3)
+    bonds = sum(r["bonds_now"] for r in res)
+    A = algorithmic_bytes(n, bonds, prof["touching"])
+    achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded packings, Latin-hypercube micro-parameters)",
+        "config": {"workload": f"calibration sweep: {len(sw.cases)} uniaxial cylinders (16 packings, "
+                               f"{min(c.n for c in sw.cases)}-{max(c.n for c in sw.cases)} spheres) in one context",
+                   "particles_per_gpu": n, "cases": len(sw.cases), "bonds": bonds,
+                   "sequential": {"cases": k_seq, "particles": n_sub, "value": seq_rate,
+                                  "device_ms": seq["device_ms"],
+                                  "note": "the same cases one context at a time (device time summed)"},
+                   "batched_over_sequential": value / D.sum(seq_rate),
+                   "l2": "inputs larger than L2, no flush"},
+        "gpu_launches": 2 * args.steps, "clocks": clocks,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_pairs", "pair_ms": prof["pair_ms"],
+                     "particle_ms": prof["particle_ms"], "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
+        "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="brazilian_disc", choices=["brazilian_disc", "uniaxial_cylinder"])
+    ap.add_argument("--workload", default="brazilian_disc",
+                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep"])
+    ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
+    ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
@@ -248,11 +315,13 @@ def main() -> int:
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank, local)
+    if args.workload == "calibration_sweep":
+        return run_sweep(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
     spec = specs[0]
-    ctx = dem.Context(device=local, graph_steps=200)
+    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks)
     sids = [ctx.add_sample(sp.material, sp.loading, sp.xyz, sp.radii) for sp in specs]
     ctx.setup()
     cnt = ctx.counts()

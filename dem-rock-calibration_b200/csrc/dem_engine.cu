@@ -125,8 +125,22 @@ class Engine final : public EngineBase {
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     int dev = opt_.device;
     CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
-    if (!opt_.pair_block || opt_.pair_block > 256) opt_.pair_block = 256;
-    if (!opt_.pair_grid) opt_.pair_grid = (uint32_t)num_sms_ * 8;
+    // the pair kernel: 256-thread blocks (one bond tile per pass), as many
+    // blocks as fit on the GPU; register budget for pair_min_blocks blocks per
+    // SM (1..4; 0 = 4 for FP32, 2 for FP64)
+    opt_.pair_block = 256;
+    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4) opt_.pair_min_blocks = sizeof(Real) == 4 ? 4 : 2;
+    switch (opt_.pair_min_blocks) {
+      case 1: pair_kernel_ = (const void*)k_pairs<Real, 1>; break;
+      case 2: pair_kernel_ = (const void*)k_pairs<Real, 2>; break;
+      case 3: pair_kernel_ = (const void*)k_pairs<Real, 3>; break;
+      default: pair_kernel_ = (const void*)k_pairs<Real, 4>; break;
+    }
+    if (!opt_.pair_grid) {
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel_, (int)opt_.pair_block, 0));
+      opt_.pair_grid = (uint32_t)num_sms_ * (uint32_t)std::max(per_sm, 1);
+    }
     if (!opt_.particle_block) opt_.particle_block = 256;
     if (!opt_.graph_steps) opt_.graph_steps = 100;
     if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.25;
@@ -514,11 +528,13 @@ class Engine final : public EngineBase {
     CK(js.alloc(std::max(nb, 1u)));
     S.out_j = js.p;
     k_pair_search<Real, true><<<grid1(np_), 128, 0, stream_>>>(S);
-    CK(b_ij_.alloc(std::max(nb, 1u)));
-    CK(b_s0_.alloc(std::max(nb, 1u)));
-    CK(b_s1_.alloc(std::max(nb, 1u)));
-    CK(b_s2_.alloc(std::max(nb, 1u)));
-    CK(b_par_.alloc(std::max(nb, 1u)));
+    // whole tiles: the pair kernel copies bond state tile by tile
+    const size_t nb_pad = ((size_t)std::max(nb, 1u) + 255) / 256 * 256;
+    CK(b_ij_.alloc(nb_pad));
+    CK(b_s0_.alloc(nb_pad));
+    CK(b_s1_.alloc(nb_pad));
+    CK(b_s2_.alloc(nb_pad));
+    CK(b_par_.alloc(nb_pad));
     CK(b_row_.alloc(np_ + 1));
     const uint32_t S_ = (uint32_t)samples_.size();
     DBuf<int32_t> counts;
@@ -707,8 +723,18 @@ class Engine final : public EngineBase {
     return A;
   }
 
+  void launch_pairs(const StepArgs<Real>& A) {
+    const dim3 g(opt_.pair_grid), b(opt_.pair_block);
+    switch (opt_.pair_min_blocks) {
+      case 1: k_pairs<Real, 1><<<g, b, 0, stream_>>>(A); break;
+      case 2: k_pairs<Real, 2><<<g, b, 0, stream_>>>(A); break;
+      case 3: k_pairs<Real, 3><<<g, b, 0, stream_>>>(A); break;
+      default: k_pairs<Real, 4><<<g, b, 0, stream_>>>(A); break;
+    }
+  }
+
   void launch_step(const StepArgs<Real>& A, int stages) {
-    if (stages & 1) k_pairs<Real><<<opt_.pair_grid, opt_.pair_block, 0, stream_>>>(A);
+    if (stages & 1) launch_pairs(A);
     if (stages & 2) {
       const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
       k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
@@ -1238,7 +1264,7 @@ class Engine final : public EngineBase {
     const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
     for (uint32_t k = 0; k < nsteps; ++k) {
       CK(cudaEventRecord(ev[4 * k], stream_));
-      k_pairs<Real><<<opt_.pair_grid, opt_.pair_block, 0, stream_>>>(A);
+      launch_pairs(A);
       CK(cudaEventRecord(ev[4 * k + 1], stream_));
       CK(cudaEventRecord(ev[4 * k + 2], stream_));
       k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
@@ -1276,6 +1302,7 @@ class Engine final : public EngineBase {
   cudaStream_t stream_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   int num_sms_ = 148;
+  const void* pair_kernel_ = nullptr;
   bool setup_done_ = false, forces_dirty_ = false, contacts_dirty_ = false, stale_ = false;
   cudaError_t last_cuda_ = cudaSuccess;
   uint64_t total_steps_ = 0, rebuilds_ = 0, stale_events_ = 0;

@@ -322,7 +322,7 @@ class Packer {
           CKP(cudaMemcpyAsync(&fire.p->dmax2, &z, sizeof(float), cudaMemcpyHostToDevice, st));
         }
         k_soft_pairs<float><<<gp, 256, 0, st>>>(A);
-        if (!viscous) k_fire_power<float><<<gn, 256, 0, st>>>(A);
+        k_fire_power<float><<<gn, 256, 0, st>>>(A);
         k_fire_move<float><<<gn, 256, 0, st>>>(A);
       }
       CKP(cudaGetLastError());

@@ -5,12 +5,13 @@
 //   k_soft_pairs      pair force of d_CalculateForces (md_calculateforces.cu:20-67):
 //                     F_i += -D (a^2/r^2) (x_j - x_i) for r < a, a = s (r_i + r_j),
 //                     or a linear overlap spring (packing by radius growth)
-//   k_fire_power      P = F.v, |v|^2, |F|^2 per sample, reduced per block
-//                     (d_FdotVEntire, md_firerelaxation.cu:375-494); the last block
-//                     adapts dt and alpha on the device (the host logic of
-//                     md_createcylindersample.cu:368-397)
-//   k_fire_move       one FIRE move and the cylinder confinement
-//                     (d_CylinderRestrictionZ, md_cylinderrestriction.cu:190-234).
+//   k_fire_power      cylinder walls as linear springs of the pair stiffness (the
+//                     confinement of d_CylinderRestrictionZ, md_cylinderrestriction.cu:190-234,
+//                     as a force so FIRE sees it), then P = F.v, |v|^2, |F|^2 per
+//                     sample, reduced per block (d_FdotVEntire, md_firerelaxation.cu:375-494);
+//                     the last block adapts dt and alpha on the device (the host
+//                     logic of md_createcylindersample.cu:368-397)
+//   k_fire_move       one FIRE move; a centre that crossed a wall is put back.
 //                     Variant 0 is inertial FIRE 2.0 (Guenole et al., Comput. Mater.
 //                     Sci. 175 (2020) 109584: half step back and v = 0 on P <= 0,
 //                     semi-implicit Euler, velocity mixing); variant 1 is the
@@ -124,14 +125,47 @@ __global__ void __launch_bounds__(256) k_fire_power(PackArgs<Real> A) {
   using V4 = typename RT<Real>::V4;
   __shared__ int s_last;
   double pw = 0.0, vv = 0.0, ff = 0.0;
+  float worst = 0.f;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
-    const V4 f = A.frc[p], v = A.vel[p];
+    const uint32_t s = A.sid[p];
+    const V4 x = A.pos[p], v = A.vel[p];
+    V4 f = A.frc[p];
+    // walls: radius R - r_i, caps at +-(H - r_i), force D * penetration
+    const Real* c = A.cyl + 5 * s;
+    const Real r = A.scale[s] * x.w, D = A.D[s];
+    const Real R0 = c[3] - r, H0 = c[4] - r;
+    const Real dx = x.x - c[0], dy = x.y - c[1], dz = x.z - c[2];
+    const Real rr = dx * dx + dy * dy;
+    Real pen = Real(0);
+    if (rr > R0 * R0) {
+      const Real rho = RT<Real>::sqrt_rn(rr);
+      pen = rho - R0;
+      const Real q = -D * pen / rho;
+      f.x += q * dx;
+      f.y += q * dy;
+    }
+    if (dz > H0) {
+      f.z -= D * (dz - H0);
+      pen = fmax(pen, dz - H0);
+    }
+    if (dz < -H0) {
+      f.z += D * (-H0 - dz);
+      pen = fmax(pen, -H0 - dz);
+    }
+    if (pen > Real(0)) {
+      A.frc[p] = f;
+      worst = fmaxf(worst, (float)(pen / (Real(2) * r)));
+    }
     pw += (double)((f.x * v.x + f.y * v.y) + f.z * v.z);
     vv += (double)((v.x * v.x + v.y * v.y) + v.z * v.z);
     ff += (double)((f.x * f.x + f.y * f.y) + f.z * f.z);
   }
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xFFFFFFFFu, worst, o));
+  if ((threadIdx.x & 31) == 0 && worst > 0.f)
+    atomicMax(reinterpret_cast<int*>(&A.fire[0].max_overlap), __float_as_int(worst));
   block_sum3(pw, vv, ff);
   FireCtl& F = A.fire[0];
+  if (A.viscous) return;
   if (threadIdx.x == 0) {
     if (pw != 0.0) atomicAdd(&F.P, pw);
     if (vv != 0.0) atomicAdd(&F.vv, vv);
@@ -240,25 +274,30 @@ __global__ void __launch_bounds__(256) k_fire_move(PackArgs<Real> A) {
       x.y += v.y * dt;
       x.z += v.z * dt;
     }
-    // cylinder confinement of the particle centre (radius R - r_i, half height H - r_i)
+    // a centre that crossed a wall surface is put back on it with its normal
+    // velocity removed (the wall springs keep everything else inside)
     const Real* c = A.cyl + 5 * s;
-    const Real R0 = c[3] - A.scale[s] * x.w, H0 = c[4] - A.scale[s] * x.w;
+    const Real R1 = c[3], H1 = c[4];
     const Real dx = x.x - c[0], dy = x.y - c[1], dz = x.z - c[2];
-    Real rr = dx * dx + dy * dy;
-    if (rr > R0 * R0) {
-      const Real q = R0 * T::rsqrt_rn(rr) - Real(1);
+    const Real rr = dx * dx + dy * dy;
+    if (rr > R1 * R1) {
+      const Real rinv = T::rsqrt_rn(rr);
+      const Real q = R1 * rinv - Real(1);
       x.x += dx * q;
       x.y += dy * q;
-      v.x = -v.x;
-      v.y = -v.y;
+      const Real vn = (v.x * dx + v.y * dy) * rinv;
+      if (vn > Real(0)) {
+        v.x -= vn * dx * rinv;
+        v.y -= vn * dy * rinv;
+      }
     }
-    if (dz > H0) {
-      x.z += H0 - dz;
-      v.z = -v.z;
+    if (dz > H1) {
+      x.z += H1 - dz;
+      if (v.z > Real(0)) v.z = Real(0);
     }
-    if (dz < -H0) {
-      x.z += -H0 - dz;
-      v.z = -v.z;
+    if (dz < -H1) {
+      x.z += -H1 - dz;
+      if (v.z < Real(0)) v.z = Real(0);
     }
     A.pos[p] = x;
     A.vel[p] = v;

@@ -170,14 +170,12 @@ __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i
 // reference is its exact mirror (all vectors negated, the unsymmetric moment
 // equal), so j receives -F, -(Mn + Mt) terms and the same unsymmetric moment.
 template <class Real>
-__device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b) {
+__device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
+                                        typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
+                                        typename RT<Real>::V4 s1, typename RT<Real>::V4 s2) {
   using T = RT<Real>;
   using V4 = typename T::V4;
-  // every load is issued before the first branch: the bond's own state, then
-  // the gathers that depend only on (i, j)
-  const uint2 ij = __ldcs(A.b_ij + b);
-  V4 par = ld4_cs(A.b_par + b);
-  V4 s0 = ld4_cs(A.b_s0 + b), s1 = ld4_cs(A.b_s1 + b), s2 = ld4_cs(A.b_s2 + b);
+  // the gathers depend only on (i, j): all issued before the first branch
   const uint32_t i = ij.x, j = ij.y;
   const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
   const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
@@ -352,16 +350,33 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
   if (!has_hist) A.c_ij[c] = make_uint2(i, j | 0x80000000u);
 }
 
-template <class Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2) k_pairs(StepArgs<Real> A) {
+// Pair kernel: one thread per bond, then one per contact-list pair, grid
+// stride.  A block's bonds of one pass are a contiguous tile of blockDim
+// bonds; while the block works on it, one thread asks the copy engine to
+// prefetch the block's next tile of bond state into L2 (five bulk prefetches),
+// so the next pass finds its streamed loads in L2.  Bond arrays are padded to
+// whole 256-bond tiles.
+template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2)>
+__global__ void __launch_bounds__(256, kMinBlocks) k_pairs(StepArgs<Real> A) {
+  using V4 = typename RT<Real>::V4;
   const uint32_t nb = A.nb;
-  const uint32_t total = nb + *A.nc;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    if (t < nb)
-      do_bond<Real>(A, t);
-    else
-      do_contact<Real>(A, t - nb);
+  const uint32_t tile = blockDim.x, stride = gridDim.x * tile;
+  for (uint32_t base = blockIdx.x * tile; base < nb; base += stride) {
+    if (threadIdx.x == 0 && base + stride < nb) {
+      const size_t nx = base + stride;
+      l2_prefetch(A.b_ij + nx, tile * sizeof(uint2));
+      l2_prefetch(A.b_par + nx, tile * sizeof(V4));
+      l2_prefetch(A.b_s0 + nx, tile * sizeof(V4));
+      l2_prefetch(A.b_s1 + nx, tile * sizeof(V4));
+      l2_prefetch(A.b_s2 + nx, tile * sizeof(V4));
+    }
+    const uint32_t b = base + threadIdx.x;
+    if (b < nb)
+      do_bond<Real>(A, b, __ldcs(A.b_ij + b), ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b),
+                    ld4_cs(A.b_s2 + b));
   }
+  const uint32_t nc = *A.nc;
+  for (uint32_t c = blockIdx.x * tile + threadIdx.x; c < nc; c += stride) do_contact<Real>(A, c);
 }
 
 // Particle-platen contact (dd_Calculate_fijn_pwHM_2 + dd_Calculate_fijtmijt_pwHM_2,

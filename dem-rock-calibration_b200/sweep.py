@@ -1,0 +1,142 @@
+"""Batched calibration sweeps: many specimens x micro-parameter sets advanced
+together in one engine context (one launch per kernel per step for all of
+them), against the same work run one specimen at a time.
+
+The reference runs one specimen per process (kernel.cu:23-123, one
+h_Calculation* call per sample, mp_calculateonesample.cu:151-214) and its
+calibration drivers call it once per parameter set (mp_determineconjgradient.cu:
+84-351: six finite-difference solves per conjugate-gradient step).  Here a
+parameter set is a dem_material, a specimen a packed cylinder; a sweep is the
+Cartesian pairing given by the caller.
+
+Parameter space of the sweep (seeded Latin hypercube):
+    bond E 10-80 GPa, kn/ks 1-4, strength mean 20-80 MPa, strength sd 10-25% of
+    the mean, friction 0.2-0.8, bond-radius factor 0.5-1.0.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (Context, TEST_UNIAXIAL, VELOCITY, Material, bounding_box, create_cylinder_sample, loading,
+               reference_space)
+from .workloads import mean_r3, rock_material
+
+# name: (low, high)
+SWEEP_SPACE = {
+    "E_bond": (10.0, 80.0),        # GPa
+    "kn_ks": (1.0, 4.0),
+    "strength": (0.020, 0.080),    # GPa (mean of N(mean, sd) per bond, normal and shear)
+    "strength_sd": (0.10, 0.25),   # fraction of the mean
+    "mu": (0.2, 0.8),
+    "bond_radius_factor": (0.5, 1.0),
+}
+
+
+def latin_hypercube(n: int, seed: int, space: dict = SWEEP_SPACE) -> list[dict]:
+    """n points, one per row of every parameter's n equal strata (seeded)."""
+    rng = np.random.default_rng(seed)
+    keys = list(space)
+    out = np.empty((n, len(keys)))
+    for k, name in enumerate(keys):
+        lo, hi = space[name]
+        u = (rng.permutation(n) + rng.random(n)) / n
+        out[:, k] = lo + u * (hi - lo)
+    return [dict(zip(keys, row)) for row in out]
+
+
+def material_for(p: dict, r_min: float, r_mean: float, seed: int) -> Material:
+    s = p["strength"]
+    return rock_material(r_min, r_mean, E_bond=p["E_bond"], kn_ks=p["kn_ks"], Ec=s, Gc=s,
+                         Ec_sd=p["strength_sd"] * s, Gc_sd=p["strength_sd"] * s, mu=p["mu"],
+                         bond_radius_factor=p["bond_radius_factor"], seed=seed)
+
+
+def cylinder(n: int, seed: int, r_min: float = 0.20, r_max: float = 0.30, packing: float = 0.58,
+             aspect: float = 2.0, device: int = 0) -> tuple[np.ndarray, np.ndarray, dict, float, float]:
+    """A packed cylinder of about n spheres (height = aspect x diameter)."""
+    R = (n * (4.0 / 3.0) * mean_r3(r_min, r_max) / (packing * math.pi * 2.0 * aspect)) ** (1.0 / 3.0)
+    half_h = aspect * R
+    xyz, rad, rep = create_cylinder_sample((0.0, 0.0, 0.0), R, half_h, n, r_min, r_max, seed=seed, growth_stages=30,
+                                           steps_per_stage=150, max_fire_steps=6000, overlap_tol=2e-3,
+                                           device=device)
+    return xyz, rad, rep, R, half_h
+
+
+@dataclass
+class SweepCase:
+    """One specimen under one parameter set, ready for add_sample."""
+    specimen: int
+    params: dict
+    material: Material
+    loading: object
+    xyz: np.ndarray
+    radii: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.radii.size
+
+
+@dataclass
+class Sweep:
+    cases: list = field(default_factory=list)
+
+    @property
+    def particles(self) -> int:
+        return sum(c.n for c in self.cases)
+
+
+def build_sweep(n_cases: int, sizes: list[int], seed: int = 1, velocity_m_s: float = 0.1, max_steps: int = 0,
+                device: int = 0) -> Sweep:
+    """n_cases parameter sets (Latin hypercube) over len(sizes) packed
+    cylinders (case k uses specimen k mod len(sizes)): uniaxial loading at
+    velocity_m_s until the peak has passed (70% of it) or 1% strain."""
+    specs = []
+    for k, n in enumerate(sizes):
+        xyz, rad, rep, R, half_h = cylinder(n, seed * 1000 + k, device=device)
+        r_max = float(rad.max())
+        space_si = (2 * R * 1.3e-3, 2 * R * 1.3e-3, 2 * half_h * 1.5e-3)
+        lsi = (2 * R * 1e-3, 2 * R * 1e-3, 2 * half_h * 1e-3)
+        box = reference_space(space_si, lsi, r_max, 3.2)
+        size_real, center_real = bounding_box(xyz, rad.size, r_max)
+        specs.append((xyz, rad, box, size_real, center_real))
+    sw = Sweep()
+    for k, p in enumerate(latin_hypercube(n_cases, seed)):
+        xyz, rad, box, size_real, center_real = specs[k % len(specs)]
+        r_min, r_mean = float(rad.min()), float(rad.mean())
+        ld = loading(TEST_UNIAXIAL, box, size_real, center_real, velocity=-velocity_m_s / VELOCITY, min_stress=0.010,
+                     max_strain=0.01, cond_fracture=0.7, dNsave=100, max_steps=max_steps, p_r_platen=r_mean)
+        sw.cases.append(SweepCase(k % len(specs), p, material_for(p, r_min, r_mean, seed * 7919 + k), ld, xyz, rad))
+    return sw
+
+
+def run_batched(sw: Sweep, steps: int, device: int = 0, graph_steps: int = 200) -> dict:
+    """All cases in one context; `steps` steps (finished cases stay frozen).
+    Returns device time, wall time (set-up included) and per-case results."""
+    t0 = time.perf_counter()
+    ctx = Context(device=device, graph_steps=graph_steps)
+    ids = [ctx.add_sample(c.material, c.loading, c.xyz, c.radii) for c in sw.cases]
+    ctx.setup()
+    ms = ctx.run_timed(steps)
+    res = [ctx.result(i) for i in ids]
+    ctx.close()
+    return dict(device_ms=ms, wall_s=time.perf_counter() - t0, results=res)
+
+
+def run_sequential(sw: Sweep, steps: int, device: int = 0, graph_steps: int = 200) -> dict:
+    """The same cases one context at a time (the reference's one-specimen-per-run
+    pattern on this engine)."""
+    t0 = time.perf_counter()
+    ms, res = 0.0, []
+    for c in sw.cases:
+        ctx = Context(device=device, graph_steps=graph_steps)
+        ctx.add_sample(c.material, c.loading, c.xyz, c.radii)
+        ctx.setup()
+        ms += ctx.run_timed(steps)
+        res.append(ctx.result(0))
+        ctx.close()
+    return dict(device_ms=ms, wall_s=time.perf_counter() - t0, results=res)

@@ -59,11 +59,14 @@ typedef struct dem_ctx dem_ctx;
 typedef struct {
   int precision;          /* 0: FP32, 1: FP64 */
   int device;             /* CUDA device ordinal */
-  uint32_t pair_block;    /* threads per block of the pair kernel (0: 256) */
-  uint32_t pair_grid;     /* blocks of the pair kernel (0: 8 per SM) */
+  uint32_t pair_block;    /* ignored: the pair kernel runs 256-thread blocks */
+  uint32_t pair_grid;     /* blocks of the pair kernel (0: all co-resident blocks) */
   uint32_t particle_block;/* threads per block of the particle kernel (0: 256) */
   uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
   double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.25) */
+  uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
+                               (1..4; 0: 4 for FP32, 2 for FP64) */
+  uint32_t reserved;
 } dem_options;
 
 /* Micro-parameters of one specimen.  The first block is the reference's

@@ -167,6 +167,7 @@ def _declare_ref(L):
     L.refh_setup_bonds.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _u32, C.c_float, C.c_float, C.c_float,
                                    C.c_float, _vp, _vp, _vp]
     L.refh_step.argtypes = [C.POINTER(StepParams), _u32] + [_vp] * 14
+    L.refh_time_steps.argtypes = [C.POINTER(StepParams), _u32] + [_vp] * 6 + [_u32, C.c_int, C.POINTER(C.c_double)]
     L.refh_run_test.argtypes = [C.c_int, C.c_char_p, C.c_char_p, C.POINTER(TestParams), C.POINTER(TestResult)]
 
 

@@ -1,9 +1,9 @@
 // Test harness around the reference's OWN CUDA kernels and host drivers
 // (test infrastructure only).  oracle/Makefile compiles the reference sources
 // from the reference tree together with this file into oracle/_ref/libdemref.so;
-// tests/golden/make_golden.py and bench.py load it with ctypes on a GPU box to
-// produce golden vectors and the reference-GPU timing.  Nothing here is part of
-// the product.
+// tests/golden/make_golden.py and the GPU tests load it with ctypes on a GPU box
+// to produce golden vectors, run the reference's drivers and time its kernels.
+// Nothing here is part of the product.
 //
 // Every entry point takes and returns host arrays in the reference layout
 // (SoA x[0..N) y[N..2N) z[2N..3N); IonP slots per particle; float3 per slot)
@@ -291,6 +291,113 @@ int refh_step(const refh_step_params* p, uint32_t N, float* R, float* V, float* 
   chk(cudaMemcpy(Mijn, td.IL.d_Mijn, S * 12, cudaMemcpyDeviceToHost));
   chk(cudaMemcpy(Mijt, td.IL.d_Mijt, S * 12, cudaMemcpyDeviceToHost));
   if (FL) chk(cudaMemcpy(FL, td.R.d_FL, 2 * bl * 4, cudaMemcpyDeviceToHost));
+  cells_free(td);
+  void* ps[] = {td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_F, td.P.d_M, td.P.d_Oiwt, td.IL.d_IL, td.IL.d_ILtype,
+                td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                td.IL.d_Mijadd, td.R.d_FL};
+  for (void* q : ps) dfree(q);
+  return g_err;
+}
+
+// Device time of nsteps passes of the reference's loop body on one state
+// (test infrastructure: the reference-GPU baseline).  Each pass launches the
+// kernels of md_calculationuniaxialcompression.cu:265-314 selected by
+// p->stages, in that order, and - when sync_fl is set - copies the platen
+// partial sums to the host as SumForcesULoading does every step
+// (md_results.cu:56-100).  *ms = CUDA-event time of the whole loop.
+int refh_time_steps(const refh_step_params* p, uint32_t N, const float* R, const float* V, const float* W,
+                    const uint32_t* IL, const uint32_t* ILtype, const float* invL0, uint32_t nsteps, int sync_fl,
+                    double* ms) {
+  g_err = 0;
+  md_task_data td;
+  setup_task(td, N, p->a, p->nx, p->ny, p->nz);
+  const uint32_t IonP = p->IonP;
+  size_t S = (size_t)N * IonP;
+  td.P.d_R = dalloc<float>(3 * N);
+  td.P.d_V = dalloc<float>(3 * N);
+  td.P.d_W = dalloc<float>(3 * N);
+  td.P.d_F = dalloc<float>(3 * N);
+  td.P.d_M = dalloc<float>(3 * N);
+  td.P.d_Oiwt = dalloc<float>(3 * N);
+  td.IL.IonP = IonP;
+  td.IL.N = S;
+  td.IL.aacut = p->il_aacut;
+  td.IL.d_IL = dalloc<uint>(S);
+  td.IL.d_ILtype = dalloc<uint>(S);
+  td.IL.d_1d_iL = dalloc<float>(S);
+  td.IL.d_rij = dalloc<float3>(S);
+  td.IL.d_Oijt = dalloc<float3>(S);
+  td.IL.d_Fijn = dalloc<float3>(S);
+  td.IL.d_Fijt = dalloc<float3>(S);
+  td.IL.d_Mijn = dalloc<float3>(S);
+  td.IL.d_Mijt = dalloc<float3>(S);
+  td.IL.d_Mijadd = dalloc<float3>(S);
+  td.R.d_FL = dalloc<float>(2 * td.A.bloks);
+  chk(cudaMemcpy(td.P.d_R, R, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_V, V, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.P.d_W, W, 3 * N * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_IL, IL, S * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_ILtype, ILtype, S * 4, cudaMemcpyHostToDevice));
+  chk(cudaMemcpy(td.IL.d_1d_iL, invL0, S * 4, cudaMemcpyHostToDevice));
+  cells_create(td);
+  const uint bl = td.A.bloks;
+  float* hFL = new float[2 * bl];
+  const float3 c = make_float3(p->center[0], p->center[1], p->center[2]);
+  const float3 sc = make_float3(p->s_center[0], p->s_center[1], p->s_center[2]);
+  const float3 s2 = make_float3(p->s_spacesized2[0], p->s_spacesized2[1], p->s_spacesized2[2]);
+  const float3 hp = make_float3(p->hidenpoint[0], p->hidenpoint[1], p->hidenpoint[2]);
+  cudaEvent_t e0, e1;
+  chk(cudaEventCreate(&e0));
+  chk(cudaEventCreate(&e1));
+  chk(cudaDeviceSynchronize());
+  chk(cudaEventRecord(e0));
+  for (uint32_t k = 0; k < nsteps; ++k) {
+    if (p->stages & 1) {
+      CellDistribution(td.P, td.A, td.S, td.C);
+      InteractionListReConstructBPM(td.P, td.A, td.S, td.IL, td.C);
+    }
+    if (p->stages & 2) {
+      chk(cudaMemset(td.P.d_F, 0, 3 * N * sizeof(float)));
+      chk(cudaMemset(td.P.d_M, 0, 3 * N * sizeof(float)));
+      d_CalculateForcesDEM_22<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                               td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                               td.P.d_F, td.P.d_M, N, IonP, p->dt, p->m_E, p->m_G, p->b_r, p->m_Ec,
+                                               p->m_Gc);
+      d_CalculateForcesDEM_21<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.IL.d_IL, td.IL.d_ILtype,
+                                               td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.P.d_F, td.P.d_M, N, IonP,
+                                               p->dt, p->hm_E, p->hm_G, p->p_A, p->p_mu, p->p_mur, p->p_m, p->p_r);
+    }
+    if (p->stages & 4) {
+      if (p->brazil)
+        d_BrazilCompression_hm<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_Oiwt, td.P.d_F, td.P.d_M, N,
+                                                p->dt, p->wall_E, p->wall_G, p->p_A, p->p_mu, p->p_mur, p->p_m,
+                                                p->p_r, td.R.d_FL, c, p->wall_RR, p->wall_top, p->wall_bot, p->wall_V,
+                                                p->Zcut);
+      else
+        d_UniaxialCompression_hm<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_Oiwt, td.P.d_F, td.P.d_M, N,
+                                                  p->dt, p->wall_E, p->wall_G, p->p_A, p->p_mu, p->p_mur, p->p_m,
+                                                  p->p_r, td.R.d_FL, c, p->wall_RR, p->wall_top, p->wall_bot,
+                                                  p->wall_V, p->Zcut);
+      if (sync_fl) chk(cudaMemcpy(hFL, td.R.d_FL, 2 * bl * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    if (p->stages & 8)
+      d_CalculateIncrementsDEM<<<bl, SMEMDIM>>>(td.P.d_F, td.P.d_V, td.P.d_R, td.P.d_M, td.P.d_W, N, p->dt_d_m,
+                                                p->dt, p->dt_d_I);
+    if (p->stages & 16) d_ParallelepipedCutRestriction<<<bl, SMEMDIM>>>(td.P.d_R, td.P.d_V, td.P.d_F, N, sc, s2, hp);
+    if (p->stages & 32)
+      d_DeleteFarLinks<<<bl, SMEMDIM>>>(td.P.d_R, N, td.IL.d_IL, td.IL.d_ILtype, td.IL.d_1d_iL, td.IL.d_rij,
+                                        td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,
+                                        td.IL.d_Mijadd, IonP, p->aa_farcut);
+  }
+  chk(cudaEventRecord(e1));
+  chk(cudaEventSynchronize(e1));
+  float t = 0.f;
+  chk(cudaEventElapsedTime(&t, e0, e1));
+  *ms = t;
+  chk(cudaGetLastError());
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  delete[] hFL;
   cells_free(td);
   void* ps[] = {td.P.d_R, td.P.d_V, td.P.d_W, td.P.d_F, td.P.d_M, td.P.d_Oiwt, td.IL.d_IL, td.IL.d_ILtype,
                 td.IL.d_1d_iL, td.IL.d_rij, td.IL.d_Oijt, td.IL.d_Fijn, td.IL.d_Fijt, td.IL.d_Mijn, td.IL.d_Mijt,

@@ -259,6 +259,16 @@ def ref_setup_bonds(st: RefState, sc: Scalars) -> None:
     st.Mijt[:] = 0
 
 
+def ref_time_steps(st: RefState, sc: Scalars, nsteps: int, stages: int = STAGE_ALL, sync_fl: bool = True) -> float:
+    """Device milliseconds of nsteps passes of the reference's loop body on the state."""
+    p = sc.to_c(stages)
+    ms = C.c_double()
+    rc = L.ref().refh_time_steps(C.byref(p), st.N, L.P(st.R), L.P(st.V), L.P(st.W), L.P(st.IL), L.P(st.ILtype),
+                                 L.P(st.invL0), nsteps, 1 if sync_fl else 0, C.byref(ms))
+    assert rc == 0, rc
+    return ms.value
+
+
 def ref_step(st: RefState, sc: Scalars, stages: int = STAGE_ALL):
     FL = np.zeros(2 * (st.N // 64 + 1), np.float32)
     p = sc.to_c(stages)

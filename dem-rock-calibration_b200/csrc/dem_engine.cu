@@ -127,9 +127,10 @@ class Engine final : public EngineBase {
     CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
     // the pair kernel: 256-thread blocks (one bond tile per pass), as many
     // blocks as fit on the GPU; register budget for pair_min_blocks blocks per
-    // SM (1..4; 0 = 4 for FP32, 2 for FP64)
+    // SM (1..4; 0 = 3 for FP32 - 80 registers, no spills, the fastest on B200 -
+    // and 2 for FP64)
     opt_.pair_block = 256;
-    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4) opt_.pair_min_blocks = sizeof(Real) == 4 ? 4 : 2;
+    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4) opt_.pair_min_blocks = sizeof(Real) == 4 ? 3 : 2;
     switch (opt_.pair_min_blocks) {
       case 1: pair_kernel_ = (const void*)k_pairs<Real, 1>; break;
       case 2: pair_kernel_ = (const void*)k_pairs<Real, 2>; break;

@@ -58,7 +58,8 @@ def material_for(p: dict, r_min: float, r_mean: float, seed: int) -> Material:
 def cylinder(n: int, seed: int, r_min: float = 0.20, r_max: float = 0.30, packing: float = 0.58,
              aspect: float = 2.0, device: int = 0) -> tuple[np.ndarray, np.ndarray, dict, float, float]:
     """A packed cylinder of about n spheres (height = aspect x diameter)."""
-    R = (n * (4.0 / 3.0) * mean_r3(r_min, r_max) / (packing * math.pi * 2.0 * aspect)) ** (1.0 / 3.0)
+    # n (4/3) pi <r^3> = packing * pi R^2 * (2 aspect R)
+    R = (n * (2.0 / 3.0) * mean_r3(r_min, r_max) / (packing * aspect)) ** (1.0 / 3.0)
     half_h = aspect * R
     xyz, rad, rep = create_cylinder_sample((0.0, 0.0, 0.0), R, half_h, n, r_min, r_max, seed=seed, growth_stages=30,
                                            steps_per_stage=150, max_fire_steps=6000, overlap_tol=2e-3,

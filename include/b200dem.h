@@ -65,7 +65,7 @@ typedef struct {
   uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
   double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.25) */
   uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
-                               (1..4; 0: 4 for FP32, 2 for FP64) */
+                               (1..4; 0: 3 for FP32, 2 for FP64) */
   uint32_t reserved;
 } dem_options;
 

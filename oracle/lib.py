@@ -168,6 +168,8 @@ def _declare_ref(L):
                                    C.c_float, _vp, _vp, _vp]
     L.refh_step.argtypes = [C.POINTER(StepParams), _u32] + [_vp] * 14
     L.refh_time_steps.argtypes = [C.POINTER(StepParams), _u32] + [_vp] * 6 + [_u32, C.c_int, C.POINTER(C.c_double)]
+    L.refh_cg_start_parameters.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp]
+    L.refh_cg_new_parameters2.argtypes = [_vp] * 7 + [C.c_int, C.c_double, _vp, _vp]
     L.refh_run_test.argtypes = [C.c_int, C.c_char_p, C.c_char_p, C.POINTER(TestParams), C.POINTER(TestResult)]
 
 

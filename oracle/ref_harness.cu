@@ -21,6 +21,7 @@
 
 #include "md.h"
 #include "mp.h"
+#include "mp_task.h"
 
 namespace {
 
@@ -493,6 +494,75 @@ int refh_run_test(int brazil, const char* workdir, const char* part, const refh_
   chk(cudaGetLastError());
   if (chdir(cwd) != 0) return -3;
   return g_err;
+}
+
+// CalculateStartParameters (mp_task.h:129-145): weights and the first
+// variation table from params[5], goal[4], multiplier[4]; goal updated in place.
+int refh_cg_start_parameters(const double* params, double* goal, const double* multiplier, int calc_u, int calc_b,
+                             int type, double delta, double* weight, double* variation) {
+  mp_task_data t;
+  t.NSteps = 2;
+  t.NParam = 5;
+  t.NResult = 4;
+  t.createarrays();
+  t.Step = 0;
+  t.ParameterVariationType = (uint8_t)type;
+  t.MaterialDeltaFactor = delta;
+  t.CalculateUTest = calc_u != 0;
+  t.CalculateBTest = calc_b != 0;
+  for (int i = 0; i < 5; ++i) t.MaterialParametersSteps[i] = params[i];
+  for (int j = 0; j < 4; ++j) {
+    t.ResultsGoal[j] = goal[j];
+    t.FunctionalParametersWeightMultiplier[j] = multiplier[j];
+  }
+  t.CalculateStartParameters();
+  for (int j = 0; j < 4; ++j) {
+    goal[j] = t.ResultsGoal[j];
+    weight[j] = t.FunctionalParametersWeight[j];
+  }
+  for (int i = 0; i < 30; ++i) variation[i] = t.ParameterVariation[i];
+  return 0;
+}
+
+// One conjugate-gradient parameter update of the reference's calibration
+// driver: mp_task_data::CalculateNewParameters2 (mp_task.h:223-311) on the
+// caller's arrays (NParam = 5, NResult = 4).  In: params[5] (the current
+// step's parameters), variation[30] (ParameterVariation), rfun[24]
+// (RFunction), goal[4], weight[4] (FunctionalParametersWeight),
+// dfun[6] / ddfun[6] (previous gradient and direction), type
+// (ParameterVariationType), delta (MaterialDeltaFactor).  Out: new_params[5],
+// variation, dfun, ddfun updated in place, functional[4].  Host-only.
+int refh_cg_new_parameters2(const double* params, double* variation, const double* rfun, const double* goal,
+                            const double* weight, double* dfun, double* ddfun, int type, double delta,
+                            double* new_params, double* functional) {
+  mp_task_data t;
+  t.NSteps = 2;
+  t.NParam = 5;
+  t.NResult = 4;
+  t.createarrays();
+  t.Step = 0;
+  t.ParameterVariationType = (uint8_t)type;
+  t.MaterialDeltaFactor = delta;
+  for (int i = 0; i < 5; ++i) t.MaterialParametersSteps[i] = params[i];
+  for (int i = 0; i < 30; ++i) t.ParameterVariation[i] = variation[i];
+  for (int i = 0; i < 24; ++i) t.RFunction[i] = rfun[i];
+  for (int j = 0; j < 4; ++j) {
+    t.ResultsGoal[j] = goal[j];
+    t.FunctionalParametersWeight[j] = weight[j];
+  }
+  for (int i = 0; i < 6; ++i) {
+    t.dFunctional[i] = dfun[i];
+    t.ddFunctional[i] = ddfun[i];
+  }
+  t.CalculateNewParameters2();
+  for (int i = 0; i < 5; ++i) new_params[i] = t.MaterialParametersSteps[5 + i];
+  for (int i = 0; i < 30; ++i) variation[i] = t.ParameterVariation[i];
+  for (int i = 0; i < 6; ++i) {
+    dfun[i] = t.dFunctional[i];
+    ddfun[i] = t.ddFunctional[i];
+  }
+  for (int j = 0; j < 4; ++j) functional[j] = t.Functional[j];
+  return 0;
 }
 
 }  // extern "C"

@@ -66,6 +66,14 @@ class Loading(C.Structure):
                 ("dNsave", C.c_uint32), ("reserved2", C.c_uint32), ("max_steps", C.c_uint64)]
 
 
+SENS_NAMES = ("E_bond", "kn_ks", "bond_radius", "E", "rho")
+
+
+class Sensitivity(C.Structure):
+    _fields_ = [("strain", C.c_double), ("stress", C.c_double), ("E_secant", C.c_double), ("nu_secant", C.c_double),
+                ("dstress", C.c_double * 5), ("dE", C.c_double * 5), ("dnu", C.c_double * 5)]
+
+
 class PackParams(C.Structure):
     _fields_ = [("center", C.c_double * 3), ("radius", C.c_double), ("half_height", C.c_double),
                 ("r_min", C.c_double), ("r_max", C.c_double), ("E", C.c_double), ("nu", C.c_double),
@@ -125,6 +133,8 @@ def _declare(L):
     L.dem_create_cylinder_sample.argtypes = [P(PackParams), _vp, _vp, _u32, P(_u32), P(PackReport)]
     L.dem_last_error_detail.restype = C.c_char_p
     L.dem_last_error_detail.argtypes = []
+    L.dem_save_lammps_data.argtypes = [_vp, C.c_int32, C.c_char_p, C.c_int]
+    L.dem_sensitivities.argtypes = [_vp, C.c_int32, P(Sensitivity)]
     L.dem_get_lateral_record.argtypes = [_vp, C.c_int32, _vp, _u32, P(_u32)]
     L.dem_ref_cells.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_cells_static.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
@@ -323,6 +333,18 @@ class Context:
         r = Result()
         _ck(_lib().dem_sample_result(self._h, sample, C.byref(r)), "dem_sample_result")
         return r.as_dict()
+
+    def save_lammps_data(self, path: str, sample: int = 0, with_energy: bool = False) -> None:
+        """SaveLammpsDATASimple: LAMMPS data file of one specimen."""
+        _ck(_lib().dem_save_lammps_data(self._h, sample, path.encode(), 1 if with_energy else 0), "dem_save_lammps_data")
+
+    def sensitivities(self, sample: int = 0) -> dict:
+        """Secant modulus and Poisson ratio at the last step; with precision=2
+        also their derivatives (arrays over SENS_NAMES)."""
+        s = Sensitivity()
+        _ck(_lib().dem_sensitivities(self._h, sample, C.byref(s)), "dem_sensitivities")
+        return dict(strain=s.strain, stress=s.stress, E_secant=s.E_secant, nu_secant=s.nu_secant,
+                    dstress=np.array(s.dstress[:]), dE=np.array(s.dE[:]), dnu=np.array(s.dnu[:]))
 
     def lateral_record(self, sample: int = 0) -> np.ndarray:
         """Mean radial distance of the lateral surface particles per record entry."""

@@ -20,7 +20,7 @@ SRC = PKG / "csrc"
 OUT = PKG / "libb200dem.so"
 
 SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_noalloc.cu", "dem_capi.cpp"]
-HEADERS = ["dem_common.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
+HEADERS = ["dem_common.cuh", "dem_dual.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
            "dem_engine.h"]
 
 NVCC_FLAGS = [

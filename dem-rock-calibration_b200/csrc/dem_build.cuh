@@ -20,7 +20,18 @@ template <class Real>
 struct Grid {
   Real ox, oy, oz, inv_a;
   uint32_t nx, ny, nz, off;
+  // the sample's hidden point: escaped particles are all parked there and,
+  // when skip_hidden is set, take part in no pair search (they interact with
+  // nothing anyway, and thousands of them in one cell would make the search
+  // quadratic)
+  Real hx, hy, hz;
+  uint32_t skip_hidden;
 };
+
+template <class Real, class V>
+__device__ __forceinline__ bool at_hidden(const Grid<Real>& g, const V& x) {
+  return g.skip_hidden && x.x == g.hx && x.y == g.hy && x.z == g.hz;
+}
 
 template <class Real>
 __device__ __forceinline__ uint32_t cell_coord(Real x, Real o, Real inv_a, uint32_t n) {
@@ -170,6 +181,10 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
     const auto xi = ld4(S.pos + i);
     const uint32_t s = S.sid[i];
     const Grid<Real> g = S.grids[s];
+    if (at_hidden(g, xi)) {
+      if (!kFill) S.count[i] = 0;
+      continue;
+    }
     const int ix = (int)cell_coord<Real>(xi.x, g.ox, g.inv_a, g.nx);
     const int iy = (int)cell_coord<Real>(xi.y, g.oy, g.inv_a, g.ny);
     const int iz = (int)cell_coord<Real>(xi.z, g.oz, g.inv_a, g.nz);
@@ -188,7 +203,7 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
           for (uint32_t k = S.cell_start[c], e = S.cell_start[c + 1]; k < e; ++k) {
             const uint32_t j = S.cell_list[k];
             const auto xj = ld4(S.pos + j);
-            if (!pair_pred<Real>(S, i, j, xi, xj, s)) continue;
+            if (at_hidden(g, xj) || !pair_pred<Real>(S, i, j, xi, xj, s)) continue;
             if (kFill && n < kMax && n < S.cap) buf[n] = j;
             ++n;
           }

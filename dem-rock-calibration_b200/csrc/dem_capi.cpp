@@ -56,7 +56,7 @@ int dem_create(const dem_options* opt, dem_ctx** out) {
   GUARD({
     dem_options o{};
     if (opt) o = *opt;
-    if (o.precision != 0 && o.precision != 1) return DEM_ERR_ARG;
+    if (o.precision < 0 || o.precision > 2) return DEM_ERR_ARG;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0 || o.device < 0 || o.device >= n) return DEM_ERR_CUDA;
     int err = DEM_OK;
@@ -98,6 +98,12 @@ int dem_counts(dem_ctx* ctx, uint32_t* p, uint32_t* b, uint32_t* c, uint32_t* s)
 int dem_sample_result(dem_ctx* ctx, int32_t sample, dem_result* out) { CTX_CALL(ctx->e->result(sample, out)); }
 int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n) {
   CTX_CALL(ctx->e->get_record(sample, rec, bonds, cap, n));
+}
+int dem_save_lammps_data(dem_ctx* ctx, int32_t sample, const char* path, int with_energy) {
+  CTX_CALL(ctx->e->save_lammps(sample, path, with_energy));
+}
+int dem_sensitivities(dem_ctx* ctx, int32_t sample, dem_sensitivity* out) {
+  CTX_CALL(ctx->e->sensitivities(sample, out));
 }
 int dem_get_lateral_record(dem_ctx* ctx, int32_t sample, double* lat, uint32_t cap, uint32_t* n) {
   CTX_CALL(ctx->e->get_lateral_record(sample, lat, cap, n));

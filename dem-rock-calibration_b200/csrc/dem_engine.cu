@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "dem_build.cuh"
+#include "dem_dual.cuh"
 #include "dem_params.h"
 #include "dem_step.cuh"
 
@@ -105,6 +106,7 @@ struct SampleHost {
   double E_b = 0, G_b = 0, hm_E = 0, hm_G = 0;
   int32_t bonds_initial = 0;
   uint32_t lat_count = 0;   // lateral surface particles (uniaxial specimens)
+  double lat_rho0 = 0;      // their mean radial distance at set-up
 };
 
 template <class Real>
@@ -118,7 +120,7 @@ class Engine final : public EngineBase {
     if (stream_) cudaStreamDestroy(stream_);
   }
 
-  int precision() const override { return sizeof(Real) == 8 ? 1 : 0; }
+  int precision() const override { return DualK<Real>::K ? 2 : (sizeof(Real) == 8 ? 1 : 0); }
 
   int init() {
     CK(cudaSetDevice(opt_.device));
@@ -130,7 +132,8 @@ class Engine final : public EngineBase {
     // SM (1..4; 0 = 3 for FP32 - 80 registers, no spills, the fastest on B200 -
     // and 2 for FP64)
     opt_.pair_block = 256;
-    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4) opt_.pair_min_blocks = sizeof(Real) == 4 ? 3 : 2;
+    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4)
+      opt_.pair_min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 3 : 2);
     switch (opt_.pair_min_blocks) {
       case 1: pair_kernel_ = (const void*)k_pairs<Real, 1>; break;
       case 2: pair_kernel_ = (const void*)k_pairs<Real, 2>; break;
@@ -197,6 +200,10 @@ class Engine final : public EngineBase {
         hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
         homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
         hmass[p] = (Real)m;
+        // sensitivity build: mass and dt/m, dt/I against the density
+        set_d(hmass[p], kSensRho, m / s.mat.rho);
+        set_d(hvel[p].w, kSensRho, -dtm / s.mat.rho);
+        set_d(homg[p].w, kSensRho, -dtI / s.mat.rho);
         hsid[p] = si;
         horig[p] = q;
       }
@@ -228,6 +235,7 @@ class Engine final : public EngineBase {
     RC(build_contacts(true));
     RC(init_controllers());
     CK(blocks_done_.alloc(1));
+    if (DualK<Real>::K) CK(sfl_tan_.alloc((size_t)S * (4 * DualK<Real>::K + 2)));
     CK(blk_stat_.alloc(2 * (size_t)num_sms_ * 8 + 64));
     CK(stat_.alloc(2));
     min_skin_ = 1e300;
@@ -262,13 +270,64 @@ class Engine final : public EngineBase {
         if (rho + s.rad[q] >= outer - 2.0 * s.rmean && std::fabs(s.xyz[2 * s.n + q] - cz) <= hz) {
           h[s.p_begin + k] = 1;
           ++s.lat_count;
+          s.lat_rho0 += rho;
         }
       }
+      if (s.lat_count) s.lat_rho0 /= s.lat_count;
       any = any || s.lat_count > 0;
     }
+    hlat_ = h;
     if (!any) return DEM_OK;
     CK(lat_.alloc(np_));
     CK(lat_.upload(h.data(), np_));
+    return DEM_OK;
+  }
+
+  // Secant modulus and secant Poisson ratio of a uniaxial specimen at the last
+  // completed step: stress from that step's platen force sums, lateral strain
+  // from the mean radial distance of the marked surface particles against
+  // set-up.  The sensitivity build (dual numbers) adds their derivatives;
+  // other builds report zeros there.
+  int sensitivities(int32_t si, dem_sensitivity* out) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !out) return DEM_ERR_ARG;
+    if (!setup_done_) return DEM_ERR_STATE;
+    constexpr int K = DualK<Real>::K;
+    const SampleHost& sh = samples_[si];
+    SampleCtl C;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&C, ctl_.p + si, sizeof(C), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    const double eps = -C.Strain;
+    out->strain = eps;
+    out->stress = C.Stress;
+    out->E_secant = std::nan("");
+    out->nu_secant = std::nan("");
+    if constexpr (K > 0) {
+      static_assert(K == DEM_SENS_COUNT, "derivative slots");
+      std::vector<double> t(4 * K + 2);
+      CK(cudaMemcpy(t.data(), sfl_tan_.p + (size_t)si * (4 * K + 2), t.size() * sizeof(double),
+                    cudaMemcpyDeviceToHost));
+      const double g0 = t[4 * K] < 0 ? -1.0 : 1.0, g1 = t[4 * K + 1] < 0 ? -1.0 : 1.0;
+      for (int k = 0; k < K; ++k) out->dstress[k] = 0.5 * (g0 * t[2 * K + k] + g1 * t[3 * K + k]) * C.inv_Area;
+    }
+    if (!(eps != 0)) return DEM_OK;
+    out->E_secant = out->stress / eps;
+    for (int k = 0; k < K; ++k) out->dE[k] = out->dstress[k] / eps;
+    if (!sh.lat_count || !(sh.lat_rho0 > 0)) return DEM_OK;
+    std::vector<V4> h(sh.n);
+    CK(cudaMemcpy(h.data(), pos_.p + sh.p_begin, sh.n * sizeof(V4), cudaMemcpyDeviceToHost));
+    const double cx = sh.load.center_real[0], cy = sh.load.center_real[1];
+    double rho = 0, drho[K > 0 ? K : 1] = {};
+    for (uint32_t k = 0; k < sh.n; ++k) {
+      if (!hlat_[sh.p_begin + k]) continue;
+      const double ex = (double)h[k].x - cx, ey = (double)h[k].y - cy, r = std::sqrt(ex * ex + ey * ey);
+      rho += r;
+      if constexpr (K > 0)
+        for (int q = 0; q < K; ++q) drho[q] += (ex * h[k].x.d[q] + ey * h[k].y.d[q]) / r;
+    }
+    rho /= sh.lat_count;
+    out->nu_secant = (rho - sh.lat_rho0) / sh.lat_rho0 / eps;
+    for (int q = 0; q < K; ++q) out->dnu[q] = drho[q] / sh.lat_count / sh.lat_rho0 / eps;
     return DEM_OK;
   }
 
@@ -359,6 +418,22 @@ class Engine final : public EngineBase {
       const bool brazil = L.test == DEM_TEST_BRAZIL;
       p.wallE = brazil ? (Real)s.hm_E : (Real)(2.0 * s.hm_E);
       p.wallG = brazil ? (Real)s.hm_G : (Real)(2.0 * s.hm_G);
+      // sensitivity build: bond moduli against E_bond and kn/ks, contact and
+      // platen moduli against the particle E (all proportional to it)
+      {
+        const int kE = m.E_bond > 0 ? kSensEBond : kSensE;
+        set_d(p.E, kE, 1.0);
+        if (m.kn_ks > 0) {
+          set_d(p.G, kE, 1.0 / m.kn_ks);
+          set_d(p.G, kSensKnKs, -s.E_b / (m.kn_ks * m.kn_ks));
+        } else {
+          set_d(p.G, kE, s.G_b / s.E_b);
+        }
+        set_d(p.hmE, kSensE, s.hm_E / m.E);
+        set_d(p.hmG, kSensE, s.hm_G / m.E);
+        set_d(p.wallE, kSensE, (double)p.wallE / m.E);
+        set_d(p.wallG, kSensE, (double)p.wallG / m.E);
+      }
       p.pA = (Real)s.pot.p_A;
       p.mu = (Real)m.mu;
       p.mur = (Real)m.mur;
@@ -383,6 +458,10 @@ class Engine final : public EngineBase {
       BondLaw<Real>& l = hl[si];
       l.br_abs = m.b_r > 0 ? (Real)s.pot.b_r : Real(0);
       l.br_factor = (Real)m.bond_radius_factor;
+      if (m.b_r > 0)
+        set_d(l.br_abs, kSensBondRadius, 1.0);
+      else
+        set_d(l.br_factor, kSensBondRadius, 1.0);
       l.sn_mean = (Real)m.Ec;
       l.sn_sd = (Real)m.Ec_sd;
       l.st_mean = (Real)m.Gc;
@@ -438,6 +517,10 @@ class Engine final : public EngineBase {
       g.nz = (uint32_t)std::ceil((hi[2] - lo[2]) / a) + 1;
       g.off = off;
       off += g.nx * g.ny * g.nz;
+      g.hx = (Real)(float)s.load.hidden_point[0];
+      g.hy = (Real)(float)s.load.hidden_point[1];
+      g.hz = (Real)(float)s.load.hidden_point[2];
+      g.skip_hidden = (s.load.space_half[0] > 0 && s.load.space_half[1] > 0 && s.load.space_half[2] > 0) ? 1u : 0u;
     }
     ncell_ = off;
     CK(grids_.alloc(S));
@@ -721,6 +804,7 @@ class Engine final : public EngineBase {
     A.blk_stat = blk_stat_.p;
     A.stat = stat_.p;
     A.lat = lat_.p;
+    A.sfl_tan = sfl_tan_.p;
     return A;
   }
 
@@ -1075,6 +1159,71 @@ class Engine final : public EngineBase {
   }
 
   // pair record: 16 values (1/L0, prev-dir xyz, Ot xyz, Mn xyz, Mt xyz, sigma_c, tau_c, b_r)
+  // SaveLammpsDATASimple (md_savelammpsdata.cpp:9-75): LAMMPS data file of
+  // one specimen in SI units - atoms, per-atom kinetic energies (translational,
+  // rotational, total; zeros unless with_energy) and every intact bond once
+  // per direction, as the reference lists its bonded slots (type 2).  The box
+  // is the escape box (the reference's S.A, S.B); masses and inertias are per
+  // sphere (the reference's single p_m, p_I for equal radii).
+  int save_lammps(int32_t si, const char* path, int with_energy) override {
+    if (si < 0 || (size_t)si >= samples_.size() || !path) return DEM_ERR_ARG;
+    if (!setup_done_) return DEM_ERR_STATE;
+    const SampleHost& s = samples_[si];
+    const uint32_t n = s.n;
+    std::vector<double> R(3 * (size_t)n), V(3 * (size_t)n), W(3 * (size_t)n);
+    RC(get_particles_t<double>(si, R.data(), V.data(), W.data(), nullptr, nullptr, nullptr));
+    uint32_t np = 0;
+    RC(get_pairs(si, 0, nullptr, nullptr, nullptr, nullptr, &np));
+    std::vector<uint32_t> pi(np), pj(np), pk(np);
+    RC(get_pairs(si, np, pi.data(), pj.data(), pk.data(), nullptr, &np));
+    std::vector<std::vector<uint32_t>> nb(n);
+    size_t nbond = 0;
+    for (uint32_t k = 0; k < np; ++k)
+      if (pk[k] == 1) {
+        nb[pi[k]].push_back(pj[k]);
+        nb[pj[k]].push_back(pi[k]);
+        nbond += 2;
+      }
+    const double length_const = 1e-3, mass_const = 1e-6, time_const = 1e-6;
+    const double energy_const = mass_const * length_const / (time_const * time_const) * length_const;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return DEM_ERR_IO;
+    const dem_loading& L = s.load;
+    std::fprintf(f, "LAMMPS Description T0=%g  (1st line of file)\n\n", s.dt);
+    std::fprintf(f, "%u atoms\n%zu bonds\n0 angles\n0 dihedrals\n0 impropers\n1 atom types\n2 bond types\n", n,
+                 nbond);
+    const char* ax[3] = {"x", "y", "z"};
+    for (int d = 0; d < 3; ++d)
+      std::fprintf(f, "%g %g %slo %shi\n", (L.space_center[d] - L.space_half[d]) * length_const,
+                   (L.space_center[d] + L.space_half[d]) * length_const, ax[d], ax[d]);
+    std::fprintf(f, "Masses\n\n1 1\nBond Coeffs\n\n2 1 2\n\nAtoms\n\n");
+    for (uint32_t i = 0; i < n; ++i)
+      std::fprintf(f, "%u 1 %g %g %g\n", i + 1, R[i] * length_const, R[n + i] * length_const,
+                   R[2 * (size_t)n + i] * length_const);
+    std::fprintf(f, "Velocities\n\n");
+    for (uint32_t i = 0; i < n; ++i) {
+      double Et = 0, Er = 0;
+      if (with_energy) {
+        double m, dtm, dtI;
+        particle_constants(s.rad[i], s.mat.rho, s.dt, m, dtm, dtI);
+        const double I = 0.4 * m * (double)s.rad[i] * s.rad[i];
+        const double v2 = V[i] * V[i] + V[n + i] * V[n + i] + V[2 * (size_t)n + i] * V[2 * (size_t)n + i];
+        const double w2 = W[i] * W[i] + W[n + i] * W[n + i] + W[2 * (size_t)n + i] * W[2 * (size_t)n + i];
+        Et = 0.5 * m * v2 * energy_const;
+        Er = 0.5 * I * w2 * energy_const;
+      }
+      std::fprintf(f, "%u %g %g %g\n", i + 1, Et, Er, Et + Er);
+    }
+    std::fprintf(f, "\nBonds\n\n");
+    size_t k = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+      std::sort(nb[i].begin(), nb[i].end());
+      for (uint32_t j : nb[i]) std::fprintf(f, "%zu 2 %u %u\n", k++, i + 1, j + 1);
+    }
+    const bool ok = std::fclose(f) == 0;
+    return ok ? DEM_OK : DEM_ERR_IO;
+  }
+
   int get_pairs(int32_t si, uint32_t cap, uint32_t* oi, uint32_t* oj, uint32_t* kind, float* st, uint32_t* n) override {
     if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
     RC(prepare());
@@ -1167,7 +1316,7 @@ class Engine final : public EngineBase {
         const size_t q = it - bij.begin();
         const bool was = par[q].x > 0;
         const bool now = kind[k] == 1;
-        const Real il = (Real)std::fabs(v[0]) > 0 ? (Real)std::fabs(v[0]) : std::fabs(par[q].x);
+        const Real il = std::fabs(v[0]) > 0 ? (Real)std::fabs(v[0]) : (par[q].x < 0 ? -par[q].x : par[q].x);
         par[q].x = now ? il : -il;
         if (was != now) delta[si] += now ? 1 : -1;
         s0[q] = make4(v[1], v[2], v[3], v[4]);
@@ -1335,6 +1484,8 @@ class Engine final : public EngineBase {
   std::vector<std::unique_ptr<DBuf<uint32_t>>> rec_bonds_;
   std::vector<std::unique_ptr<DBuf<double>>> rec_lat_;
   DBuf<uint8_t> lat_;
+  std::vector<uint8_t> hlat_;
+  DBuf<double> sfl_tan_;
 };
 
 EngineBase* make_engine(const dem_options& o, int* err) {
@@ -1342,6 +1493,10 @@ EngineBase* make_engine(const dem_options& o, int* err) {
   int rc = DEM_OK;
   if (o.precision == 1) {
     auto* x = new Engine<double>(o);
+    rc = x->init();
+    e = x;
+  } else if (o.precision == 2) {
+    auto* x = new Engine<Dual<kSensCount>>(o);
     rc = x->init();
     e = x;
   } else {
@@ -1365,7 +1520,7 @@ int ref_grid_bin(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny
   std::vector<float4> h(n);
   for (uint32_t i = 0; i < n; ++i) h[i] = make_float4(xyz[i], xyz[n + i], xyz[2 * n + i], 0.f);
   ncell = nx * ny * nz;
-  Grid<float> g{0.f, 0.f, 0.f, (float)(1.0 / (double)a), nx, ny, nz, 0};
+  Grid<float> g{0.f, 0.f, 0.f, (float)(1.0 / (double)a), nx, ny, nz, 0, 0.f, 0.f, 0.f, 0u};
   if (pos.alloc(n) || sid.alloc(n) || grid.alloc(1) || cell_of.alloc(n) || cstart.alloc(ncell + 1) || clist.alloc(n))
     return DEM_ERR_CUDA;
   if (pos.upload(h.data(), n) || grid.upload(&g, 1)) return DEM_ERR_CUDA;

@@ -30,6 +30,8 @@ class EngineBase {
   virtual int result(int32_t sample, dem_result* out) = 0;
   virtual int get_record(int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n) = 0;
   virtual int get_lateral_record(int32_t sample, double* lat, uint32_t cap, uint32_t* n) = 0;
+  virtual int sensitivities(int32_t sample, dem_sensitivity* out) = 0;
+  virtual int save_lammps(int32_t sample, const char* path, int with_energy) = 0;
   virtual int get_particles(int32_t s, float* R, float* V, float* W, float* F, float* M, float* O) = 0;
   virtual int get_particles_d(int32_t s, double* R, double* V, double* W, double* F, double* M, double* O) = 0;
   virtual int set_particles(int32_t s, const float* R, const float* V, const float* W, const float* O) = 0;

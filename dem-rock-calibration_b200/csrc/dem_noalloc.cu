@@ -129,7 +129,7 @@ int ref_cells_static(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_
   uint32_t* tmp1 = at<uint32_t>(s, kLayout.tmp1);
   uint32_t* tmp2 = at<uint32_t>(s, kLayout.tmp2);
   Grid<float>* grid = at<Grid<float>>(s, kLayout.grid);
-  const Grid<float> g{0.f, 0.f, 0.f, (float)(1.0 / (double)a), nx, ny, nz, 0};
+  const Grid<float> g{0.f, 0.f, 0.f, (float)(1.0 / (double)a), nx, ny, nz, 0, 0.f, 0.f, 0.f, 0u};
   // what must start at zero: the per-particle grid id (one grid) and the cell counters
   if (cudaMemsetAsync(sid, 0, n * sizeof(uint32_t), st) != cudaSuccess ||
       cudaMemsetAsync(count, 0, (ncell + 1) * sizeof(uint32_t), st) != cudaSuccess ||

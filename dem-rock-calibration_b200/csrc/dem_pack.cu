@@ -111,6 +111,8 @@ class Packer {
     g.ny = g.nx;
     g.nz = (uint32_t)std::ceil((2 * P.half_height + 2 * a) / a) + 1;
     g.off = 0;
+    g.hx = g.hy = g.hz = 0.f;
+    g.skip_hidden = 0;  // nothing is parked while packing
     ncell = g.nx * g.ny * g.nz;
     CKP(grid.alloc(1));
     CKP(cudaMemcpy(grid.p, &g, sizeof(g), cudaMemcpyHostToDevice));

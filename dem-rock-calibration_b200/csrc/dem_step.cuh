@@ -55,7 +55,15 @@ struct StepArgs {
   float* blk_stat;  // per block: max |v|^2 and max displacement^2 since the last list build
   float* stat;      // running maxima over blocks and steps (reset by the host)
   const uint8_t* lat;  // per particle: 1 = on the lateral surface near mid-height (or null)
+  double* sfl_tan;     // sensitivity build only: per sample the platen-force tangents (see dem_dual.cuh)
 };
+
+// Hooks of the sensitivity build (dem_dual.cuh overloads them for dual
+// numbers); for float and double they do nothing.
+template <class Real>
+__device__ __forceinline__ void tangent_wall(const StepArgs<Real>&, uint32_t, int, const Real&) {}
+template <class Real>
+__device__ __forceinline__ void tangent_step_end(const StepArgs<Real>&, const SampleCtl&, uint32_t) {}
 
 // Hertz-Mindlin contact of pair (i, j) seen from i (n points from i to j), in
 // the polydisperse form that reduces bit for bit to dd_Calculate_fijn_ppHM_2 /
@@ -550,12 +558,16 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
           Real o[3] = {o4.x, o4.y, o4.z};
           const Real ri = x.w, mi = A.mass[p];
           if (wtop - r[ax] < ri) {
-            st = -(double)wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
+            const Real f = wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
+            st = -(double)f;
+            tangent_wall(A, s, 1, f);
           } else {
             o[0] = o[1] = o[2] = Real(0);
           }
           if (r[ax] - wbot < ri) {
-            sb = -(double)wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
+            const Real f = wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
+            sb = -(double)f;
+            tangent_wall(A, s, 0, f);
           } else {
             o[0] = o[1] = o[2] = Real(0);
           }
@@ -674,7 +686,10 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   __threadfence();
   for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
     SampleCtl& C = A.ctl[s];
-    if (!C.done) controller_step(C);
+    if (!C.done) {
+      tangent_step_end(A, C, s);
+      controller_step(C);
+    }
   }
   float a = 0.f, b = 0.f;
   for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {

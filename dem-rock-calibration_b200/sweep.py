@@ -56,15 +56,21 @@ def material_for(p: dict, r_min: float, r_mean: float, seed: int) -> Material:
 
 
 def cylinder(n: int, seed: int, r_min: float = 0.20, r_max: float = 0.30, packing: float = 0.58,
-             aspect: float = 2.0, device: int = 0) -> tuple[np.ndarray, np.ndarray, dict, float, float]:
-    """A packed cylinder of about n spheres (height = aspect x diameter)."""
+             aspect: float = 2.0, device: int = 0):
+    """A packed cylinder of about n spheres (height = aspect x diameter),
+    placed at the centre of its reference-style escape box.  Returns
+    (xyz, radii, pack report, escape box, size_real, center_real)."""
     # n (4/3) pi <r^3> = packing * pi R^2 * (2 aspect R)
     R = (n * (2.0 / 3.0) * mean_r3(r_min, r_max) / (packing * aspect)) ** (1.0 / 3.0)
     half_h = aspect * R
-    xyz, rad, rep = create_cylinder_sample((0.0, 0.0, 0.0), R, half_h, n, r_min, r_max, seed=seed, growth_stages=30,
-                                           steps_per_stage=150, max_fire_steps=6000, overlap_tol=2e-3,
-                                           device=device)
-    return xyz, rad, rep, R, half_h
+    space_si = (2 * R * 1.3e-3, 2 * R * 1.3e-3, 2 * half_h * 1.5e-3)
+    lsi = (2 * R * 1e-3, 2 * R * 1e-3, 2 * half_h * 1e-3)
+    box = reference_space(space_si, lsi, r_max, 3.2)
+    xyz, rad, rep = create_cylinder_sample(box.center.astype(np.float64), R, half_h, n, r_min, r_max, seed=seed,
+                                           growth_stages=30, steps_per_stage=150, max_fire_steps=6000,
+                                           overlap_tol=2e-3, device=device)
+    size_real, center_real = bounding_box(xyz, rad.size, float(rad.max()))
+    return xyz, rad, rep, box, size_real, center_real
 
 
 @dataclass
@@ -98,12 +104,7 @@ def build_sweep(n_cases: int, sizes: list[int], seed: int = 1, velocity_m_s: flo
     velocity_m_s until the peak has passed (70% of it) or 1% strain."""
     specs = []
     for k, n in enumerate(sizes):
-        xyz, rad, rep, R, half_h = cylinder(n, seed * 1000 + k, device=device)
-        r_max = float(rad.max())
-        space_si = (2 * R * 1.3e-3, 2 * R * 1.3e-3, 2 * half_h * 1.5e-3)
-        lsi = (2 * R * 1e-3, 2 * R * 1e-3, 2 * half_h * 1e-3)
-        box = reference_space(space_si, lsi, r_max, 3.2)
-        size_real, center_real = bounding_box(xyz, rad.size, r_max)
+        xyz, rad, rep, box, size_real, center_real = cylinder(n, seed * 1000 + k, device=device)
         specs.append((xyz, rad, box, size_real, center_real))
     sw = Sweep()
     for k, p in enumerate(latin_hypercube(n_cases, seed)):

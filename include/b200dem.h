@@ -57,7 +57,7 @@ extern "C" {
 typedef struct dem_ctx dem_ctx;
 
 typedef struct {
-  int precision;          /* 0: FP32, 1: FP64 */
+  int precision;          /* 0: FP32, 1: FP64, 2: FP64 with tangents (dem_sensitivities) */
   int device;             /* CUDA device ordinal */
   uint32_t pair_block;    /* ignored: the pair kernel runs 256-thread blocks */
   uint32_t pair_grid;     /* blocks of the pair kernel (0: all co-resident blocks) */
@@ -65,7 +65,7 @@ typedef struct {
   uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
   double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.25) */
   uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
-                               (1..4; 0: 3 for FP32, 2 for FP64) */
+                               (1..4; 0: 3 for FP32, 2 for FP64, 1 for the sensitivity build) */
   uint32_t reserved;
 } dem_options;
 
@@ -166,6 +166,30 @@ int dem_sample_result(dem_ctx* ctx, int32_t sample, dem_result* out);
 /* Loading record: 3 doubles per entry (strain, sigma_bottom, sigma_top in GPa)
  * and bonded directed-slot counts, as the reference's h_sFL / h_sSI. */
 int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, uint32_t cap, uint32_t* n);
+/* Secant modulus and secant Poisson ratio of a uniaxial specimen at the last
+ * completed step (no counterpart in the reference).  With precision 2 (the
+ * sensitivity build: FP64 values carried with their derivatives with respect
+ * to DEM_SENS_COUNT micro-parameters, forward mode) also their derivatives;
+ * other precisions leave the derivative arrays zero.  The time step is held
+ * fixed: set dem_material.dt explicitly when comparing with finite
+ * differences. */
+#define DEM_SENS_E_BOND 0        /* dem_material.E_bond */
+#define DEM_SENS_KN_KS 1         /* dem_material.kn_ks */
+#define DEM_SENS_BOND_RADIUS 2   /* bond_radius_factor (or the absolute b_r when b_r > 0) */
+#define DEM_SENS_E 3             /* particle E (contacts, platens) */
+#define DEM_SENS_RHO 4           /* density */
+#define DEM_SENS_COUNT 5
+typedef struct {
+  double strain;                 /* axial strain at the last step, compression positive */
+  double stress;                 /* platen stress of the last step, GPa */
+  double E_secant;               /* stress / strain */
+  double nu_secant;              /* lateral / axial strain (uniaxial specimens; NaN otherwise) */
+  double dstress[DEM_SENS_COUNT];
+  double dE[DEM_SENS_COUNT];
+  double dnu[DEM_SENS_COUNT];
+} dem_sensitivity;
+int dem_sensitivities(dem_ctx* ctx, int32_t sample, dem_sensitivity* out);
+
 /* Lateral record of a uniaxial specimen (no counterpart in the reference): per
  * loading-record entry the mean radial distance (mm) of the particles on the
  * lateral surface near mid-height; *n = 0 for specimens without one. */
@@ -238,6 +262,10 @@ int dem_calculation_test(const dem_options* opt, const dem_material* mat, const 
 int dem_load_cylinder_sample(const char* path, double p_r, float* xyz, uint32_t cap, uint32_t* n,
                              double size_real[3], double center_real[3]);
 int dem_save_cylinder_sample(const char* path, const float* xyz, uint32_t n, const double hidden_point[3]);
+/* LAMMPS data file of one specimen (SaveLammpsDATASimple, md_savelammpsdata.cpp:9-75):
+ * atoms in metres, per-atom kinetic energies when with_energy != 0, intact
+ * bonds once per direction (type 2). */
+int dem_save_lammps_data(dem_ctx* ctx, int32_t sample, const char* path, int with_energy);
 /* "EpsZ StressZ_bottom StressZ_top" file of SaveSumForcesLoading (stresses in Pa). */
 int dem_save_sum_forces_loading(const char* path, const double* rec, uint32_t n);
 

@@ -80,12 +80,14 @@ def test_solve_parameters_skip_unvaried_rows():
 
 @pytest.mark.gpu
 def test_cg_step_runs_its_solves_in_one_context(tmp_path):
-    """Two CG steps on a small reference-mode cylinder: six uniaxial solves per
-    step in one batched context (bounded to 3000 steps each), then the update."""
+    """Two CG steps on a small reference-mode cylinder (about 800 spheres of
+    0.5 mm): six uniaxial solves per step in one batched context (bounded to
+    3000 steps each), then the update."""
     import dem_testlib as T
     from test_gpu_parity import _loading
 
-    c = T.ref_case(seed=2, lsi=(0.0045, 0.0045, 0.007), space=(0.009, 0.009, 0.013), jitter_frac=0.1,
+    # p_r 0.5 mm: the particle radius SetVariationParameters uses
+    c = T.ref_case(seed=2, lsi=(0.009, 0.009, 0.014), space=(0.018, 0.018, 0.026), p_r_si=0.5e-3, jitter_frac=0.1,
                    lattice_gap=0.5)
     uni = cal.Specimen(xyz=c.R, loading=_loading(c))
     p0 = np.array([30.0, 0.040, 0.040, 0.2, 0.025])  # E, Ec, Gc (GPa), b_r, gap (mm)

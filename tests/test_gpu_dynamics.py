@@ -168,3 +168,30 @@ def test_uniaxial_peak_statistics_match_reference_driver(tmp_path):
     assert abs(m["ucs"][0] - m["ucs"][1]) <= 0.08 * m["ucs"][1], m
     assert abs(m["eps"][0] - m["eps"][1]) <= 0.08 * m["eps"][1], m
     assert abs(m["E"][0] - m["E"][1]) <= 0.03 * m["E"][1], m
+
+
+def test_lammps_data_file(tmp_path):
+    """SaveLammpsDATASimple's format: header counts, atoms in metres, every
+    intact bond once per direction with type 2."""
+    c = T.ref_case(seed=5, **SMALL)
+    ctx = dem.Context()
+    sid = ctx.add_sample(_material(c), _loading(c), c.R)
+    ctx.setup()
+    ctx.step(20)
+    path = tmp_path / "dump.data"
+    ctx.save_lammps_data(str(path), sid, with_energy=True)
+    r = ctx.result(sid)
+    p = ctx.particles(sid)
+    ctx.close()
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith("LAMMPS Description T0=")
+    assert lines[2] == f"{c.N} atoms" and lines[3] == f"{2 * r['bonds_now']} bonds"
+    a = lines.index("Atoms") + 2
+    atoms = np.array([list(map(float, l.split()[2:5])) for l in lines[a:a + c.N]])
+    R = p["R"].reshape(3, -1).T.astype(np.float64) * 1e-3
+    assert np.allclose(atoms, R, rtol=1e-5, atol=1e-9)
+    b = lines.index("Bonds") + 2
+    bonds = [tuple(map(int, l.split())) for l in lines[b:]]
+    assert len(bonds) == 2 * r["bonds_now"] and all(t == 2 for _, t, _, _ in bonds)
+    pairs = {(i, j) for _, _, i, j in bonds}
+    assert all((j, i) in pairs for i, j in pairs)

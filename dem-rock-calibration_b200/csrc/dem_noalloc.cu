@@ -1,15 +1,24 @@
 // dem_ref_cells_static: the cell binning of dem_ref_cells (CellDistribution,
-// md_cell_distribution.cu:130-172) run out of one file-scope device array
-// instead of per-call device buffers.  The call allocates nothing, neither on
-// the device nor on the host: the scratch array's address is looked up once per
-// device with cudaGetSymbolAddress, the input and the three outputs are copied
-// straight between the caller's host buffers and sub-ranges of the array, and
-// the reference layouts (CIs, pnC) are produced on the device.
+// md_cell_distribution.cu:130-172) for callers that cannot allocate GPU memory
+// - cudaMalloc/cudaFree may synchronise the whole device and stall the other
+// streams of a serving process, they fail when another framework's caching
+// allocator holds most of the memory, and some host frameworks forbid a
+// plug-in its own allocations.  It runs out of one file-scope device array
+// instead of per-call buffers and allocates nothing, neither on the device nor
+// on the host: the input and the three outputs are copied straight between
+// the caller's host buffers and sub-ranges of the array, and the reference
+// layouts (CIs, pnC) are produced on the device.
+//
+// Set-up: host code cannot use the array's name as a device address, so the
+// first call on each device looks the address up with cudaGetSymbolAddress
+// (that device current) and caches it; that first call should come before
+// any stream capture.
 //
 // Limits: n <= DEM_STATIC_MAX_PARTICLES particles and nx*ny*nz <=
 // DEM_STATIC_MAX_CELLS cells; larger calls return DEM_ERR_CAPACITY before any
-// device work.  The array is shared by every call on a device, so calls that
-// overlap in time on the same device (two host threads) race on it; callers
+// device work.  The array keeps the last call's contents and is shared by
+// every call on a device: what must start at zero is cleared per call, and
+// calls that overlap on the GPU (two host threads) race on it, so callers
 // serialise them.
 #include <cuda_runtime.h>
 
@@ -64,7 +73,8 @@ constexpr int kMaxDevices = 64;
 std::mutex g_addr_mu;
 unsigned char* g_addr[kMaxDevices] = {};
 
-// Device address of g_scratch on the current device (looked up on first use).
+// Device address of g_scratch on the current device: looked up with
+// cudaGetSymbolAddress on the first call on that device, then cached.
 int scratch_address(unsigned char** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DEM_ERR_CUDA;

@@ -234,15 +234,22 @@ int dem_ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t n
 int dem_ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz,
                           float add_thr, float del_thr, uint32_t cap, uint32_t* sets, uint32_t* overflow);
 
-/* dem_ref_cells without any allocation (no counterpart in the reference: the
- * reference's CellDistribution works on buffers its caller allocated).  Same
- * arguments and outputs as dem_ref_cells; the device work runs out of one
- * file-scope device array of DEM_STATIC_SCRATCH_BYTES per device, whose
- * address is looked up once per device with cudaGetSymbolAddress.  Returns
- * DEM_ERR_CAPACITY when n > DEM_STATIC_MAX_PARTICLES or nx*ny*nz >
- * DEM_STATIC_MAX_CELLS.  Calls on the same device share that array: calls
- * that overlap in time (several host threads) race on it and must be
- * serialised by the caller. */
+/* dem_ref_cells for callers that cannot allocate GPU memory (no counterpart
+ * in the reference, whose CellDistribution bins into buffers its driver
+ * allocated).  cudaMalloc and cudaFree may synchronise the whole device and so
+ * stall every other stream of a serving process, they fail once another
+ * framework's caching allocator holds most of the device memory, and some
+ * host frameworks do not let a plug-in allocate on its own; such callers use
+ * this entry point.  Same arguments and outputs as dem_ref_cells, and it calls
+ * no allocating routine: the device work runs out of one file-scope device
+ * array of DEM_STATIC_SCRATCH_BYTES (4.5 MiB), which every GPU that loads the
+ * library holds until the process exits.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress, with that device
+ * current) and keeps it; make that first call before any stream capture.
+ * Returns DEM_ERR_CAPACITY, before any device work, when n >
+ * DEM_STATIC_MAX_PARTICLES or nx*ny*nz > DEM_STATIC_MAX_CELLS.  All calls on
+ * a device share the array: calls that overlap on the GPU (several host
+ * threads) race on it and must be serialised by the caller. */
 #define DEM_STATIC_MAX_PARTICLES 65536u
 #define DEM_STATIC_MAX_CELLS 65536u
 #define DEM_STATIC_SCRATCH_BYTES 4718592u /* 4.5 MiB */

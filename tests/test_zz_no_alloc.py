@@ -1,4 +1,6 @@
-"""dem_ref_cells_static (the binning entry point that allocates nothing)
+"""dem_ref_cells_static, the binning entry point for callers that cannot
+allocate GPU memory (cudaMalloc/cudaFree may synchronise the device, fail
+under another framework's caching allocator, or be forbidden to a plug-in),
 against dem_ref_cells on the same inputs.
 
 Two calls in a row on different specimens (the larger first, so counters left

@@ -79,12 +79,13 @@ class PackParams(C.Structure):
                 ("r_min", C.c_double), ("r_max", C.c_double), ("E", C.c_double), ("nu", C.c_double),
                 ("rho", C.c_double), ("overlap_tol", C.c_double), ("n", C.c_uint32), ("growth_stages", C.c_uint32),
                 ("steps_per_stage", C.c_uint32), ("max_fire_steps", C.c_uint32), ("seed", C.c_uint64),
-                ("device", C.c_int), ("fire_variant", C.c_int)]
+                ("device", C.c_int), ("fire_variant", C.c_int), ("max_removed", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class PackReport(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("max_overlap", C.c_double), ("packing_fraction", C.c_double),
-                ("rebuilds", C.c_uint32), ("reserved", C.c_uint32)]
+                ("rebuilds", C.c_uint32), ("removed", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -136,6 +137,7 @@ def _declare(L):
     L.dem_save_lammps_data.argtypes = [_vp, C.c_int32, C.c_char_p, C.c_int]
     L.dem_sensitivities.argtypes = [_vp, C.c_int32, P(Sensitivity)]
     L.dem_get_lateral_record.argtypes = [_vp, C.c_int32, _vp, _u32, P(_u32)]
+    L.dem_reference_space.argtypes = [_vp, _vp, C.c_double, C.c_double, P(Loading)]
     L.dem_ref_cells.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_cells_static.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, _vp, _vp, _vp]
     L.dem_ref_neighbor_sets.argtypes = [_vp, _u32, C.c_float, _u32, _u32, _u32, C.c_float, C.c_float, _u32, _vp,
@@ -465,12 +467,14 @@ def calculation_test(mat: Material, load: Loading, xyz: np.ndarray, radii=None, 
 def create_cylinder_sample(center, radius: float, half_height: float, n: int, r_min: float, r_max: float,
                            E: float = 50.0, nu: float = 0.25, rho: float = 2.65, overlap_tol: float = 1e-3,
                            growth_stages: int = 40, steps_per_stage: int = 200, max_fire_steps: int = 20000,
-                           seed: int = 1, device: int = 0, fire_variant: int = 0):
+                           seed: int = 1, device: int = 0, fire_variant: int = 0, max_removed: int = 0):
     """Seeded packed cylinder (h_CreateCylinderSample): returns xyz (SoA), radii, report.
-    fire_variant 0 relaxes with inertial FIRE 2.0, 1 with the reference's FIRE update."""
+    fire_variant 0 relaxes with inertial FIRE 2.0, 1 with the reference's FIRE update;
+    max_removed > 0 lets it remove spheres of the worst overlaps (fewer than n are returned)."""
     p = PackParams(radius=radius, half_height=half_height, r_min=r_min, r_max=r_max, E=E, nu=nu, rho=rho,
                    overlap_tol=overlap_tol, n=n, growth_stages=growth_stages, steps_per_stage=steps_per_stage,
-                   max_fire_steps=max_fire_steps, seed=seed, device=device, fire_variant=fire_variant)
+                   max_fire_steps=max_fire_steps, seed=seed, device=device, fire_variant=fire_variant,
+                   max_removed=max_removed)
     for d in range(3):
         p.center[d] = float(center[d])
     xyz = np.zeros(3 * n, np.float32)
@@ -479,8 +483,10 @@ def create_cylinder_sample(center, radius: float, half_height: float, n: int, r_
     rep = PackReport()
     _ck(_lib().dem_create_cylinder_sample(C.byref(p), _p(xyz), _p(rad), n, C.byref(m), C.byref(rep)),
         "dem_create_cylinder_sample")
-    return xyz, rad, dict(steps=rep.steps, max_overlap=rep.max_overlap, packing_fraction=rep.packing_fraction,
-                          rebuilds=rep.rebuilds)
+    k = m.value
+    return np.ascontiguousarray(xyz[:3 * k]), rad[:k].copy(), dict(
+        steps=rep.steps, max_overlap=rep.max_overlap, packing_fraction=rep.packing_fraction, rebuilds=rep.rebuilds,
+        removed=rep.removed)
 
 
 def load_cylinder_sample(path: str, p_r: float):

@@ -18,6 +18,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 SRC = PKG / "csrc"
 OUT = PKG / "libb200dem.so"
+CLI = PKG / "rockfit-dem"  # the reference's command line over the library (csrc/rockfit_cli.cpp)
 
 SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_noalloc.cu", "dem_capi.cpp"]
 HEADERS = ["dem_common.cuh", "dem_dual.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
@@ -44,8 +45,8 @@ def stale() -> bool:
     if not OUT.exists():
         return True
     t = OUT.stat().st_mtime
-    deps = [SRC / s for s in SOURCES + HEADERS] + [ROOT / "include" / "b200dem.h"]
-    return any(p.stat().st_mtime > t for p in deps)
+    deps = [SRC / s for s in SOURCES + HEADERS + ["rockfit_cli.cpp"]] + [ROOT / "include" / "b200dem.h"]
+    return not CLI.exists() or any(p.stat().st_mtime > t for p in deps)
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
@@ -64,7 +65,21 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("libb200dem build failed")
     os.replace(str(OUT) + ".tmp", OUT)
+    build_cli()
     return OUT
+
+
+def build_cli() -> Path:
+    """rockfit-dem, linked against the in-tree library (rpath $ORIGIN)."""
+    gxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+    cmd = [gxx, "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(SRC / "rockfit_cli.cpp"), "-o", str(CLI) + ".tmp",
+           "-L", str(PKG), "-lb200dem", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("rockfit-dem build failed")
+    os.replace(str(CLI) + ".tmp", CLI)
+    return CLI
 
 
 if __name__ == "__main__":

@@ -44,6 +44,27 @@ const char* dem_strerror(int code) {
 
 const char* dem_last_error_detail(void) { return dem::last_error_detail(); }
 
+int dem_reference_space(const double space_si[3], const double lsi_si[3], double p_r, double farcut, dem_loading* out) {
+  if (!space_si || !lsi_si || !out || !(p_r > 0) || !(farcut > 0)) return DEM_ERR_ARG;
+  // sample_data::SetSpaceSizeSi / SetLSi / CalculateParameters (md_data_types.h:87-123):
+  // float members, cell edge C.a = 2 a_farcut; the escape box does not depend on LSi
+  const float Ca = (float)(2.0 * farcut * p_r);
+  float size[3], half[3], A[3], Bv[3];
+  for (int d = 0; d < 3; ++d) {
+    size[d] = (float)(space_si[d] / 1e-3);
+    half[d] = (float)(0.5 * (double)size[d]);
+    A[d] = (float)(1.01 * (double)Ca);
+    Bv[d] = A[d] + size[d];
+    out->space_center[d] = (float)(0.5 * (double)(float)(A[d] + Bv[d]));
+    out->space_half[d] = half[d];
+  }
+  out->hidden_point[0] = (float)((double)A[0] + 0.5 * (double)size[0]);
+  out->hidden_point[1] = (float)((double)A[1] + 0.5 * (double)size[1]);
+  out->hidden_point[2] = (float)(((double)(float)std::floor((float)((double)Bv[2] / (double)Ca)) + 3 - 0.5) * (double)Ca);
+  out->zcut = (float)((float)out->space_center[2] + half[2]);
+  return DEM_OK;
+}
+
 int dem_device_count(int* n) {
   int c = 0;
   if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;

@@ -892,7 +892,8 @@ class Engine final : public EngineBase {
   uint64_t chunk_steps(const Flags& f) const {
     const double budget = 0.5 * min_skin_ - std::sqrt((double)f.d2max);
     const double v = std::sqrt((double)f.v2max);
-    if (!(v > 0)) return opt_.graph_steps;
+    // no speed seen yet (the first chunk after set-up): a short chunk measures it
+    if (!(v > 0)) return std::min<uint64_t>(opt_.graph_steps, 16);
     const double k = 0.5 * budget / (v * max_dt_);
     if (!(k >= 1.0)) return 1;
     return (uint64_t)std::min<double>(k, opt_.graph_steps);

@@ -61,12 +61,13 @@ class Packer {
   explicit Packer(const dem_pack_params& p) : P(p) {}
 
   int run(float* xyz, float* radii, uint32_t cap, uint32_t* n_out, dem_pack_report* rep) {
+    n_ = P.n;
     CKP(cudaSetDevice(P.device));
     CKP(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P.device);
     nsm = (uint32_t)sms;
-    const uint32_t n = P.n;
+    const uint32_t n = n_;
     if (n == 0 || n > cap || !(P.r_max >= P.r_min) || !(P.r_min > 0) || !(P.radius > P.r_max) ||
         !(P.half_height > P.r_max))
       return DEM_ERR_ARG;
@@ -135,6 +136,7 @@ class Packer {
                          (float)P.half_height};
     CKP(cudaMemcpy(cyl.p, cy, sizeof(cy), cudaMemcpyHostToDevice));
     CKP(fire.alloc(1));
+    CKP(povl.alloc(n));
     CKP(blocks_done.alloc(1));
     CKP(scan_tmp.alloc(2 * cdiv(std::max(ncell, n), kScanBlock) + 2048));
     // linear repulsion stiffness ~ E * r (force per overlap)
@@ -180,23 +182,39 @@ class Packer {
     CKP(cudaMemcpy(scale.p, &one, sizeof(float), cudaMemcpyHostToDevice));
     int rc = relax(false, 0.f, P.max_fire_steps, P.overlap_tol, steps);
     if (rc) return rc;
-    // results
-    CKP(cudaMemcpy(hp.data(), pos.p, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
+    // the reference's d_ReduceParticleNumber (md_reduceparticlenumber.cu:18-38,
+    // md_createcylindersample.cu:323-338, 402-417): while the largest overlap
+    // stays above the tolerance, remove the spheres of the worst overlaps and
+    // relax again
+    uint32_t removed = 0;
+    while (P.max_removed && last_overlap >= P.overlap_tol && removed < P.max_removed) {
+      const uint32_t before = removed;
+      rc = remove_worst(P.max_removed - removed, removed);
+      if (rc) return rc;
+      if (removed == before) break;
+      rc = relax(false, 0.f, std::max(P.max_fire_steps / 4, 500u), P.overlap_tol, steps);
+      if (rc) return rc;
+    }
+    // results (the spheres kept, first nf entries of each SoA block)
+    const uint32_t nf = n_;
+    hp.resize(nf);
+    CKP(cudaMemcpy(hp.data(), pos.p, nf * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nf; ++i) {
       xyz[i] = hp[i].x;
-      xyz[n + i] = hp[i].y;
-      xyz[2 * n + i] = hp[i].z;
+      xyz[nf + i] = hp[i].y;
+      xyz[2 * nf + i] = hp[i].z;
       if (radii) radii[i] = hp[i].w;
     }
-    *n_out = n;
+    *n_out = nf;
     if (rep) {
       std::memset(rep, 0, sizeof(*rep));
       rep->steps = steps;
       rep->max_overlap = last_overlap;
       double vs = 0;
-      for (uint32_t i = 0; i < n; ++i) vs += 4.0 / 3.0 * kPiD * std::pow((double)hp[i].w, 3);
+      for (uint32_t i = 0; i < nf; ++i) vs += 4.0 / 3.0 * kPiD * std::pow((double)hp[i].w, 3);
       rep->packing_fraction = vs / (kPiD * P.radius * P.radius * 2.0 * P.half_height);
       rep->rebuilds = rebuilds;
+      rep->removed = removed;
     }
     cudaStreamDestroy(st);
     return DEM_OK;
@@ -217,8 +235,43 @@ class Packer {
     return DEM_OK;
   }
 
+  // Removes up to `budget` spheres (at most 0.1% of them per round, worst
+  // first): of the spheres whose largest overlap in the last step is above the
+  // tolerance, every second one in order of that overlap - both spheres of a
+  // pair carry its overlap - by compacting the arrays.
+  int remove_worst(uint32_t budget, uint32_t& removed) {
+    const uint32_t n = n_;
+    std::vector<float> ov(n);
+    CKP(cudaMemcpy(ov.data(), povl.p, n * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> cand;
+    for (uint32_t i = 0; i < n; ++i)
+      if (ov[i] >= P.overlap_tol) cand.push_back(i);
+    if (cand.empty()) return DEM_OK;
+    std::stable_sort(cand.begin(), cand.end(), [&](uint32_t a, uint32_t b) { return ov[a] > ov[b]; });
+    uint32_t k = (uint32_t)std::max<size_t>(1, cand.size() / 2);
+    k = std::min<uint32_t>({k, budget, std::max(1u, n / 1000)});
+    std::vector<uint8_t> gone(n, 0);
+    for (uint32_t q = 0, t = 0; q < cand.size() && t < k; q += 2, ++t) gone[cand[q]] = 1;
+    std::vector<float4> hp(n), hv(n);
+    CKP(cudaMemcpy(hp.data(), pos.p, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CKP(cudaMemcpy(hv.data(), vel.p, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < n; ++i)
+      if (!gone[i]) {
+        hp[m] = hp[i];
+        hv[m] = make_float4(0.f, 0.f, 0.f, hv[i].w);
+        ++m;
+      }
+    removed += n - m;
+    n_ = m;
+    CKP(cudaMemcpy(pos.p, hp.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
+    CKP(cudaMemcpy(vel.p, hv.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
+    CKP(cudaMemset(frc.p, 0, n * sizeof(float4)));
+    return DEM_OK;
+  }
+
   int rebuild() {
-    const uint32_t n = P.n;
+    const uint32_t n = n_;
     const uint32_t g1 = std::max(1u, std::min(cdiv(n, 256), nsm * 16));
     CKP(cudaMemsetAsync(cell_count.p, 0, (ncell + 1) * sizeof(uint32_t), st));
     k_cell_index<float><<<g1, 256, 0, st>>>(pos.p, sid.p, n, grid.p, cell_of.p, cell_count.p);
@@ -272,7 +325,7 @@ class Packer {
   // checks are sized so that the fastest particle of the previous chunk cannot
   // use up the rest of that quarter.
   int relax(bool viscous, float vis, uint32_t max_steps, double tol, uint64_t& steps) {
-    const uint32_t n = P.n;
+    const uint32_t n = n_;
     PackArgs<float> A{};
     A.pos = pos.p;
     A.vel = vel.p;
@@ -285,6 +338,7 @@ class Packer {
     A.D = Dk.p;
     A.linear = 1;
     A.fire = fire.p;
+    A.povl = P.max_removed ? povl.p : nullptr;
     A.cyl = cyl.p;
     A.nsamples = 1;
     A.blocks_done = blocks_done.p;
@@ -322,6 +376,7 @@ class Packer {
         if (k == m - 1) {
           CKP(cudaMemcpyAsync(&fire.p->max_overlap, &z, sizeof(float), cudaMemcpyHostToDevice, st));
           CKP(cudaMemcpyAsync(&fire.p->dmax2, &z, sizeof(float), cudaMemcpyHostToDevice, st));
+          if (A.povl) CKP(cudaMemsetAsync(povl.p, 0, n * sizeof(float), st));
         }
         k_soft_pairs<float><<<gp, 256, 0, st>>>(A);
         k_fire_power<float><<<gn, 256, 0, st>>>(A);
@@ -342,7 +397,7 @@ class Packer {
 
   dem_pack_params P;
   cudaStream_t st = nullptr;
-  uint32_t nsm = 148, ncell = 0;
+  uint32_t nsm = 148, ncell = 0, n_ = 0;
   double skin = 0;
   float last_overlap = 0.f;
   uint32_t rebuilds = 0;
@@ -351,7 +406,7 @@ class Packer {
   Buf<uint2> cij;
   Buf<Grid<float>> grid;
   Buf<double> skin_d;
-  Buf<float> scale, Dk, cyl;
+  Buf<float> scale, Dk, cyl, povl;
   Buf<FireCtl> fire;
   Buf<unsigned int> blocks_done;
 };

@@ -52,6 +52,7 @@ struct PackArgs {
   const Real* D;       // per sample: soft-force constant (reference Po.D) or spring stiffness
   int linear;          // 0: reference soft force, 1: linear overlap spring
   FireCtl* fire;       // per sample
+  float* povl;         // per particle: largest relative overlap of the step (null: not tracked)
   const Real* cyl;     // per sample: centre x,y,z, radius R, half height H (5 values)
   uint32_t nsamples;
   unsigned int* blocks_done;
@@ -87,6 +88,10 @@ __global__ void __launch_bounds__(256) k_soft_pairs(PackArgs<Real> A) {
     acc3(A.frc + j, -fm * dx, -fm * dy, -fm * dz);
     const float ov = (float)((a - RT<Real>::sqrt_rn(rr)) / a);
     worst = fmaxf(worst, ov);
+    if (A.povl && ov > 0.f) {
+      atomicMax(reinterpret_cast<int*>(A.povl + i), __float_as_int(ov));
+      atomicMax(reinterpret_cast<int*>(A.povl + j), __float_as_int(ov));
+    }
   }
   // block max of the relative overlap, then one atomic per block
   for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xFFFFFFFFu, worst, o));

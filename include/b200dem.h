@@ -276,6 +276,14 @@ int dem_save_lammps_data(dem_ctx* ctx, int32_t sample, const char* path, int wit
 /* "EpsZ StressZ_bottom StressZ_top" file of SaveSumForcesLoading (stresses in Pa). */
 int dem_save_sum_forces_loading(const char* path, const double* rec, uint32_t n);
 
+/* Escape box of the reference's sample set-up (sample_data::SetSpaceSizeSi,
+ * SetLSi, CalculateParameters, md_data_types.h:87-123, cell edge 2 farcut p_r):
+ * fills out->space_center, space_half, hidden_point and zcut (mm), rounded to
+ * float as the reference stores them; the rest of *out is left as it is
+ * (lsi_si is accepted for the reference's argument order; the box does not
+ * depend on it). */
+int dem_reference_space(const double space_si[3], const double lsi_si[3], double p_r, double farcut, dem_loading* out);
+
 /* Seeded sample creation (the role of h_CreateCylinderSample): n spheres with
  * radii uniform in [r_min, r_max] filled at random into a z-axis cylinder
  * (a column for the uniaxial test, a disc for the Brazilian test), grown from
@@ -297,6 +305,10 @@ typedef struct {
   uint64_t seed;
   int device;
   int fire_variant;
+  uint32_t max_removed;      /* > 0: remove up to this many spheres of the worst overlaps while the largest
+                                overlap stays >= overlap_tol (the reference's d_ReduceParticleNumber);
+                                *n then returns the spheres kept */
+  uint32_t reserved;
 } dem_pack_params;
 
 typedef struct {
@@ -304,7 +316,7 @@ typedef struct {
   double max_overlap;        /* largest relative overlap at the end */
   double packing_fraction;   /* sphere volume / cylinder volume */
   uint32_t rebuilds;
-  uint32_t reserved;
+  uint32_t removed;          /* spheres removed (max_removed) */
 } dem_pack_report;
 
 int dem_create_cylinder_sample(const dem_pack_params* p, float* xyz, float* radii, uint32_t cap, uint32_t* n,

@@ -171,8 +171,14 @@ def cpu_baseline(spec, nsteps: int, threads: int):
     rad = spec.radii.astype(np.float32)
     r = rad.astype(np.float64)
     mass = mat.rho * (4.0 * (1.0 / 3.0) * np.pi * r ** 3)
-    dt = mat.dt_rayleigh_factor * np.pi * r.min() * np.sqrt(2.0 * mat.rho * (1.0 + mat.nu)) / (
-        np.sqrt(mat.E) * (0.163 * mat.nu + 0.8766))
+    # the engine's rule: factor * min(Rayleigh time, bond time) of the smallest sphere
+    rmin = r.min()
+    t_r = np.pi * rmin * np.sqrt(2.0 * mat.rho * (1.0 + mat.nu)) / (np.sqrt(mat.E) * (0.163 * mat.nu + 0.8766))
+    e_b = mat.E_bond if mat.E_bond > 0 else mat.E
+    g_b = e_b / mat.kn_ks if mat.kn_ks > 0 else 0.5 * e_b / (1.0 + mat.nu)
+    k_b = max(e_b, g_b) * np.pi * (mat.bond_radius_factor * rmin) ** 2 / (2.0 * rmin)
+    t_b = 2.0 * np.sqrt(mat.rho * 4.0 / 3.0 * np.pi * rmin ** 3 / k_b)
+    dt = mat.dt_rayleigh_factor * min(t_r, t_b)
     dtm = ((1.0 / mass) * dt).astype(np.float32)
     dtI = (dt / (0.4 * mass * r * r)).astype(np.float32)
     hmE = 0.5 * mat.E / (1 - mat.nu ** 2)

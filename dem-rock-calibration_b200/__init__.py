@@ -237,11 +237,18 @@ def reference_space(space_si, lsi_si, p_r: float, farcut: float = 3.2) -> SpaceB
                     Vext=Vext)
 
 
-def bounding_box(xyz: np.ndarray, n: int, p_r: float):
-    """h_LoadCylinderSample bounding box (md_createcylindersample.cu:448-465)."""
+def bounding_box(xyz: np.ndarray, n: int, p_r: float, radii=None):
+    """h_LoadCylinderSample bounding box (md_createcylindersample.cu:448-465):
+    extent of the centres plus 2 p_r and their midpoint.  With per-sphere radii
+    the extent of the spheres themselves (equal radii give the same box), so
+    polydisperse platens start on the specimen's surface."""
     x = xyz.reshape(3, n).astype(np.float64)
-    mn, mx = x.min(1), x.max(1)
-    return mx - mn + 2.0 * p_r, 0.5 * (mx + mn)
+    if radii is None:
+        mn, mx = x.min(1), x.max(1)
+        return mx - mn + 2.0 * p_r, 0.5 * (mx + mn)
+    r = np.asarray(radii, np.float64)[None, :]
+    lo, hi = (x - r).min(1), (x + r).max(1)
+    return hi - lo, 0.5 * (hi + lo)
 
 
 def loading(test: int, box: SpaceBox, size_real, center_real, velocity: float, min_stress: float, max_strain: float,

@@ -138,6 +138,11 @@ __host__ __device__ inline Dual<K> floor(const Dual<K>& a) {
 }
 
 template <int K>
+__host__ __device__ inline Dual<K> frozen(const Dual<K>& a) {
+  return Dual<K>(a.v);
+}
+
+template <int K>
 struct Dual4 {
   Dual<K> x, y, z, w;
 };

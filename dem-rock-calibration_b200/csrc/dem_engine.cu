@@ -359,11 +359,23 @@ class Engine final : public EngineBase {
     P.p_mur = m.mur;
     P.a_farcut = m.farcut * (m.p_r > 0 ? m.p_r : s.rmean);
     P.calculate();
-    s.dt = P.dt;
-    if (m.dt_rayleigh_factor > 0) s.dt = m.dt_rayleigh_factor * rayleigh_time(s.rmin, m.rho, m.E, m.nu);
-    if (m.dt > 0) s.dt = m.dt;
     s.E_b = m.E_bond > 0 ? m.E_bond : m.E;
     s.G_b = m.kn_ks > 0 ? s.E_b / m.kn_ks : 0.5 * s.E_b / (1.0 + m.nu);
+    s.dt = P.dt;
+    if (m.dt_rayleigh_factor > 0) {
+      // the reference's rule (0.05 min(T_Rayleigh, T_bond), potential_data::
+      // CalculateParameters) with the caller's factor, for the smallest sphere
+      // and the stiffest bond it can carry: T_bond = 2 sqrt(m / k), k the bond
+      // stiffness max(E_b, G_b) pi b^2 / (2 r) of a bond of that sphere
+      const double r = s.rmin;
+      const double b = m.b_r > 0 ? P.b_r : m.bond_radius_factor * r;
+      const double k = std::max(s.E_b, s.G_b) * kPiD * b * b / (2.0 * r);
+      const double mass = m.rho * 4.0 * (1.0 / 3.0) * kPiD * r * r * r;
+      double T = rayleigh_time(r, m.rho, m.E, m.nu);
+      if (k > 0) T = std::min(T, 2.0 * std::sqrt(mass / k));
+      s.dt = m.dt_rayleigh_factor * T;
+    }
+    if (m.dt > 0) s.dt = m.dt;
     s.hm_E = P.hm_E;
     s.hm_G = P.hm_G;
   }

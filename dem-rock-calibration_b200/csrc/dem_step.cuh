@@ -65,6 +65,18 @@ __device__ __forceinline__ void tangent_wall(const StepArgs<Real>&, uint32_t, in
 template <class Real>
 __device__ __forceinline__ void tangent_step_end(const StepArgs<Real>&, const SampleCtl&, uint32_t) {}
 
+// A value whose derivative the sensitivity build drops (the identity for float
+// and double).  Used for the contact terms that are not Lipschitz in the state:
+// the overlap factor sqrt(R* overlap) inside the damping coefficients
+// sqrt(K m) (derivative ~ overlap^-3/4 at first touch; the moduli and masses
+// keep theirs), and the unit directions of the Coulomb cap and of rolling
+// friction (derivative ~ 1/|v| near rest).  Their derivatives would swamp the
+// tangents of a loading run with spikes at every contact onset.
+template <class Real>
+__device__ __forceinline__ Real frozen(const Real& x) {
+  return x;
+}
+
 // Hertz-Mindlin contact of pair (i, j) seen from i (n points from i to j), in
 // the polydisperse form that reduces bit for bit to dd_Calculate_fijn_ppHM_2 /
 // dd_Calculate_fijtmijt_ppHM_2 / dd_Calculate_mijroll_ppHM_2
@@ -87,6 +99,9 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   Real cef1 = T::sqrt_rn(reff * (sumr - rijm));
   const Real Kn = Real(2) * sp.hmE * cef1;
   const Real Kt = Real(8) * sp.hmG * cef1;
+  // the same stiffnesses with their overlap dependence frozen (for the damping
+  // coefficients; identical values)
+  const Real Knd = Real(2) * sp.hmE * frozen(cef1), Ktd = Real(8) * sp.hmG * frozen(cef1);
   const Real rbar = half * sumr, rdif = half * (rj - ri);
   const Real sw0 = wj.x + wi.x, sw1 = wj.y + wi.y, sw2 = wj.z + wi.z;
   const Real dw0 = wj.x - wi.x, dw1 = wj.y - wi.y, dw2 = wj.z - wi.z;
@@ -96,7 +111,7 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   const Real vn = n0 * v0 + n1 * v1 + n2 * v2;
   const Real fijnm = (rijm - sumr) * Kn * T::kTwoThirds;
   const Real m2 = mi * ((mj + mj) / (mi + mj));
-  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * half * m2);
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Knd * half * m2);
   const Real fn0 = n0 * (fijnm + cef1), fn1 = n1 * (fijnm + cef1), fn2 = n2 * (fijnm + cef1);
   const Real vt0 = v0 - n0 * vn, vt1 = v1 - n1 * vn, vt2 = v2 - n2 * vn;
   // rotate the old tangential overlap into the new tangent plane, keep its length
@@ -118,16 +133,16 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   Real ft0 = t0 * Kt, ft1 = t1 * Kt, ft2 = t2 * Kt;
   const Real ftmm = (ft0 * ft0 + ft1 * ft1) + ft2 * ft2;
   if (ftmm > sp.mu * sp.mu * fijnm * fijnm) {
-    cef1 = sp.mu * T::fabs_(fijnm) * T::rsqrt_rn(ftmm);
-    ft0 *= cef1;
-    ft1 *= cef1;
-    ft2 *= cef1;
+    cef1 = sp.mu * T::fabs_(fijnm) * frozen(T::rsqrt_rn(ftmm));
+    ft0 = frozen(ft0) * cef1;
+    ft1 = frozen(ft1) * cef1;
+    ft2 = frozen(ft2) * cef1;
     cef1 = T::rcp(Kt);
     t0 = ft0 * cef1;
     t1 = ft1 * cef1;
     t2 = ft2 * cef1;
   } else {
-    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * half * m2);
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Ktd * half * m2);
     ft0 += vt0 * cef1;
     ft1 += vt1 * cef1;
     ft2 += vt2 * cef1;
@@ -151,16 +166,16 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   dropI = !(wim > Real(1e-18));
   dropJ = !(wjm > Real(1e-18));
   if (!dropI) {
-    const Real c = -sp.mur * afn * T::rsqrt_rn(wim);
-    mI[0] += wi.x * c;
-    mI[1] += wi.y * c;
-    mI[2] += wi.z * c;
+    const Real c = -sp.mur * afn * frozen(T::rsqrt_rn(wim));
+    mI[0] += frozen(wi.x) * c;
+    mI[1] += frozen(wi.y) * c;
+    mI[2] += frozen(wi.z) * c;
   }
   if (!dropJ) {
-    const Real c = -sp.mur * afn * T::rsqrt_rn(wjm);
-    mJ[0] += wj.x * c;
-    mJ[1] += wj.y * c;
-    mJ[2] += wj.z * c;
+    const Real c = -sp.mur * afn * frozen(T::rsqrt_rn(wjm));
+    mJ[0] += frozen(wj.x) * c;
+    mJ[1] += frozen(wj.y) * c;
+    mJ[2] += frozen(wj.z) * c;
   }
 }
 
@@ -401,13 +416,14 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
   Real cef1 = T::sqrt_rn(ri * T::fabs_(ri - riwm));
   const Real Kn = Real(2) * sp.wallE * cef1;
   const Real Kt = Real(8) * sp.wallG * cef1;
+  const Real Knd = Real(2) * sp.wallE * frozen(cef1), Ktd = Real(8) * sp.wallG * frozen(cef1);
   Real viw[3];
   viw[0] = wv[0] - v.x + ri * (niw[1] * w.z - niw[2] * w.y);
   viw[1] = wv[1] - v.y + ri * (niw[2] * w.x - niw[0] * w.z);
   viw[2] = wv[2] - v.z + ri * (niw[0] * w.y - niw[1] * w.x);
   const Real vn = niw[0] * viw[0] + niw[1] * viw[1] + niw[2] * viw[2];
   const Real fiwnm = (riwm - ri) * Kn * T::kTwoThirds;
-  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * mi);
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Knd * mi);
   const Real fiwn[3] = {niw[0] * (fiwnm + cef1), niw[1] * (fiwnm + cef1), niw[2] * (fiwnm + cef1)};
   const Real vt[3] = {viw[0] - niw[0] * vn, viw[1] - niw[1] * vn, viw[2] - niw[2] * vn};
   cef1 = niw[0] * o[0] + niw[1] * o[1] + niw[2] * o[2];
@@ -429,16 +445,16 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
   Real ft[3] = {ot[0] * Kt, ot[1] * Kt, ot[2] * Kt};
   const Real ftmm = (ft[0] * ft[0] + ft[1] * ft[1]) + ft[2] * ft[2];
   if (ftmm > sp.mu * sp.mu * fiwnm * fiwnm) {
-    cef1 = sp.mu * T::fabs_(fiwnm) * T::rsqrt_rn(ftmm);
-    ft[0] *= cef1;
-    ft[1] *= cef1;
-    ft[2] *= cef1;
+    cef1 = sp.mu * T::fabs_(fiwnm) * frozen(T::rsqrt_rn(ftmm));
+    ft[0] = frozen(ft[0]) * cef1;
+    ft[1] = frozen(ft[1]) * cef1;
+    ft[2] = frozen(ft[2]) * cef1;
     cef1 = T::rcp(Kt);
     ot[0] = ft[0] * cef1;
     ot[1] = ft[1] * cef1;
     ot[2] = ft[2] * cef1;
   } else {
-    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * mi);
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Ktd * mi);
     ft[0] += vt[0] * cef1;
     ft[1] += vt[1] * cef1;
     ft[2] += vt[2] * cef1;
@@ -451,10 +467,10 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
   const Real wim = (w.x * w.x + w.y * w.y) + w.z * w.z;
   Real madd[3] = {0, 0, 0};
   if (wim > Real(1e-18)) {
-    cef1 = -sp.mur * T::fabs_(fiwnm) * T::rsqrt_rn(wim);
-    madd[0] = w.x * cef1;
-    madd[1] = w.y * cef1;
-    madd[2] = w.z * cef1;
+    cef1 = -sp.mur * T::fabs_(fiwnm) * frozen(T::rsqrt_rn(wim));
+    madd[0] = frozen(w.x) * cef1;
+    madd[1] = frozen(w.y) * cef1;
+    madd[2] = frozen(w.z) * cef1;
   }
   F[0] += fiwn[0] + ft[0];
   F[1] += fiwn[1] + ft[1];

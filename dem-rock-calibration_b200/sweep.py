@@ -69,7 +69,7 @@ def cylinder(n: int, seed: int, r_min: float = 0.20, r_max: float = 0.30, packin
     xyz, rad, rep = create_cylinder_sample(box.center.astype(np.float64), R, half_h, n, r_min, r_max, seed=seed,
                                            growth_stages=30, steps_per_stage=150, max_fire_steps=6000,
                                            overlap_tol=2e-3, device=device)
-    size_real, center_real = bounding_box(xyz, rad.size, float(rad.max()))
+    size_real, center_real = bounding_box(xyz, rad.size, float(rad.max()), radii=rad)
     return xyz, rad, rep, box, size_real, center_real
 
 

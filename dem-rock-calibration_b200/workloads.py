@@ -7,7 +7,7 @@
 Micro-parameters: particle E = 50 GPa, nu = 0.25, rho = 2650 kg/m^3, friction
 0.5; bond E = 30 GPa, kn/ks = 2.5, bond radius 0.8 min(r_i, r_j), bonds for
 gaps < 0.1 r_min, normal and shear strengths N(40, 8) MPa per bond; dt = 0.2
-of the Rayleigh time of the smallest particle.  Every value in reference
+of the smaller of the Rayleigh time and the bond time of the smallest particle.  Every value in reference
 units (mm, mg, us, GPa).  Packings come from create_cylinder_sample (the
 reference draws its fill from time(NULL); here the seed is explicit).
 """
@@ -63,7 +63,7 @@ def _specimen(name, test, diameter, height, r_min, r_max, packing, seed, velocit
     pk.update(pack_kw or {})
     xyz, rad, rep = create_cylinder_sample(box.center.astype(np.float64), radius, half_h, n, r_min, r_max, E=50.0,
                                            nu=0.25, rho=2.65, seed=seed, **pk)
-    size_real, center_real = bounding_box(xyz, n, r_max)
+    size_real, center_real = bounding_box(xyz, n, r_max, radii=rad)
     ld = loading(test, box, size_real, center_real, velocity=-velocity_m_s / VELOCITY, min_stress=min_stress_gpa,
                  max_strain=max_strain, cond_fracture=0.1, dNsave=dNsave, max_steps=max_steps, p_r_platen=r_mean)
     mat = rock_material(r_min, r_mean, **mat_over)

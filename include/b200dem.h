@@ -90,7 +90,8 @@ typedef struct {
   double Ec_sd, Gc_sd;       /* > 0: per-bond strengths drawn from N(Ec, Ec_sd), N(Gc, Gc_sd) */
   double bond_radius_factor; /* used when b_r <= 0 */
   double dt;                 /* > 0: time step, us (else the reference rule 0.05*min(T_R, T_bond)) */
-  double dt_rayleigh_factor; /* > 0: dt = factor * Rayleigh time of the smallest particle */
+  double dt_rayleigh_factor; /* > 0: dt = factor * min(Rayleigh time, bond time 2 sqrt(m/k)) of the
+                                smallest particle (the reference's rule with this factor for its 0.05) */
   uint64_t seed;             /* per-bond strength draws */
   int nobreak;               /* 1: bonds never break (elastic stage, d_CalculateForcesDEM_22_ncb) */
   int reserved;

@@ -36,6 +36,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "BPM particle-steps/s"
 UNIT = "particle-steps/s"
+# DRAM bytes (read + write) of one k_pairs launch on the default workload (two
+# 245,098-sphere Brazilian discs), ncu --set full early in the loading
+PAIR_TRAFFIC_DISC_X2 = 204.7e6
 
 
 def dist_env():
@@ -382,6 +385,7 @@ def main() -> int:
         cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                "sample": f"{args.cpu_steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
                          f"integration) of the {spec.n}-sphere specimen"}
+    default_disc = args.workload == "brazilian_disc" and args.specimens == 2
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -400,7 +404,10 @@ def main() -> int:
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
+                     # DRAM read + write bytes of one pair-kernel launch on this workload, from the ncu
+                     # capture summarised in profiles/k_pairs_brazilian_disc_x2.md (not re-measured here)
+                     "traffic": PAIR_TRAFFIC_DISC_X2 if default_disc else None,
+                     "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
                      "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
                      "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,

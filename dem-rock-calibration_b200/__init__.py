@@ -147,6 +147,17 @@ def _declare(L):
     L.dem_load_cylinder_sample.argtypes = [C.c_char_p, C.c_double, _vp, _u32, P(_u32), _vp, _vp]
     L.dem_save_cylinder_sample.argtypes = [C.c_char_p, _vp, _u32, _vp]
     L.dem_save_sum_forces_loading.argtypes = [C.c_char_p, _vp, _u32]
+    _sz, _f = C.c_size_t, C.c_float
+    L.dem_mlp_gemm_tn.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, _vp]
+    L.dem_mlp_status.argtypes = [P(C.c_int)]
+    L.dem_mlp_pack_bf16.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp]
+    L.dem_mlp_gather.argtypes = [_vp, _vp, C.c_int, C.c_int, _vp, _vp]
+    L.dem_mlp_transpose_bf16.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp]
+    L.dem_mlp_act_backward.argtypes = [_vp, _vp, _sz, C.c_int, _vp, _vp, _vp]
+    L.dem_mlp_colsum.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp]
+    L.dem_mlp_mse_grad.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp]
+    L.dem_mlp_adam.argtypes = [_vp, _vp, _vp, _vp, _sz, _f, _f, _f, _f, _f, _vp, _vp, _vp]
+    L.dem_mlp_tick.argtypes = [_vp, _vp]
 
 
 def _lib():

@@ -20,7 +20,7 @@ SRC = PKG / "csrc"
 OUT = PKG / "libb200dem.so"
 CLI = PKG / "rockfit-dem"  # the reference's command line over the library (csrc/rockfit_cli.cpp)
 
-SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_noalloc.cu", "dem_capi.cpp"]
+SOURCES = ["dem_engine.cu", "dem_pack.cu", "dem_noalloc.cu", "dem_mlp.cu", "dem_capi.cpp"]
 HEADERS = ["dem_common.cuh", "dem_dual.cuh", "dem_types.h", "dem_step.cuh", "dem_build.cuh", "dem_pack.cuh", "dem_params.h",
            "dem_engine.h"]
 

@@ -31,6 +31,7 @@
 #ifndef B200DEM_H
 #define B200DEM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -256,6 +257,45 @@ int dem_ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, ui
 #define DEM_STATIC_SCRATCH_BYTES 4718592u /* 4.5 MiB */
 int dem_ref_cells_static(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
                          uint32_t* CIs, uint32_t* pnC);
+
+/* --- surrogate MLP on the tensor cores (the role of NN_MP.py's MLPRegressor,
+ * NN_MP.py:374-378, 895; the reference trains it with sklearn on the CPU) ---
+ * Device pointers, an optional cudaStream_t (NULL: the default stream).
+ * dem_mlp_gemm_tn: C[M x N] = A[M x K] B[N x K]^T, A and B row-major BF16,
+ * 16-byte aligned, K a multiple of 32, FP32 accumulation on tcgen05; epilogue
+ * DEM_MLP_PLAIN (out_f32 = C), DEM_MLP_BIAS (out_f32 = C + bias),
+ * DEM_MLP_BIAS_GELU / DEM_MLP_BIAS_RELU (out_bf16 = act(C + bias), and
+ * out_f32 = C + bias when given).  dem_mlp_status reports a tensor-core commit
+ * that timed out (the GEMM then leaves its output tile unwritten). */
+#define DEM_MLP_PLAIN 0
+#define DEM_MLP_BIAS 1
+#define DEM_MLP_BIAS_GELU 2
+#define DEM_MLP_BIAS_RELU 3
+int dem_mlp_gemm_tn(const void* A, const void* B, int M, int N, int K, const float* bias, int mode, float* out_f32,
+                    void* out_bf16, void* stream);
+int dem_mlp_status(int* timed_out);
+/* x (rows x k FP32) -> BF16 rows of kpad elements, zero padded; output row r is
+ * row idx[r] of x when idx (device int array of rows entries) is given */
+int dem_mlp_pack_bf16(const float* x, const int* idx, int rows, int k, int kpad, void* out_bf16, void* stream);
+/* out row r = row idx[r] of x (FP32, k columns) */
+int dem_mlp_gather(const float* x, const int* idx, int rows, int k, float* out, void* stream);
+/* out (cols x ldo BF16) = transpose of in (rows x cols BF16), columns >= rows zeroed */
+int dem_mlp_transpose_bf16(const void* in, int rows, int cols, int ldo, void* out, void* stream);
+/* dZ = dH * act'(Z), act DEM_MLP_BIAS_GELU or DEM_MLP_BIAS_RELU; BF16 (and FP32 when dz_f32 is given) */
+int dem_mlp_act_backward(const float* dh, const float* z, size_t n, int act, void* dz_bf16, float* dz_f32,
+                         void* stream);
+/* out[c] = sum over rows of in[r][c] (FP32, a fixed summation order);
+ * scratch holds DEM_MLP_COLSUM_SPLIT * cols floats */
+#define DEM_MLP_COLSUM_SPLIT 32
+int dem_mlp_colsum(const float* in, int rows, int cols, float* out, float* scratch, void* stream);
+/* dY = 2 (y - t) / n (BF16, and FP32 when given); *loss (double, device) += mean squared error */
+int dem_mlp_mse_grad(const float* y, const float* t, size_t n, void* dy_bf16, float* dy_f32, double* loss, void* stream);
+/* one Adam step on FP32 weights with gradient g + l2 w and the step number
+ * read from *step (device int, >= 1; bias corrections 1 - b^t); BF16 copy
+ * refreshed when w_bf16 is given.  dem_mlp_tick adds 1 to *step on the stream. */
+int dem_mlp_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps,
+                 float l2, const int* step, void* w_bf16, void* stream);
+int dem_mlp_tick(int* step, void* stream);
 
 /* --- reference entry points --- */
 /* One loading test of one specimen from host positions to macro results and

@@ -20,6 +20,7 @@ all host threads) on a bounded number of steps of the same specimen.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import importlib
 import json
 import os
@@ -94,6 +95,14 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def tensor_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["bf16_tflops"]), "measured (burst)"
+    return 1590.0, "fallback"
 
 
 class Clocks:
@@ -304,6 +313,115 @@ def run_sweep(args, ws, rank, local):
     return 0
 
 
+def surrogate_flops(sizes, rows: int) -> float:
+    """Algorithmic FLOPs of one training pass over `rows` samples: forward
+    GEMMs, weight-gradient GEMMs, and input-gradient GEMMs of every layer but
+    the first (unpadded layer sizes)."""
+    mm = [a * b for a, b in zip(sizes[:-1], sizes[1:])]
+    return 2.0 * rows * (2 * sum(mm) + sum(mm[1:]))
+
+
+def run_surrogate(args, ws, rank, local):
+    """Surrogate MLP 6-256-256-256-4 (GELU, BF16 operands, FP32 accumulation in
+    tensor memory) trained by mini-batch Adam (batch 256) on 8192 samples, one
+    CUDA-graph replay per epoch; every rank trains its own network (weak
+    scaling).  Inputs are the six sweep micro-parameters scaled to [-1, 1],
+    targets a seeded smooth four-output map standing in for (UCS, E, nu,
+    tensile strength) of simulated specimens.  Also times the forward GEMM of
+    a 65,536-candidate proposal batch."""
+    import torch
+    S = importlib.import_module("dem-rock-calibration_b200.surrogate")
+    D = Dist(ws)
+    torch.cuda.set_device(local)
+    sizes = (6, 256, 256, 256, 4)
+    n, batch = 8192, 256
+    rng = np.random.default_rng(17 + rank)
+    X = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+    Y = np.stack([np.sin(2 * X[:, 0]) + X[:, 1] ** 2 - X[:, 3], X[:, 2] * X[:, 3] + 0.5 * X[:, 0],
+                  np.exp(0.5 * X[:, 4]) - X[:, 5] * X[:, 1], X[:, 0] * X[:, 5] + 0.3 * X[:, 2]], 1)
+    Y = ((Y - Y.mean(0)) / Y.std(0)).astype(np.float32)
+    net = S.MLP(sizes, seed=rank, device=local)
+    ep = S.Epochs(net, X, Y, batch, seed=rank)
+    loss0 = ep.run()
+    for _ in range(max(args.warmup, 3)):
+        ep.run()
+    epochs = max(1, args.steps)
+    D.barrier()
+    clk = Clocks(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ep.stream.synchronize()
+    e0.record(ep.stream)
+    for _ in range(epochs):
+        ep.launch()
+    e1.record(ep.stream)
+    e1.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    loss1 = float(net.loss_acc.item()) / ep.nb
+    D.barrier()
+    ms_max = D.max(ms)
+    rows = ep.nb * batch
+    value = D.sum(float(rows)) * epochs / (ms_max * 1e-3)
+    flops = surrogate_flops(sizes, rows) * epochs
+    ep.close()
+    # inference GEMM of a 65,536-candidate proposal batch (hidden layer 256 x 256), alone
+    M, N, K = 65536, 256, 256
+    A = torch.randn(M, K, device=net.dev).to(torch.bfloat16)
+    Bm = torch.randn(N, K, device=net.dev).to(torch.bfloat16)
+    bias = torch.zeros(N, device=net.dev)
+    zf = torch.empty(M, N, device=net.dev)
+    zh = torch.empty(M, N, dtype=torch.bfloat16, device=net.dev)
+    P = lambda t: C.c_void_p(t.data_ptr())
+    st = torch.cuda.current_stream(net.dev)
+    call = lambda: net.L.dem_mlp_gemm_tn(P(A), P(Bm), M, N, K, P(bias), S.BIAS_GELU, P(zf), P(zh),
+                                         C.c_void_p(st.cuda_stream))
+    for _ in range(5):
+        call()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    g0.record(st)
+    for _ in range(reps):
+        call()
+    g1.record(st)
+    g1.synchronize()
+    gemm_ms = g0.elapsed_time(g1) / reps
+    net.check()
+    gemm_tf = 2.0 * M * N * K / (gemm_ms * 1e-3) / 1e12
+    # end to end through the public API: host arrays in, a fitted network and host predictions out
+    t0 = time.perf_counter()
+    net2 = S.MLP(sizes, seed=rank + 100, device=local)
+    net2.fit(X, Y, epochs=epochs, batch=batch, seed=rank)
+    _ = net2.predict(X[:batch])
+    t_e2e = time.perf_counter() - t0
+    peak_tf, peak_kind = tensor_peak()
+    line = {
+        "metric": "surrogate training samples/s", "value": value, "unit": "samples/s", "n_gpus": ws,
+        "steps": epochs, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / epochs, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 operands, f32 accumulation",
+        "data": "synthetic (seeded inputs in the sweep box, smooth 4-output targets)",
+        "config": {"workload": f"surrogate MLP {'-'.join(map(str, sizes))} GELU, {rows} samples per epoch, "
+                               f"batch {batch}, Adam", "step": "one epoch (one CUDA-graph replay)",
+                   "loss_first_epoch": loss0, "loss_last_epoch": loss1,
+                   "train_tflops": flops / (ms_max * 1e-3) / 1e12,
+                   "l2": "dataset and weights inside the L2 (the whole job is 10 MB)"},
+        "gpu_launches": epochs * ep.nb * 33,
+        "clocks": clocks,
+        "roofline": {"bound": "tensor", "achieved": gemm_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": gemm_tf / peak_tf, "traffic": None,
+                     "kernel": f"k_gemm_tn<256> forward layer {M} x {N} x {K} (bias + GELU epilogue)",
+                     "gemm_us": gemm_ms * 1e3, "peak_kind": peak_kind},
+        "e2e": {"value": rows * epochs / t_e2e, "unit": "samples/s",
+                "h2d_bytes_per_step": (X.nbytes + Y.nbytes) / epochs, "d2h_bytes_per_step": 4.0 * 2,
+                "seconds": t_e2e, "note": "MLP.fit from host arrays (upload, eager first epoch, graph capture, "
+                                          "replays, loss read per epoch) plus one host prediction"},
+        "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -311,7 +429,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brazilian_disc",
-                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep"])
+                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep", "surrogate"])
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
@@ -326,6 +444,8 @@ def main() -> int:
         return run_reference(args, ws, rank, local)
     if args.workload == "calibration_sweep":
         return run_sweep(args, ws, rank, local)
+    if args.workload == "surrogate":
+        return run_surrogate(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]

@@ -219,43 +219,11 @@ class MLP:
             graph: bool = True) -> list[float]:
         """Mini-batch Adam over (X, Y) (float arrays, rows = samples) for the
         given number of epochs, rows shuffled every epoch (seeded), the last
-        partial batch dropped; one CUDA graph replay per epoch.  Returns the
-        mean training loss of each epoch."""
-        torch = self.torch
-        X = np.ascontiguousarray(X, np.float32)
-        Y = np.ascontiguousarray(Y, np.float32)
-        n = X.shape[0]
-        batch = min(batch, n)
-        nb = n // batch
-        xd = torch.from_numpy(X).to(self.dev)
-        yd = torch.from_numpy(Y).to(self.dev)
-        perm = torch.zeros(nb * batch, dtype=torch.int32, device=self.dev)
-        rng = np.random.default_rng(seed)
-        stream = torch.cuda.Stream(self.dev)
-        stream.wait_stream(torch.cuda.current_stream(self.dev))   # uploads and weights
-        g = None
-        losses = []
-        with torch.cuda.stream(stream):
-            for e in range(epochs):
-                perm.copy_(torch.from_numpy(rng.permutation(n)[:nb * batch].astype(np.int32)))
-                self.loss_acc.zero_()
-                if not graph or e == 0:
-                    # eager: the first epoch also loads every kernel and the error flag
-                    # before a capture starts
-                    for k in range(nb):
-                        self.train_step(xd, yd, perm[k * batch:(k + 1) * batch])
-                else:
-                    if g is None:
-                        stream.synchronize()
-                        g = torch.cuda.CUDAGraph()
-                        with torch.cuda.graph(g, stream=stream):
-                            for k in range(nb):
-                                self.train_step(xd, yd, perm[k * batch:(k + 1) * batch])
-                    g.replay()
-                losses.append(float(self.loss_acc.item()) / nb)
-        torch.cuda.synchronize(self.dev)
-        del g
-        self.check()
+        partial batch dropped; after the first (eager) epoch, one CUDA graph
+        replay per epoch.  Returns the mean training loss of each epoch."""
+        ep = Epochs(self, X, Y, batch, seed)
+        losses = [ep.run(graph) for _ in range(epochs)]
+        ep.close()
         return losses
 
     def predict(self, X: np.ndarray, chunk: int = 65536) -> np.ndarray:
@@ -309,6 +277,63 @@ class MLP:
             out_W.append(self.W[l][:fo, :fi].cpu().numpy())
             out_b.append(self.b[l][:fo].cpu().numpy())
         return out_W, out_b
+
+
+class Epochs:
+    """Training epochs of an MLP over a dataset held on the device: a seeded
+    permutation per epoch, one Adam step per mini-batch; the first epoch runs
+    eagerly (it also loads every kernel before a capture starts), the later ones
+    replay one captured CUDA graph on a private stream."""
+
+    def __init__(self, net: MLP, X: np.ndarray, Y: np.ndarray, batch: int = 256, seed: int = 0):
+        torch = net.torch
+        self.net, self.torch = net, torch
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        self.n = X.shape[0]
+        self.batch = min(batch, self.n)
+        self.nb = self.n // self.batch
+        self.stream = torch.cuda.Stream(net.dev)
+        self.stream.wait_stream(torch.cuda.current_stream(net.dev))   # weights set up on the caller's stream
+        with torch.cuda.stream(self.stream):
+            self.x = torch.from_numpy(X).to(net.dev)
+            self.y = torch.from_numpy(Y).to(net.dev)
+            self.perm = torch.zeros(self.nb * self.batch, dtype=torch.int32, device=net.dev)
+        self.rng = np.random.default_rng(seed)
+        self.graph = None
+        self.count = 0
+
+    def _steps(self):
+        for k in range(self.nb):
+            self.net.train_step(self.x, self.y, self.perm[k * self.batch:(k + 1) * self.batch])
+
+    def launch(self, graph: bool = True) -> None:
+        """Enqueue one epoch on self.stream (no host synchronisation)."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            self.perm.copy_(torch.from_numpy(self.rng.permutation(self.n)[:self.nb * self.batch].astype(np.int32)))
+            self.net.loss_acc.zero_()
+            if not graph or self.count == 0:
+                self._steps()
+            else:
+                if self.graph is None:
+                    self.stream.synchronize()
+                    self.graph = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(self.graph, stream=self.stream):
+                        self._steps()
+                self.graph.replay()
+        self.count += 1
+
+    def run(self, graph: bool = True) -> float:
+        """One epoch; returns its mean training loss."""
+        self.launch(graph)
+        self.stream.synchronize()
+        return float(self.net.loss_acc.item()) / self.nb
+
+    def close(self) -> None:
+        self.torch.cuda.synchronize(self.net.dev)
+        self.graph = None
+        self.net.check()
 
 
 @dataclass
@@ -386,3 +411,120 @@ def macro_error(props: np.ndarray, target: np.ndarray, weights=None) -> np.ndarr
     if weights is not None:
         rel = rel[:, np.asarray(weights) > 0]
     return rel.max(axis=1)
+
+
+# ---- the plain simulator as the judge, and the calibration loop ----------
+
+PROPS = ("UCS", "E", "nu")
+
+
+class UniaxialJudge:
+    """Uniaxial tests of one packed cylinder (about n spheres) under many
+    parameter sets (rows in the order of sweep.SWEEP_SPACE) in one batched
+    context.  Every case draws its bond strengths with the same seed, so the
+    macro properties are a deterministic function of the parameters.  Returns
+    rows (UCS GPa, chord modulus GPa, Poisson ratio)."""
+
+    def __init__(self, n: int = 2000, seed: int = 5, velocity_m_s: float = 0.1, max_steps: int = 400000,
+                 device: int = 0):
+        from . import sweep
+        self.sweep, self.seed, self.device = sweep, seed, device
+        self.velocity, self.max_steps = velocity_m_s, max_steps
+        self.xyz, self.rad, _, self.box, self.size_real, self.center_real = sweep.cylinder(n, seed, device=device)
+        self.keys = list(sweep.SWEEP_SPACE)
+        self.calls = 0
+        self.cases = 0
+
+    def __call__(self, P: np.ndarray) -> np.ndarray:
+        from . import TEST_UNIAXIAL, VELOCITY, Context, loading
+        P = np.atleast_2d(np.asarray(P, np.float64))
+        r_min, r_mean = float(self.rad.min()), float(self.rad.mean())
+        ctx = Context(device=self.device)
+        try:
+            for row in P:
+                p = dict(zip(self.keys, row))
+                ld = loading(TEST_UNIAXIAL, self.box, self.size_real, self.center_real,
+                             velocity=-self.velocity / VELOCITY, min_stress=0.010, max_strain=0.01,
+                             cond_fracture=0.7, dNsave=100, max_steps=self.max_steps, p_r_platen=r_mean)
+                ctx.add_sample(self.sweep.material_for(p, r_min, r_mean, self.seed * 7919 + 1), ld, self.xyz,
+                               self.rad)
+            ctx.setup()
+            ctx.run(self.max_steps)
+            res = [ctx.result(i) for i in range(len(P))]
+        finally:
+            ctx.close()
+        self.calls += 1
+        self.cases += len(P)
+        return np.array([[r["FractureStress"], r["E_chord"], r["nu"]] for r in res])
+
+
+@dataclass
+class CalibrationRun:
+    target: np.ndarray
+    X: np.ndarray
+    Y: np.ndarray
+    best: np.ndarray          # parameters of the best simulated case
+    best_props: np.ndarray    # its simulated properties
+    best_error: float         # its largest relative deviation from the target
+    accepted: bool            # best_error <= tol, confirmed by the simulator
+    rounds: int
+    simulations: int
+    errors: list              # best error after the initial set and after each round
+
+
+def latin_box(n: int, lo, hi, seed: int) -> np.ndarray:
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    rng = np.random.default_rng(seed)
+    u = (np.stack([rng.permutation(n) for _ in lo], axis=1) + rng.random((n, lo.size))) / n
+    return lo + u * (hi - lo)
+
+
+def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_round: int = 16, tol: float = 0.01,
+              epochs: int = 300, weights=None, seed: int = 0, X0=None, Y0=None, device: int = 0) -> CalibrationRun:
+    """The reference's surrogate loop (NN_MP.py:766-930) with the simulator as
+    the judge: simulate a Latin-hypercube start set (or take X0, Y0), then per
+    round fit the surrogate to everything simulated so far, propose per_round
+    parameter sets whose predicted properties are closest to target, simulate
+    them, and stop when a simulated case is within tol (largest relative
+    deviation over the weighted properties).  Only simulated properties decide
+    acceptance; the surrogate only chooses what to simulate."""
+    target = np.asarray(target, np.float64)
+    if X0 is None:
+        X = latin_box(n_init, lo, hi, seed)
+        Y = judge(X)
+    else:
+        X, Y = np.asarray(X0, np.float64), np.asarray(Y0, np.float64)
+    sims = len(X)
+    err = macro_error(Y, target, weights)
+    errors = [float(err.min())]
+    sur = Surrogate(np.asarray(lo, np.float64), np.asarray(hi, np.float64), seed=seed, device=device)
+    r = 0
+    while r < rounds and errors[-1] > tol:
+        r += 1
+        ok = np.all(np.isfinite(Y), axis=1)
+        sur.fit(X[ok], Y[ok], epochs=epochs, batch=min(256, int(ok.sum())))
+        P, _ = sur.propose(target, k=per_round, weights=weights, seed=seed + r)
+        Yp = judge(P)
+        sims += len(P)
+        X, Y = np.vstack([X, P]), np.vstack([Y, Yp])
+        err = macro_error(Y, target, weights)
+        errors.append(float(err.min()))
+    i = int(np.argmin(err))
+    return CalibrationRun(target, X, Y, X[i], Y[i], float(err[i]), bool(err[i] <= tol), r, sims, errors)
+
+
+def random_search(judge, target, lo, hi, budget: int, weights=None, seed: int = 0, X0=None, Y0=None,
+                  batch: int = 16) -> CalibrationRun:
+    """The method without the network at the same simulator budget: further
+    Latin-hypercube points after the start set, the best simulated case kept."""
+    target = np.asarray(target, np.float64)
+    X, Y = np.asarray(X0, np.float64), np.asarray(Y0, np.float64)
+    errors = [float(macro_error(Y, target, weights).min())]
+    extra = latin_box(budget - len(X), lo, hi, seed + 1000) if budget > len(X) else np.empty((0, len(lo)))
+    for a in range(0, len(extra), batch):
+        P = extra[a:a + batch]
+        X, Y = np.vstack([X, P]), np.vstack([Y, judge(P)])
+        errors.append(float(macro_error(Y, target, weights).min()))
+    err = macro_error(Y, target, weights)
+    i = int(np.argmin(err))
+    return CalibrationRun(target, X, Y, X[i], Y[i], float(err[i]), False, len(errors) - 1, len(X), errors)

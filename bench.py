@@ -1,7 +1,8 @@
 """Benchmark of the bonded-particle DEM step (BPM + Hertz-Mindlin) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload brazilian_disc|uniaxial_cylinder]
+                    [--workload brazilian_disc|uniaxial_cylinder|calibration_sweep|
+                                calibration_solves|surrogate]
 
 A step is one DEM time step of a loading test (pair forces, platens,
 integration, loading controller; contact-list rebuilds when needed) over the
@@ -16,6 +17,12 @@ torch.distributed.
 
 --impl reference times the CPU restatement of the reference step (oracle,
 all host threads) on a bounded number of steps of the same specimen.
+
+Other workloads (each prints its own line): calibration_sweep (many
+cylinders and parameter sets in one context against one context at a time),
+calibration_solves (whole uniaxial solves per hour, batched against one
+solve per context), surrogate (training of the tensor-core MLP and its
+forward GEMM against the tensor peak).
 """
 from __future__ import annotations
 
@@ -357,10 +364,10 @@ def run_surrogate(args, ws, rank, local):
     e1.synchronize()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
-    loss1 = float(net.loss_acc.item()) / ep.nb
+    loss1 = float(net.loss_acc.item()) / len(ep.sizes)
     D.barrier()
     ms_max = D.max(ms)
-    rows = ep.nb * batch
+    rows = ep.n
     value = D.sum(float(rows)) * epochs / (ms_max * 1e-3)
     flops = surrogate_flops(sizes, rows) * epochs
     ep.close()
@@ -404,7 +411,7 @@ def run_surrogate(args, ws, rank, local):
                    "loss_first_epoch": loss0, "loss_last_epoch": loss1,
                    "train_tflops": flops / (ms_max * 1e-3) / 1e12,
                    "l2": "dataset and weights inside the L2 (the whole job is 10 MB)"},
-        "gpu_launches": epochs * ep.nb * 33,
+        "gpu_launches": epochs * len(ep.sizes) * net.launches_per_step(),
         "clocks": clocks,
         "roofline": {"bound": "tensor", "achieved": gemm_tf, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": gemm_tf / peak_tf, "traffic": None,
@@ -422,6 +429,63 @@ def run_surrogate(args, ws, rank, local):
     return 0
 
 
+def run_solves(args, ws, rank, local):
+    """Calibration solves per hour: `cases` uniaxial tests of one packed
+    cylinder of about 2,000 spheres (Latin-hypercube micro-parameters over the
+    sweep box), each run until its peak has passed (stress down to 70% of the
+    peak) or 1% strain, all in one context; against the same solves one
+    context at a time (the plain method: one specimen per run, as the
+    reference's CalculateOneSample), on a bounded sample of the cases.  Times
+    are wall-clock per whole solve (context, set-up, loading to the end,
+    results back), the unit a calibration pays for; every rank solves its own
+    cases (weak scaling)."""
+    import torch
+    S = importlib.import_module("dem-rock-calibration_b200.surrogate")
+    sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
+    D = Dist(ws)
+    torch.cuda.set_device(local)
+    J = S.UniaxialJudge(n=2000, seed=5 + rank, device=local)
+    lo = np.array([v[0] for v in sweep.SWEEP_SPACE.values()])
+    hi = np.array([v[1] for v in sweep.SWEEP_SPACE.values()])
+    X = S.latin_box(args.cases, lo, hi, 1 + rank)
+    for _ in range(max(1, min(args.warmup, 3))):
+        J(X[:2])                                       # kernel loading, allocator warm-up
+    D.barrier()
+    clk = Clocks(local)
+    t0 = time.perf_counter()
+    Yb = J(X)
+    t_b = time.perf_counter() - t0
+    clocks = clk.stop()
+    t_b = D.max(t_b)
+    k = min(args.cases, 8)
+    t0 = time.perf_counter()
+    Ys = np.vstack([J(X[i:i + 1]) for i in range(k)])
+    t_s = time.perf_counter() - t0
+    agree = float(np.max(np.abs(Yb[:k] - Ys) / np.maximum(np.abs(Ys), 1e-30)))
+    value = D.sum(float(args.cases)) / t_b * 3600.0
+    plain = D.sum(float(k) / t_s * 3600.0)
+    line = {
+        "metric": "calibration solves/hour", "value": value, "unit": "solves/hour", "n_gpus": ws, "steps": 1,
+        "warmup": max(1, min(args.warmup, 3)), "ms_per_step": t_b * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded packing, Latin-hypercube micro-parameters)",
+        "config": {"workload": f"{args.cases} uniaxial solves of a {J.rad.size}-sphere cylinder to 70% post-peak "
+                               f"(or 1% strain) in one context",
+                   "step": "the whole batch of solves, wall-clock (context, set-up, loading, results)",
+                   "plain": {"solves": k, "seconds": t_s, "value": plain,
+                             "note": "one context per solve, one after another"},
+                   "batched_over_plain": value / plain,
+                   "max_rel_difference_batched_vs_plain": agree,
+                   "ucs_gpa_range": [float(Yb[:, 0].min()), float(Yb[:, 0].max())],
+                   "l2": "whole state inside the L2 (small specimens); no flush"},
+        "gpu_launches": None, "clocks": clocks, "roofline": None, "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -429,7 +493,8 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brazilian_disc",
-                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep", "surrogate"])
+                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep", "calibration_solves",
+                             "surrogate"])
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
@@ -446,6 +511,8 @@ def main() -> int:
         return run_sweep(args, ws, rank, local)
     if args.workload == "surrogate":
         return run_surrogate(args, ws, rank, local)
+    if args.workload == "calibration_solves":
+        return run_solves(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]

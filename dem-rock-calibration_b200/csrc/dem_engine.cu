@@ -127,19 +127,19 @@ class Engine final : public EngineBase {
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     int dev = opt_.device;
     CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
-    // the pair kernel: 256-thread blocks (one bond tile per pass), as many
-    // blocks as fit on the GPU; register budget for pair_min_blocks blocks per
-    // SM (1..4; 0 = 3 for FP32 - 80 registers, no spills, the fastest on B200 -
-    // and 2 for FP64)
+    // the pair kernel: one bond tile per block and pass, as many blocks as fit
+    // on the GPU; register budget for pair_min_blocks blocks per SM: 1..4 of
+    // 256 threads, and for FP32 also 5..8 of 128 threads (102, 85, 72 and 64
+    // registers).  0 = 7 for FP32 (128 threads, 72 registers, no spills: 28
+    // warps per SM, measured 3% faster than 3 x 256 threads at 80 registers
+    // and than 64 registers with spills), 2 for FP64, 1 for the sensitivity
+    // build.
     opt_.pair_block = 256;
-    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > 4)
-      opt_.pair_min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 3 : 2);
-    switch (opt_.pair_min_blocks) {
-      case 1: pair_kernel_ = (const void*)k_pairs<Real, 1>; break;
-      case 2: pair_kernel_ = (const void*)k_pairs<Real, 2>; break;
-      case 3: pair_kernel_ = (const void*)k_pairs<Real, 3>; break;
-      default: pair_kernel_ = (const void*)k_pairs<Real, 4>; break;
-    }
+    constexpr bool kSmallBlocks = sizeof(Real) == 4 && !DualK<Real>::K;
+    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > (kSmallBlocks ? 8u : 4u))
+      opt_.pair_min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 7 : 2);
+    if (opt_.pair_min_blocks > 4) opt_.pair_block = 128;
+    pair_kernel_ = pair_kernel_ptr(opt_.pair_min_blocks);
     if (!opt_.pair_grid) {
       int per_sm = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel_, (int)opt_.pair_block, 0));
@@ -820,14 +820,29 @@ class Engine final : public EngineBase {
     return A;
   }
 
+  static const void* pair_kernel_ptr(uint32_t min_blocks) {
+    if constexpr (sizeof(Real) == 4 && !DualK<Real>::K) {
+      switch (min_blocks) {
+        case 5: return (const void*)k_pairs<Real, 5, 128>;
+        case 6: return (const void*)k_pairs<Real, 6, 128>;
+        case 7: return (const void*)k_pairs<Real, 7, 128>;
+        case 8: return (const void*)k_pairs<Real, 8, 128>;
+        default: break;
+      }
+    }
+    switch (min_blocks) {
+      case 1: return (const void*)k_pairs<Real, 1>;
+      case 2: return (const void*)k_pairs<Real, 2>;
+      case 3: return (const void*)k_pairs<Real, 3>;
+      default: return (const void*)k_pairs<Real, 4>;
+    }
+  }
+
   void launch_pairs(const StepArgs<Real>& A) {
     const dim3 g(opt_.pair_grid), b(opt_.pair_block);
-    switch (opt_.pair_min_blocks) {
-      case 1: k_pairs<Real, 1><<<g, b, 0, stream_>>>(A); break;
-      case 2: k_pairs<Real, 2><<<g, b, 0, stream_>>>(A); break;
-      case 3: k_pairs<Real, 3><<<g, b, 0, stream_>>>(A); break;
-      default: k_pairs<Real, 4><<<g, b, 0, stream_>>>(A); break;
-    }
+    StepArgs<Real> a = A;
+    void* params[] = {&a};
+    cudaLaunchKernel(pair_kernel_, g, b, params, 0, stream_);
   }
 
   void launch_step(const StepArgs<Real>& A, int stages) {

@@ -3,16 +3,19 @@
 // FP32 accumulation on the 5th-generation tensor cores.
 //
 //   k_gemm_tn   C[M x N] = A[M x K] . B[N x K]^T, A and B row-major BF16 (both
-//               "K-major"), accumulator in tensor memory: a 128-row tile of A and
-//               an N-tile (32..256) of B are staged in shared memory in the
-//               canonical no-swizzle core-matrix layout (8 rows x 16 bytes per
-//               core matrix), one thread issues tcgen05.mma (M = 128, K = 16 per
-//               instruction, kind::f16) into a TMEM accumulator and commits to an
-//               mbarrier; the four warps read the accumulator back with
-//               tcgen05.ld (32 lanes each) and apply the epilogue: + bias and
-//               GELU or ReLU to BF16 (hidden layers, pre-activation kept in
-//               FP32), + bias to FP32 (output layer), or plain FP32 (weight and
-//               activation gradients).
+//               "K-major"), accumulator in tensor memory.  A 128-row tile of A
+//               and an N-tile (32..256, narrowed for small grids) of B stream
+//               through a 2-4 stage cp.async pipeline (64 of K per stage) into
+//               shared memory in the canonical no-swizzle core-matrix layout
+//               (8 rows x 16 bytes per core matrix); one thread issues
+//               tcgen05.mma (M = 128, K = 16 per instruction, kind::f16) and
+//               commits each stage to its mbarrier, which frees the stage for
+//               the next load.  The eight warps then read the accumulator with
+//               tcgen05.ld (warps w and w + 4 share lanes 32 (w % 4) and split
+//               the columns), stage 32 x 32 chunks in shared memory and store
+//               whole rows: + bias and GELU or ReLU to BF16 (hidden layers,
+//               pre-activation kept in FP32), + bias to FP32 (output layer), or
+//               plain FP32 (weight and activation gradients).
 //   small kernels: input packing, transposes, activation backward, column
 //               sums, MSE gradient, Adam.
 //
@@ -31,8 +34,8 @@
 namespace dem {
 namespace {
 
-constexpr int kTM = 128;   // rows per tile (tcgen05 M)
-constexpr int kTK = 32;    // K staged per round (two K = 16 instructions)
+constexpr int kTM = 128;      // rows per tile (tcgen05 M)
+constexpr int kThreads = 256; // eight warps: all load, warp 0 lane 0 issues, all eight drain the accumulator
 constexpr uint32_t kPollLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -70,67 +73,128 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;
 }
 
-// exact (erf) GELU and its derivative; ReLU takes 0 as its derivative at 0, as
-// sklearn's MLPRegressor does (NN_MP.py:374 uses its default activation)
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in the tanh form of Hendrycks & Gimpel (2016),
+//   gelu(z) = z/2 (1 + tanh(u)) = z s,  s = 1 / (1 + exp(-2u)),
+//   u = sqrt(2/pi) (z + 0.044715 z^3),
+// evaluated as z s with the hardware exponential (__expf), which keeps its
+// relative accuracy in both tails (the form 1 + tanh(u) cancels for large
+// negative z); its derivative
+//   gelu'(z) = s + 2 z s (1 - s) sqrt(2/pi) (1 + 3 0.044715 z^2).
+// ReLU takes 0 as its derivative at 0, as sklearn's MLPRegressor does
+// (NN_MP.py:374 uses its default activation).
+constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2/pi)
+constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu_s(float z) {
+  const float u = kGeluC * __fmaf_rn(kGeluA * z * z, z, z);
+  return __frcp_rn(1.f + __expf(-2.f * u));
+}
+__device__ __forceinline__ float gelu(float z) { return z * gelu_s(z); }
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float s = gelu_s(z);
+  const float du = kGeluC * __fmaf_rn(3.f * kGeluA, z * z, 1.f);
+  return __fmaf_rn(2.f * z * s * (1.f - s), du, s);
+}
+
+// Pipeline geometry of a TN-column tile: a stage holds 64 of K (32 for the
+// 256-column tile) as 16-byte groups of 8 BF16 per row, for the 128 rows of A
+// and the TN rows of B; as many stages as fit in about 100 KB (2..4), so that
+// two blocks share an SM and one block's epilogue overlaps the other's main
+// loop.
+template <int TN>
+struct GemmCfg {
+  static constexpr int kSK = TN >= 256 ? 32 : 64;   // K per stage (narrower stages for the widest tile)
+  static constexpr int kGroups = kSK / 8;           // 16-byte K groups per row and stage
+  static constexpr int kStageBytes = (kTM + TN) * kGroups * 16;
+  static constexpr int kStages = (100 * 1024 / kStageBytes) < 2 ? 2 : ((100 * 1024 / kStageBytes) > 4 ? 4 : (100 * 1024 / kStageBytes));
+  static constexpr int kBars = 8 * kStages;                      // one mbarrier (8 bytes) per stage
+  static constexpr int kSmem = kStages * kStageBytes + kBars + 16 + 128;   // + tmem slot + alignment slack
+  static constexpr uint32_t kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256));
+};
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Stage s of round c: rows of A (kTM) then rows of B (TN), each as kGroups
+// core-matrix columns: group g of row r at byte (g * rows + r) * 16, so the
+// 8-row core matrices are 128 bytes apart (SBO) and the K groups rows * 16
+// bytes apart (LBO).  Rows beyond M / N and K beyond the end are zero-filled
+// (source size 0, address clamped to the operand's base).
+template <int TN>
+__device__ __forceinline__ void load_stage(uint32_t st, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N,
+                                           int K, int m0, int n0, int k0, int tid) {
+  using Cfg = GemmCfg<TN>;
+  for (int q = tid; q < Cfg::kGroups * (kTM + TN); q += kThreads) {
+    const int g = q % Cfg::kGroups, r = q / Cfg::kGroups;
+    const int k = k0 + 8 * g;
+    const __nv_bfloat16* src;
+    uint32_t dst, bytes;
+    if (r < kTM) {
+      const bool in = (m0 + r < M) && (k < K);
+      src = in ? A + (size_t)(m0 + r) * K + k : A;
+      bytes = in ? 16u : 0u;
+      dst = st + (uint32_t)(g * kTM + r) * 16u;
+    } else {
+      const int rb = r - kTM;
+      const bool in = (n0 + rb < N) && (k < K);
+      src = in ? B + (size_t)(n0 + rb) * K + k : B;
+      bytes = in ? 16u : 0u;
+      dst = st + (uint32_t)(kTM * Cfg::kGroups * 16) + (uint32_t)(g * TN + rb) * 16u;
+    }
+    cp_async16(dst, src, bytes);
+  }
 }
 
 template <int TN>
-struct __align__(128) GemmSmem {
-  uint4 a[4 * kTM];   // 4 K-groups of 8 BF16 x 128 rows
-  uint4 b[4 * TN];    // 4 K-groups x TN rows
-  uint64_t bar;
-  uint32_t tmem;
-};
-
-template <int TN>
-__global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B,
+__global__ void __launch_bounds__(kThreads) k_gemm_tn(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B,
                                                  int M, int N, int K, const float* __restrict__ bias, int mode,
                                                  float* __restrict__ outf, __nv_bfloat16* __restrict__ outh,
                                                  unsigned int* err) {
-  constexpr uint32_t kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256));
-  __shared__ GemmSmem<TN> sm;
+  using Cfg = GemmCfg<TN>;
+  constexpr int S = Cfg::kStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * Cfg::kStageBytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + S * Cfg::kStageBytes + Cfg::kBars);
+  const uint32_t sbase = saddr(base);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * TN;
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&sm.tmem)),
-                 "r"(kCols)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                 "r"(Cfg::kCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0) bar_init(&sm.bar);
+  if (tid == 0)
+    for (int s = 0; s < S; ++s) bar_init(&bars[s]);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = sm.tmem;
+  const uint32_t tmem = *tslot;
   // instruction descriptor: F32 accumulate, BF16 A and B, both K-major, N, M = 128
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
-  const int rounds = K / kTK;
+  const int rounds = (K + Cfg::kSK - 1) / Cfg::kSK;
+  // prologue: stages 0 .. S-2 in flight
+  for (int s = 0; s < S - 1; ++s) {
+    if (s < rounds) load_stage<TN>(sbase + s * Cfg::kStageBytes, A, B, M, N, K, m0, n0, s * Cfg::kSK, tid);
+    cp_async_commit();
+  }
   bool ok = true;
+  int issued = 0;                                             // rounds whose MMAs have been committed
   for (int c = 0; c < rounds; ++c) {
-    const int k0 = c * kTK;
-    for (int q = tid; q < 4 * kTM; q += 128) {
-      const int g = q & 3, r = q >> 2;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (m0 + r < M) v = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * K + k0 + 8 * g);
-      sm.a[g * kTM + r] = v;
-    }
-    for (int q = tid; q < 4 * TN; q += 128) {
-      const int g = q & 3, r = q >> 2;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (n0 + r < N) v = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * K + k0 + 8 * g);
-      sm.b[g * TN + r] = v;
-    }
-    // the tensor core reads shared memory through the async proxy
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const int s = c % S;
+    cp_async_wait<S - 2>();                                   // this thread's copies of round c have landed
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core's proxy
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      for (int kk = 0; kk < kTK / 16; ++kk) {
-        const uint64_t da = smem_desc(saddr(&sm.a[2 * kk * kTM]), kTM * 16, 128);
-        const uint64_t db = smem_desc(saddr(&sm.b[2 * kk * TN]), TN * 16, 128);
+      const uint32_t st = sbase + s * Cfg::kStageBytes;
+      for (int kk = 0; kk < Cfg::kSK / 16; ++kk) {
+        const uint64_t da = smem_desc(st + (uint32_t)(2 * kk * kTM * 16), kTM * 16, 128);
+        const uint64_t db = smem_desc(st + (uint32_t)(kTM * Cfg::kGroups * 16 + 2 * kk * TN * 16), TN * 16, 128);
         const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -140,21 +204,44 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16* __restrict
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       saddr(&sm.bar))
+                       saddr(&bars[s]))
                    : "memory");
     }
-    ok = bar_wait(&sm.bar, (uint32_t)(c & 1));
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(err, 1u);
-      bar_wait(&sm.bar, (uint32_t)(c & 1));
-      ok = false;
-      break;
+    issued = c + 1;
+    // refill the stage that round c - 1 read, once its MMAs have completed
+    const int cn = c + S - 1;
+    if (c >= 1) {
+      const int sp = (c - 1) % S;
+      ok = bar_wait(&bars[sp], (uint32_t)(((c - 1) / S) & 1));
+      if (__syncthreads_or(!ok)) break;
     }
+    if (cn < rounds) load_stage<TN>(sbase + (cn % S) * Cfg::kStageBytes, A, B, M, N, K, m0, n0, cn * Cfg::kSK, tid);
+    cp_async_commit();
   }
   if (ok && rounds > 0) {
+    const int cl = rounds - 1;
+    ok = bar_wait(&bars[cl % S], (uint32_t)((cl / S) & 1));
+    ok = !__syncthreads_or(!ok);
+  }
+  cp_async_wait<0>();
+  if (!ok) {
+    if (tid == 0) atomicOr(err, 1u);
+    // one more bounded wait for the last commit, so that no MMA is left reading
+    // shared memory or writing the accumulator when the block frees them
+    if (issued > 0) bar_wait(&bars[(issued - 1) % S], (uint32_t)(((issued - 1) / S) & 1));
+  }
+  __syncthreads();
+  if (ok && rounds > 0) {
     tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
-    for (int col0 = 0; col0 < TN; col0 += 32) {
+    // epilogue: warp w reads accumulator lanes 32 (w % 4) .. +31 (the lanes its
+    // quarter of the warps may access), warps w and w + 4 taking alternate
+    // 32-column chunks; a thread holds 32 consecutive columns of one row and
+    // writes them with 16-byte stores (scalar stores at a ragged right edge
+    // or when a row is not a multiple of 16 bytes)
+    const int q4 = warp & 3, half = warp >> 2;
+    const int row = m0 + q4 * 32 + lane;
+    const bool act = mode == DEM_MLP_BIAS_GELU || mode == DEM_MLP_BIAS_RELU;
+    for (int col0 = 32 * half; col0 < TN; col0 += 64) {
       uint32_t r[32];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -164,31 +251,58 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16* __restrict
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
             "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
             "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col0)
+          : "r"(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)col0)
           : "memory");
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
-        for (int j = 0; j < 32; ++j) {
-          const int n = n0 + col0 + j;
-          if (n >= N) break;
-          float v = __uint_as_float(r[j]);
-          const size_t o = (size_t)row * N + n;
-          if (mode == DEM_MLP_BIAS_GELU || mode == DEM_MLP_BIAS_RELU) {
-            v += bias[n];
-            if (outf) outf[o] = v;
-            outh[o] = __float2bfloat16_rn(mode == DEM_MLP_BIAS_GELU ? gelu(v) : fmaxf(v, 0.f));
-          } else if (mode == DEM_MLP_BIAS) {
-            outf[o] = v + bias[n];
-          } else {
-            outf[o] = v;
-          }
+      const int nc = n0 + col0;
+      if (row >= M || nc >= N) continue;
+      const int cols = min(32, N - nc);
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+      if (mode != DEM_MLP_PLAIN) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += (j < cols) ? __ldg(bias + nc + j) : 0.f;
+      }
+      const size_t o = (size_t)row * N + nc;
+      if (outf) {
+        if (cols == 32 && (N & 3) == 0) {
+          float4* dst = reinterpret_cast<float4*>(outf + o);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j < cols) outf[o + j] = v[j];
+        }
+      }
+      if (act) {
+        const bool g = mode == DEM_MLP_BIAS_GELU;
+        uint32_t h[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float a0 = g ? gelu(v[2 * j]) : fmaxf(v[2 * j], 0.f);
+          const float a1 = g ? gelu(v[2 * j + 1]) : fmaxf(v[2 * j + 1], 0.f);
+          const __nv_bfloat162 p = __floats2bfloat162_rn(a0, a1);
+          h[j] = *reinterpret_cast<const uint32_t*>(&p);
+        }
+        if (cols == 32 && (N & 7) == 0) {
+          uint4* dst = reinterpret_cast<uint4*>(outh + o);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dst[j] = make_uint4(h[4 * j], h[4 * j + 1], h[4 * j + 2], h[4 * j + 3]);
+        } else {
+          unsigned short* dst = reinterpret_cast<unsigned short*>(outh + o);
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j < cols) dst[j] = (unsigned short)((j & 1) ? (h[j >> 1] >> 16) : (h[j >> 1] & 0xFFFFu));
         }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols) : "memory");
 }
 
 // x (rows x k FP32) -> BF16 rows of kpad, zero padded; row r of the output is
@@ -325,6 +439,26 @@ int err_flag(unsigned int** out) {
 
 uint32_t blocks(size_t n) { return (uint32_t)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+// the pipeline needs more than the default 48 KB of dynamic shared memory: the
+// limit is raised once per device and tile width (before any graph capture,
+// since the first call of every shape comes from eager code)
+template <int TN>
+int launch_gemm(unsigned gx, unsigned gy, cudaStream_t st, const __nv_bfloat16* a, const __nv_bfloat16* b, int M,
+                int N, int K, const float* bias, int mode, float* outf, __nv_bfloat16* oh, unsigned int* err) {
+  static bool raised[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return DEM_ERR_CUDA;
+  if (!raised[dev]) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (cudaFuncSetAttribute(k_gemm_tn<TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<TN>::kSmem) !=
+        cudaSuccess)
+      return DEM_ERR_CUDA;
+    raised[dev] = true;
+  }
+  k_gemm_tn<TN><<<dim3(gx, gy), kThreads, GemmCfg<TN>::kSmem, st>>>(a, b, M, N, K, bias, mode, outf, oh, err);
+  return DEM_OK;
+}
+
 }  // namespace
 }  // namespace dem
 
@@ -347,15 +481,21 @@ int dem_mlp_gemm_tn(const void* A, const void* B, int M, int N, int K, const flo
   const auto* b = static_cast<const __nv_bfloat16*>(B);
   auto* oh = static_cast<__nv_bfloat16*>(out_bf16);
   const unsigned gx = (unsigned)((M + kTM - 1) / kTM);
-  if (N <= 32)
-    k_gemm_tn<32><<<dim3(gx, 1), 128, 0, st>>>(a, b, M, N, K, bias, mode, out_f32, oh, err);
-  else if (N <= 64)
-    k_gemm_tn<64><<<dim3(gx, 1), 128, 0, st>>>(a, b, M, N, K, bias, mode, out_f32, oh, err);
-  else if (N <= 128)
-    k_gemm_tn<128><<<dim3(gx, 1), 128, 0, st>>>(a, b, M, N, K, bias, mode, out_f32, oh, err);
+  // tile width: the widest that covers N, narrowed while the grid would leave
+  // most SMs idle (small batches), down to 32 columns
+  int tn = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  while (tn > 32 && (size_t)gx * (size_t)((N + tn - 1) / tn) < 148) tn >>= 1;
+  const unsigned gy = (unsigned)((N + tn - 1) / tn);
+  int rc;
+  if (tn == 32)
+    rc = launch_gemm<32>(gx, gy, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+  else if (tn == 64)
+    rc = launch_gemm<64>(gx, gy, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+  else if (tn == 128)
+    rc = launch_gemm<128>(gx, gy, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
   else
-    k_gemm_tn<256><<<dim3(gx, (unsigned)((N + 255) / 256)), 128, 0, st>>>(a, b, M, N, K, bias, mode, out_f32, oh,
-                                                                         err);
+    rc = launch_gemm<256>(gx, gy, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+  if (rc) return rc;
   return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 

@@ -379,8 +379,8 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
 // prefetch the block's next tile of bond state into L2 (five bulk prefetches),
 // so the next pass finds its streamed loads in L2.  Bond arrays are padded to
 // whole 256-bond tiles.
-template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2)>
-__global__ void __launch_bounds__(256, kMinBlocks) k_pairs(StepArgs<Real> A) {
+template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2), int kBlock = 256>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) {
   using V4 = typename RT<Real>::V4;
   const uint32_t nb = A.nb;
   const uint32_t tile = blockDim.x, stride = gridDim.x * tile;

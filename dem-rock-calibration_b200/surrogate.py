@@ -53,8 +53,8 @@ def _ck(rc: int, what: str) -> None:
 
 
 class MLP:
-    """Dense network sizes[0] -> ... -> sizes[-1], hidden activation GELU (exact
-    erf form) or ReLU, identity output, loss mean((y - t)^2).
+    """Dense network sizes[0] -> ... -> sizes[-1], hidden activation GELU (tanh
+    form) or ReLU, identity output, loss mean((y - t)^2).
 
     Device layout: layer l holds FP32 master weights W_l (out_p x in_p), a BF16
     copy, bias b_l (out_p) and Adam moments; in_p and the hidden out_p are the
@@ -199,6 +199,15 @@ class MLP:
             _ck(L.dem_mlp_adam(P(w), P(g), P(m), P(v), w.numel(), self.lr, self.b1, self.b2, self.eps, l2,
                                P(self.step), wh, s), "dem_mlp_adam")
 
+    def launches_per_step(self) -> int:
+        """Kernel launches of one train_step: gather + input pack + one GEMM per
+        layer; MSE gradient + pack, per layer two transposes, the weight-gradient
+        GEMM and the two column-sum passes, per layer but the first a transpose,
+        the input-gradient GEMM and the activation backward; the step tick and
+        one Adam launch per weight and bias array."""
+        nl = len(self.W)
+        return (2 + nl) + (2 + 5 * nl + 3 * (nl - 1)) + (1 + 2 * nl)
+
     def train_step(self, x, t, idx):
         """One Adam step on the rows idx (device int32) of x / t (device FP32)."""
         bufs = self._buffers(int(idx.numel()))
@@ -219,8 +228,9 @@ class MLP:
             graph: bool = True) -> list[float]:
         """Mini-batch Adam over (X, Y) (float arrays, rows = samples) for the
         given number of epochs, rows shuffled every epoch (seeded), the last
-        partial batch dropped; after the first (eager) epoch, one CUDA graph
-        replay per epoch.  Returns the mean training loss of each epoch."""
+        batch smaller when batch does not divide the rows; after the first
+        (eager) epoch, one CUDA graph replay per epoch.  Returns the mean
+        training loss of each epoch (the mean of its batch losses)."""
         ep = Epochs(self, X, Y, batch, seed)
         losses = [ep.run(graph) for _ in range(epochs)]
         ep.close()
@@ -281,7 +291,8 @@ class MLP:
 
 class Epochs:
     """Training epochs of an MLP over a dataset held on the device: a seeded
-    permutation per epoch, one Adam step per mini-batch; the first epoch runs
+    permutation per epoch, one Adam step per mini-batch (the last one smaller
+    when batch does not divide the rows); the first epoch runs
     eagerly (it also loads every kernel before a capture starts), the later ones
     replay one captured CUDA graph on a private stream."""
 
@@ -293,25 +304,29 @@ class Epochs:
         self.n = X.shape[0]
         self.batch = min(batch, self.n)
         self.nb = self.n // self.batch
+        # the last, smaller batch is trained too (as sklearn's gen_batches yields it)
+        self.sizes = [self.batch] * self.nb + ([self.n - self.nb * self.batch] if self.n % self.batch else [])
         self.stream = torch.cuda.Stream(net.dev)
         self.stream.wait_stream(torch.cuda.current_stream(net.dev))   # weights set up on the caller's stream
         with torch.cuda.stream(self.stream):
             self.x = torch.from_numpy(X).to(net.dev)
             self.y = torch.from_numpy(Y).to(net.dev)
-            self.perm = torch.zeros(self.nb * self.batch, dtype=torch.int32, device=net.dev)
+            self.perm = torch.zeros(self.n, dtype=torch.int32, device=net.dev)
         self.rng = np.random.default_rng(seed)
         self.graph = None
         self.count = 0
 
     def _steps(self):
-        for k in range(self.nb):
-            self.net.train_step(self.x, self.y, self.perm[k * self.batch:(k + 1) * self.batch])
+        a = 0
+        for b in self.sizes:
+            self.net.train_step(self.x, self.y, self.perm[a:a + b])
+            a += b
 
     def launch(self, graph: bool = True) -> None:
         """Enqueue one epoch on self.stream (no host synchronisation)."""
         torch = self.torch
         with torch.cuda.stream(self.stream):
-            self.perm.copy_(torch.from_numpy(self.rng.permutation(self.n)[:self.nb * self.batch].astype(np.int32)))
+            self.perm.copy_(torch.from_numpy(self.rng.permutation(self.n).astype(np.int32)))
             self.net.loss_acc.zero_()
             if not graph or self.count == 0:
                 self._steps()
@@ -328,7 +343,7 @@ class Epochs:
         """One epoch; returns its mean training loss."""
         self.launch(graph)
         self.stream.synchronize()
-        return float(self.net.loss_acc.item()) / self.nb
+        return float(self.net.loss_acc.item()) / len(self.sizes)
 
     def close(self) -> None:
         self.torch.cuda.synchronize(self.net.dev)
@@ -404,15 +419,6 @@ class Surrogate:
         return params, self.predict(params)
 
 
-def macro_error(props: np.ndarray, target: np.ndarray, weights=None) -> np.ndarray:
-    """Largest relative deviation of each row of props from target (weighted
-    properties only)."""
-    rel = np.abs(np.asarray(props, np.float64) / np.asarray(target, np.float64) - 1.0)
-    if weights is not None:
-        rel = rel[:, np.asarray(weights) > 0]
-    return rel.max(axis=1)
-
-
 # ---- the plain simulator as the judge, and the calibration loop ----------
 
 PROPS = ("UCS", "E", "nu")
@@ -461,15 +467,17 @@ class UniaxialJudge:
 @dataclass
 class CalibrationRun:
     target: np.ndarray
+    tol: np.ndarray           # per-property relative tolerance
     X: np.ndarray
     Y: np.ndarray
     best: np.ndarray          # parameters of the best simulated case
     best_props: np.ndarray    # its simulated properties
-    best_error: float         # its largest relative deviation from the target
-    accepted: bool            # best_error <= tol, confirmed by the simulator
+    best_score: float         # its largest deviation in units of the tolerance (<= 1: within tol)
+    accepted: bool            # best_score <= 1 in the batched run and in its plain re-run
+    confirmed_props: np.ndarray | None   # the plain re-run of the accepted case
     rounds: int
     simulations: int
-    errors: list              # best error after the initial set and after each round
+    scores: list              # best score after the start set and after each round
 
 
 def latin_box(n: int, lo, hi, seed: int) -> np.ndarray:
@@ -479,52 +487,153 @@ def latin_box(n: int, lo, hi, seed: int) -> np.ndarray:
     return lo + u * (hi - lo)
 
 
-def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_round: int = 16, tol: float = 0.01,
-              epochs: int = 300, weights=None, seed: int = 0, X0=None, Y0=None, device: int = 0) -> CalibrationRun:
+def score(props, target, tol) -> np.ndarray:
+    """Per row: the largest relative deviation from target in units of the
+    per-property tolerance (a property with tolerance inf is not compared)."""
+    rel = np.abs(np.atleast_2d(np.asarray(props, np.float64)) / np.asarray(target, np.float64) - 1.0)
+    out = (rel / np.broadcast_to(np.asarray(tol, np.float64), rel.shape[1:])).max(axis=1)
+    return np.where(np.isfinite(out), out, np.inf)
+
+
+def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_round: int = 16, tol=0.01,
+              epochs: int = 300, seed: int = 0, X0=None, Y0=None, device: int = 0) -> CalibrationRun:
     """The reference's surrogate loop (NN_MP.py:766-930) with the simulator as
     the judge: simulate a Latin-hypercube start set (or take X0, Y0), then per
     round fit the surrogate to everything simulated so far, propose per_round
-    parameter sets whose predicted properties are closest to target, simulate
-    them, and stop when a simulated case is within tol (largest relative
-    deviation over the weighted properties).  Only simulated properties decide
-    acceptance; the surrogate only chooses what to simulate."""
+    parameter sets whose predicted properties are closest to target (errors
+    weighted by 1 / tol^2), simulate them in one batched context, and stop
+    once a simulated case is within tol on every property AND a plain re-run
+    of that case (one sample per context: the plain method) is within tol as
+    well.  Simulated properties alone decide acceptance; the surrogate only
+    chooses what to simulate.  A case whose re-run misses tol stays in the data
+    but cannot be accepted."""
     target = np.asarray(target, np.float64)
+    tol = np.broadcast_to(np.asarray(tol, np.float64), target.shape).copy()
     if X0 is None:
         X = latin_box(n_init, lo, hi, seed)
         Y = judge(X)
     else:
         X, Y = np.asarray(X0, np.float64), np.asarray(Y0, np.float64)
     sims = len(X)
-    err = macro_error(Y, target, weights)
-    errors = [float(err.min())]
+    rejected = np.zeros(len(X), bool)
     sur = Surrogate(np.asarray(lo, np.float64), np.asarray(hi, np.float64), seed=seed, device=device)
-    r = 0
-    while r < rounds and errors[-1] > tol:
+    w = 1.0 / np.where(np.isfinite(tol), tol, np.inf) ** 2
+    w = w / w.max()
+    accepted, confirmed, r = False, None, 0
+    sc = score(Y, target, tol)
+    scores = [float(sc.min())]
+
+    def confirm():
+        nonlocal sims, confirmed, accepted
+        while True:
+            cand = np.where(rejected, np.inf, score(Y, target, tol))
+            i = int(np.argmin(cand))
+            if cand[i] > 1.0:
+                return
+            again = judge(X[i:i + 1])[0]
+            sims += 1
+            if score(again, target, tol)[0] <= 1.0:
+                accepted, confirmed = True, again
+                return
+            rejected[i] = True
+
+    confirm()
+    while r < rounds and not accepted:
         r += 1
         ok = np.all(np.isfinite(Y), axis=1)
         sur.fit(X[ok], Y[ok], epochs=epochs, batch=min(256, int(ok.sum())))
-        P, _ = sur.propose(target, k=per_round, weights=weights, seed=seed + r)
+        P, _ = sur.propose(target, k=per_round, weights=w, seed=seed + r)
         Yp = judge(P)
         sims += len(P)
         X, Y = np.vstack([X, P]), np.vstack([Y, Yp])
-        err = macro_error(Y, target, weights)
-        errors.append(float(err.min()))
-    i = int(np.argmin(err))
-    return CalibrationRun(target, X, Y, X[i], Y[i], float(err[i]), bool(err[i] <= tol), r, sims, errors)
+        rejected = np.concatenate([rejected, np.zeros(len(P), bool)])
+        scores.append(float(score(Y, target, tol).min()))
+        confirm()
+    sc = np.where(rejected, np.inf, score(Y, target, tol))
+    i = int(np.argmin(sc))
+    return CalibrationRun(target, tol, X, Y, X[i], Y[i], float(sc[i]), accepted, confirmed, r, sims, scores)
 
 
-def random_search(judge, target, lo, hi, budget: int, weights=None, seed: int = 0, X0=None, Y0=None,
+def random_search(judge, target, lo, hi, budget: int, tol=0.01, seed: int = 0, X0=None, Y0=None,
                   batch: int = 16) -> CalibrationRun:
     """The method without the network at the same simulator budget: further
-    Latin-hypercube points after the start set, the best simulated case kept."""
+    Latin-hypercube points after the start set, the best simulated case kept
+    (scored as in calibrate; not re-run)."""
     target = np.asarray(target, np.float64)
+    tol = np.broadcast_to(np.asarray(tol, np.float64), target.shape).copy()
     X, Y = np.asarray(X0, np.float64), np.asarray(Y0, np.float64)
-    errors = [float(macro_error(Y, target, weights).min())]
+    scores = [float(score(Y, target, tol).min())]
     extra = latin_box(budget - len(X), lo, hi, seed + 1000) if budget > len(X) else np.empty((0, len(lo)))
     for a in range(0, len(extra), batch):
         P = extra[a:a + batch]
         X, Y = np.vstack([X, P]), np.vstack([Y, judge(P)])
-        errors.append(float(macro_error(Y, target, weights).min()))
-    err = macro_error(Y, target, weights)
-    i = int(np.argmin(err))
-    return CalibrationRun(target, X, Y, X[i], Y[i], float(err[i]), False, len(errors) - 1, len(X), errors)
+        scores.append(float(score(Y, target, tol).min()))
+    sc = score(Y, target, tol)
+    i = int(np.argmin(sc))
+    return CalibrationRun(target, tol, X, Y, X[i], Y[i], float(sc[i]), False, None, len(scores) - 1, len(X),
+                          scores)
+
+
+class MLPRegressorB200:
+    """sklearn.neural_network.MLPRegressor's interface (the surrogate of
+    NN_MP.py:374-378: fit(X, y) at :895, predict at :395) over the tensor-core
+    MLP, so that the workflow swaps one constructor:
+
+        mlp = MLPRegressorB200(hidden_layer_sizes=[300, 500, 900, 500, 300], max_iter=20000, tol=0)
+
+    Same meaning as sklearn for hidden_layer_sizes, activation ('relu' or
+    'gelu'; sklearn's default 'relu'), alpha (L2 penalty, weights only, its
+    gradient alpha W / batch against the data gradient of sum((y - t)^2) / (2
+    batch)), batch_size ('auto' = min(200, n)), learning_rate_init, max_iter
+    (epochs), tol and n_iter_no_change (stop when the epoch loss has not
+    improved by tol for n_iter_no_change epochs), beta_1, beta_2, epsilon,
+    shuffle (always on), random_state.  Inputs are used as given (sklearn
+    does not scale them either); a 1-D y gives 1-D predictions.  The numerics
+    differ from sklearn's float64 CPU path by BF16 operands (FP32
+    accumulation and master weights)."""
+
+    def __init__(self, hidden_layer_sizes=(100,), activation="relu", alpha=1e-4, batch_size="auto",
+                 learning_rate_init=1e-3, max_iter=200, tol=1e-4, n_iter_no_change=10, beta_1=0.9, beta_2=0.999,
+                 epsilon=1e-8, random_state=None, device=0):
+        self.hidden_layer_sizes = tuple(hidden_layer_sizes)
+        self.activation, self.alpha, self.batch_size = activation, alpha, batch_size
+        self.learning_rate_init, self.max_iter, self.tol = learning_rate_init, max_iter, tol
+        self.n_iter_no_change, self.beta_1, self.beta_2, self.epsilon = n_iter_no_change, beta_1, beta_2, epsilon
+        self.random_state, self.device = random_state, device
+        self.net = None
+        self.loss_curve_ = []
+        self.n_iter_ = 0
+
+    def fit(self, X, y):
+        X = np.asarray(X, np.float32)
+        y = np.asarray(y, np.float32)
+        self._1d = y.ndim == 1
+        Y = y.reshape(len(y), -1)
+        n = len(X)
+        batch = min(200, n) if self.batch_size == "auto" else min(int(self.batch_size), n)
+        seed = 0 if self.random_state is None else int(self.random_state)
+        n_out = Y.shape[1]
+        # device loss mean((y - t)^2) has gradient (2 / n_out) x sklearn's data term
+        l2 = self.alpha / batch * 2.0 / n_out
+        self.net = MLP((X.shape[1],) + self.hidden_layer_sizes + (n_out,), self.activation, seed, self.device,
+                       self.learning_rate_init, l2, (self.beta_1, self.beta_2), self.epsilon)
+        ep = Epochs(self.net, X, Y, batch, seed)
+        best, stall = np.inf, 0
+        self.loss_curve_ = []
+        for it in range(self.max_iter):
+            loss = 0.5 * n_out * ep.run()          # sklearn's loss scale, sum((y - t)^2) / (2 n)
+            self.loss_curve_.append(loss)
+            self.n_iter_ = it + 1
+            if loss > best - self.tol:
+                stall += 1
+            else:
+                stall = 0
+            best = min(best, loss)
+            if stall > self.n_iter_no_change:
+                break
+        ep.close()
+        return self
+
+    def predict(self, X):
+        out = self.net.predict(np.asarray(X, np.float32))
+        return out[:, 0] if self._1d else out

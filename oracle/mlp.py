@@ -14,7 +14,9 @@ backprop gradients (tests/test_mlp_oracle.py).  The bf16=True path restates
 what the device computes: every GEMM operand (inputs, weights, hidden
 activations, output and hidden-layer gradients) rounded to bfloat16 (round to
 nearest even), products accumulated in float32 or better, pre-activations,
-gradients and master weights in float32.
+gradients and master weights in float32.  GELU is the tanh form (the device
+evaluates its tanh with the hardware approximation, relative error about
+2^-11; this file with numpy's tanh).
 
 Weights follow the device layout: W_l has shape (out, in) (sklearn's coefs_
 are the transposes), loss = mean over all rows and outputs of (y - t)^2.
@@ -22,7 +24,6 @@ are the transposes), loss = mean over all rows and outputs of (y - t)^2.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 
 def bf16(x: np.ndarray) -> np.ndarray:
@@ -32,16 +33,23 @@ def bf16(x: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32)
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def act(z: np.ndarray, kind: str) -> np.ndarray:
+    """ReLU, or GELU in the tanh form of Hendrycks & Gimpel (2016):
+    z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
     if kind == "relu":
         return np.maximum(z, 0)
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def act_grad(z: np.ndarray, kind: str) -> np.ndarray:
+    """Derivative of act (ReLU: 0 at 0, as sklearn)."""
     if kind == "relu":
         return (z > 0).astype(z.dtype)
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def _mm(a, b, rnd):

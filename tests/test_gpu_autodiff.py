@@ -1,0 +1,72 @@
+"""ElasticResponse (torch.autograd.Function over the sensitivity build)
+against the sensitivities themselves and against central finite
+differences of a calibration loss.
+
+Specimen and run as in test_gpu_sensitivity.py: a polydisperse cylinder of
+about 3,000 spheres, unbreakable bonds, 2,000 steps of uniaxial loading at a
+fixed time step.  Loss = sum(((y - y*) / s)^2) over (secant E, secant nu)
+with y* the response at 1.1 x the bond modulus and 0.9 x kn/ks.
+Tolerances: autograd = J^T g to 1e-12 (the same numbers); against central
+differences with h = 1e-3 within 5% (the sensitivity test's 3% per
+derivative, combined); a batch of two equals the two single runs to 1e-9.
+"""
+from __future__ import annotations
+
+import importlib
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+AD = importlib.import_module("dem-rock-calibration_b200.autodiff")
+W = importlib.import_module("dem-rock-calibration_b200.workloads")
+pytestmark = pytest.mark.gpu
+
+STEPS = 2000
+BASE = [30.0, 2.5, 0.8, 50.0, 2.65]
+
+
+def _case():
+    d = (3000 * 0.068068 / (0.58 * math.pi * 0.5)) ** (1 / 3)
+    spec = W.uniaxial_cylinder(seed=3, diameter=d, height=2 * d)
+    r_min = float(spec.radii.min())
+    nu, rho, E = 0.25, 2.65, 50.0
+    t_r = math.pi * r_min * math.sqrt(2 * rho * (1 + nu)) / (math.sqrt(E) * (0.163 * nu + 0.8766))
+    return AD.ElasticCase(spec.xyz, spec.radii, spec.loading, STEPS, 0.2 * t_r)
+
+
+def test_autograd_gradient_matches_sensitivities_and_finite_differences():
+    case = _case()
+    tgt_p = np.array(BASE) * np.array([1.1, 0.9, 1.0, 1.0, 1.0])
+    target = torch.from_numpy(AD.elastic_run(tgt_p, case)[0][0])
+    scale = torch.tensor([1.0, 0.01], dtype=torch.float64)
+
+    def loss_of(y):
+        return (((y - target) / scale) ** 2).sum()
+
+    p = torch.tensor(BASE, dtype=torch.float64, requires_grad=True)
+    y = AD.elastic_response(p, case)
+    L = loss_of(y)
+    L.backward()
+    vals, jac = AD.elastic_run(np.array(BASE), case)
+    g_out = 2 * (torch.from_numpy(vals[0]) - target) / scale ** 2
+    assert torch.allclose(p.grad, g_out @ torch.from_numpy(jac[0]), rtol=1e-12, atol=0)
+    assert abs(float(y[0]) - vals[0][0]) <= 1e-12 * abs(vals[0][0])
+    h = 1e-3
+    for k in (0, 1, 2):
+        up, dn = np.array(BASE), np.array(BASE)
+        up[k] *= 1 + h
+        dn[k] *= 1 - h
+        fd = (float(loss_of(torch.from_numpy(AD.elastic_run(up, case)[0][0]))) -
+              float(loss_of(torch.from_numpy(AD.elastic_run(dn, case)[0][0])))) / (2 * h * BASE[k])
+        assert abs(float(p.grad[k]) - fd) <= 0.05 * abs(fd), (k, float(p.grad[k]), fd)
+
+
+def test_batched_response_equals_single_runs():
+    case = _case()
+    P = torch.tensor([BASE, [40.0, 2.0, 0.7, 50.0, 2.65]], dtype=torch.float64)
+    yb = AD.elastic_response(P, case)
+    for i in range(2):
+        ys = AD.elastic_response(P[i], case)
+        assert torch.allclose(yb[i], ys, rtol=1e-9, atol=0)

@@ -5,7 +5,8 @@ Tolerances:
   GEMM (FP32 accumulation of BF16 products, summation order free):
       |C - C_ref| <= 1e-5 * (|A| |B|^T) + 1e-6 elementwise
   BF16 activations: within one BF16 rounding of the FP32 reference
-      (relative 2^-8 of the value, plus 1e-6)
+      (relative 2^-8 of the value) plus the hardware tanh's error in GELU
+      (relative 1e-3 of the value, plus 1e-6)
   network gradients against the oracle's BF16 path: relative Frobenius error
       <= 2e-2 per layer (hidden activations rounded to BF16 on both sides may
       differ by one BF16 unit where the FP32 sums differ in their last bits)
@@ -65,9 +66,12 @@ def test_gemm_tn_against_torch_fp32(M, N, K, mode):
         ref = ref + bias
     assert torch.all((outf - ref).abs() <= bound), float((outf - ref).abs().max())
     if act:
-        fn = torch.nn.functional.gelu if mode == S.BIAS_GELU else torch.relu
+        if mode == S.BIAS_GELU:
+            fn = lambda x: torch.nn.functional.gelu(x, approximate="tanh")
+        else:
+            fn = torch.relu
         want = fn(ref)
-        assert torch.all((outh.float() - want).abs() <= want.abs() * 2.0 ** -8 + 1e-6 + fn(ref + bound).sub(
+        assert torch.all((outh.float() - want).abs() <= want.abs() * (2.0 ** -8 + 1e-3) + 1e-6 + fn(ref + bound).sub(
             fn(ref - bound)).abs())
 
 
@@ -103,13 +107,11 @@ def test_small_kernels():
         dz16 = torch.zeros(4000, dtype=torch.bfloat16, device="cuda")
         dz = torch.zeros(4000, device="cuda")
         assert L.dem_mlp_act_backward(_p(dh), _p(z), 4000, act, _p(dz16), _p(dz), _s()) == 0
-        zz = z.double()
-        if act == S.BIAS_GELU:
-            d = 0.5 * (1 + torch.erf(zz / 2 ** 0.5)) + zz * torch.exp(-0.5 * zz * zz) / (2 * np.pi) ** 0.5
-        else:
-            d = (zz > 0).double()
-        ref = dh.double() * d
-        assert torch.all((dz.double() - ref).abs() <= 1e-5 * ref.abs() + 1e-6)
+        d = torch.from_numpy(O.act_grad(z.double().cpu().numpy(), "gelu" if act == S.BIAS_GELU else "relu"))
+        ref = dh.double() * d.cuda()
+        # hardware tanh (relative error ~2^-11) inside the GELU derivative
+        tol = 1e-3 * dh.double().abs() * (1 + z.double().abs()) if act == S.BIAS_GELU else 1e-7 * ref.abs()
+        assert torch.all((dz.double() - ref).abs() <= tol + 1e-6)
         assert torch.equal(dz16, dz.to(torch.bfloat16))
     # MSE gradient and loss
     y = torch.randn(1000, 4, device="cuda", generator=g)

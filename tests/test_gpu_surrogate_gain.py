@@ -1,0 +1,56 @@
+"""What the trained network gains over the method without it.
+
+Targets: the simulated (UCS, chord modulus E, Poisson ratio) of two hidden
+parameter sets inside the sweep box, on one packed cylinder of about 2,000
+spheres (uniaxial loading to 70% post-peak).  Tolerances: 1% on E and on nu,
+5% on UCS (two FP32 runs of one parameter set differ by up to a few percent
+in UCS: force accumulation by floating-point atomics is not order-fixed and
+the post-peak fracture amplifies it; E and nu agree to about 0.5%).  Both
+methods start from the same 64 Latin-hypercube simulations and may spend 16
+simulations per round for up to four rounds:
+
+  with the network  surrogate.calibrate: fit the tensor-core MLP to all
+                    simulations so far, propose 16 parameter sets whose
+                    predicted properties are closest to the target, simulate
+                    them in one batched context, and accept a case only when
+                    it is within tolerance there and in a plain re-run (one
+                    sample per context)
+  without it        surrogate.random_search: 16 more Latin-hypercube points
+                    per round, the best simulated case kept
+
+Measured on a B200: the network reaches the tolerance within one or two
+rounds; the Latin hypercube stays several tolerances away.  The test asserts
+acceptance (confirmed by the plain re-run) and that at the same simulation
+budget the best case without the network is outside the tolerance and at
+least twice as far from the target in units of the tolerance.
+"""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+
+S = importlib.import_module("dem-rock-calibration_b200.surrogate")
+sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
+pytestmark = pytest.mark.gpu
+
+TOL = np.array([0.05, 0.01, 0.01])     # UCS, E, nu
+
+
+def test_surrogate_beats_latin_hypercube_at_equal_simulation_budget():
+    J = S.UniaxialJudge(n=2000, seed=5)
+    lo = np.array([v[0] for v in sweep.SWEEP_SPACE.values()])
+    hi = np.array([v[1] for v in sweep.SWEEP_SPACE.values()])
+    X0 = S.latin_box(64, lo, hi, 1)
+    Y0 = J(X0)
+    assert np.all(np.isfinite(Y0)) and np.all(Y0[:, 1] > 0)
+    hidden = S.latin_box(2, lo + 0.2 * (hi - lo), hi - 0.2 * (hi - lo), 99)
+    T = J(hidden)
+    for k in range(len(T)):
+        a = S.calibrate(J, T[k], lo, hi, rounds=4, per_round=16, tol=TOL, X0=X0, Y0=Y0, epochs=400, seed=k)
+        assert a.accepted and a.best_score <= 1.0, (k, a.scores)
+        assert S.score(a.confirmed_props, T[k], TOL)[0] <= 1.0
+        b = S.random_search(J, T[k], lo, hi, budget=a.simulations, tol=TOL, X0=X0, Y0=Y0, seed=k)
+        assert b.simulations >= a.simulations - 1
+        assert b.best_score > 1.0 and b.best_score >= 2 * a.best_score, (k, a.scores, b.scores)

@@ -236,6 +236,46 @@ def cpu_baseline(spec, nsteps: int, threads: int):
     return n * nsteps / el, el, L.lib().orc_get_threads()
 
 
+def reference_bpm_cpu(spec, pairs, seconds: float = 3.0, max_bonds: int = 20000):
+    """The reference's own CPU BPM routine, h_CalculateForceElastic
+    (md_calculateforcesbpm_cpu.cu:20-262), compiled from the reference sources
+    into oracle/_ref/libdemref.so: one call per directed bond slot of the
+    specimen's first max_bonds intact bonds (fresh bond state), on one host
+    thread (the routine prints on every call and is not re-entrant; its output
+    goes to /dev/null), for `seconds`.  Reported as directed-bond evaluations
+    per second and as the particle-steps/s of a BPM-only step (2 B evaluations
+    per step over the whole specimen).  None when the library is absent."""
+    if pairs is None:
+        return None
+    sys.path.insert(0, str(ROOT / "tests"))
+    try:
+        from oracle import lib as L
+        R = L.ref()
+    except Exception as e:                      # library not built / not shipped
+        return {"value": None, "unavailable": f"oracle/_ref/libdemref.so: {type(e).__name__}: {e}"[:200]}
+    bond = pairs["kind"] == 1
+    bi = np.ascontiguousarray(pairs["i"][bond][:max_bonds], np.uint32)
+    bj = np.ascontiguousarray(pairs["j"][bond][:max_bonds], np.uint32)
+    br = np.ascontiguousarray(pairs["state"][bond][:max_bonds, 15], np.float32)
+    n = spec.n
+    Rs = np.ascontiguousarray(spec.xyz, np.float32)
+    V = np.zeros(3 * n, np.float32)
+    W = np.zeros(3 * n, np.float32)
+    m = spec.material
+    ev, sec = C.c_double(), C.c_double()
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = R.refh_time_bpm_cpu(P(Rs), P(V), P(W), n, P(bi), P(bj), P(br), bi.size, 1e-3, m.E_bond,
+                             m.E_bond / m.kn_ks, m.Ec, m.Gc, seconds, C.byref(ev), C.byref(sec))
+    if rc != 0:
+        return {"value": None, "unavailable": f"refh_time_bpm_cpu returned {rc}"}
+    B = int(bond.sum())
+    return {"value": n * ev.value / (2.0 * B), "unit": UNIT, "cores": 1, "kind": "reference",
+            "bond_evaluations_per_s": ev.value, "seconds": sec.value,
+            "sample": f"h_CalculateForceElastic over {bi.size} of the {B} bonds of the {n}-sphere specimen, "
+                      f"both directions, repeated for {sec.value:.1f} s; value = particle-steps/s of a BPM-only "
+                      f"step (2 x {B} evaluations)"}
+
+
 def run_reference(args, ws, rank, local):
     """--impl reference: the CPU restatement on host cores (rank 0 only)."""
     if rank != 0:
@@ -252,6 +292,11 @@ def run_reference(args, ws, rank, local):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                              "sample": f"{steps} full loading steps of the {spec.n}-sphere specimen"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    ctx = dem.Context(device=local)
+    ctx.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
+    ctx.setup()
+    line["cpu_baseline_reference_bpm"] = reference_bpm_cpu(spec, ctx.pairs(0))
+    ctx.close()
     print(json.dumps(line), flush=True)
     return 0
 
@@ -500,6 +545,8 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="exact fixed-point force sums (bit-reproducible runs) instead of float atomics")
     ap.add_argument("--specimens", type=int, default=2,
                     help="specimens of the workload advanced together per GPU (2 discs: state above the L2)")
     args = ap.parse_args()
@@ -517,7 +564,8 @@ def main() -> int:
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
     spec = specs[0]
-    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks)
+    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
+                      deterministic=args.deterministic)
     sids = [ctx.add_sample(sp.material, sp.loading, sp.xyz, sp.radii) for sp in specs]
     ctx.setup()
     cnt = ctx.counts()
@@ -540,6 +588,7 @@ def main() -> int:
     peak, peak_kind = peaks()
     state_mb = (n_gpu * (7 * 16 + 8) + cnt["bonds"] * (8 + 4 * 16) + cnt["contacts"] * 24) / 1e6
     stale = sum(r["stale"] for r in res)
+    pairs0 = ctx.pairs(sids[0]) if rank == 0 and ws == 1 and not args.no_cpu else None
     ctx.close()
     # the same pipeline on one specimen alone (state inside the L2), for reference
     one = dem.Context(device=local, graph_steps=200)
@@ -566,12 +615,13 @@ def main() -> int:
     e2e_val = D.sum(n_gpu * args.steps / t_e2e)
     h2d = sum(sp.xyz.nbytes + sp.radii.nbytes for sp in specs)
     d2h = sum(r.nbytes + b.nbytes for r, b in recs) + len(specs) * 160
-    cpu = None
+    cpu = cpu_bpm = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, el, th = cpu_baseline(spec, args.cpu_steps, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                "sample": f"{args.cpu_steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
                          f"integration) of the {spec.n}-sphere specimen"}
+        cpu_bpm = reference_bpm_cpu(spec, pairs0)
     default_disc = args.workload == "brazilian_disc" and args.specimens == 2
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -585,6 +635,7 @@ def main() -> int:
                    "touching_contacts": prof["touching"], "parallelism": f"{ws} GPU(s), independent specimens",
                    "l2": f"inputs larger than L2: state {state_mb:.0f} MB per GPU vs 126 MB L2, no flush",
                    "packing": spec.pack, "stale_lists": stale,
+                   "force_sums": "fixed point (deterministic)" if args.deterministic else "float atomics",
                    "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
                                        "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
                                        "note": "state inside the L2"}},
@@ -601,6 +652,7 @@ def main() -> int:
                 "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e,
                 "note": "public API from host positions: upload, set-up, steps, results and records read back"},
         "cpu_baseline": cpu,
+        "cpu_baseline_reference_bpm": cpu_bpm,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -44,7 +44,7 @@ class DemError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("pair_block", C.c_uint32),
                 ("pair_grid", C.c_uint32), ("particle_block", C.c_uint32), ("graph_steps", C.c_uint32),
-                ("skin_factor", C.c_double), ("pair_min_blocks", C.c_uint32), ("reserved", C.c_uint32)]
+                ("skin_factor", C.c_double), ("pair_min_blocks", C.c_uint32), ("deterministic", C.c_uint32)]
 
 
 class Material(C.Structure):
@@ -66,7 +66,7 @@ class Loading(C.Structure):
                 ("dNsave", C.c_uint32), ("reserved2", C.c_uint32), ("max_steps", C.c_uint64)]
 
 
-SENS_NAMES = ("E_bond", "kn_ks", "bond_radius", "E", "rho")
+SENS_NAMES = ("E_bond", "kn_ks", "bond_radius", "E", "mu")
 
 
 class Sensitivity(C.Structure):
@@ -289,11 +289,12 @@ class Context:
     """One engine context: specimens advance together on one GPU."""
 
     def __init__(self, precision: int = 0, device: int = 0, pair_block: int = 0, pair_grid: int = 0,
-                 particle_block: int = 0, graph_steps: int = 0, skin_factor: float = 0.0, pair_min_blocks: int = 0):
+                 particle_block: int = 0, graph_steps: int = 0, skin_factor: float = 0.0, pair_min_blocks: int = 0,
+                 deterministic: bool = False):
         L = _lib()
         self._opt = Options(precision=precision, device=device, pair_block=pair_block, pair_grid=pair_grid,
                             particle_block=particle_block, graph_steps=graph_steps, skin_factor=skin_factor,
-                            pair_min_blocks=pair_min_blocks)
+                            pair_min_blocks=pair_min_blocks, deterministic=1 if deterministic else 0)
         h = C.c_void_p()
         _ck(L.dem_create(C.byref(self._opt), C.byref(h)), "dem_create")
         self._h = h

@@ -7,8 +7,8 @@ tangents carried through the same pair and particle kernels, breakage off)
 and returns its secant modulus and secant Poisson ratio at the last step;
 backward multiplies the incoming gradient by the 2 x 5 Jacobian the run
 produced.  The five parameters are, in order, the bond modulus E_bond (GPa),
-kn/ks, the bond-radius factor, the particle modulus E (GPa) and the density
-rho (mg/mm^3) - the order of SENS_NAMES.  A batch p of shape (B, 5) runs as B
+kn/ks, the bond-radius factor, the particle modulus E (GPa) and the sliding
+friction coefficient mu - the order of SENS_NAMES.  A batch p of shape (B, 5) runs as B
 samples of one context.
 
 This is the gradient path of a calibration: where the reference's conjugate
@@ -27,7 +27,7 @@ import torch
 from . import SENS_NAMES, Context, Loading
 from .workloads import rock_material
 
-PARAMS = ("E_bond", "kn_ks", "bond_radius_factor", "E", "rho")
+PARAMS = ("E_bond", "kn_ks", "bond_radius_factor", "E", "mu")
 
 
 @dataclass
@@ -66,7 +66,7 @@ def elastic_run(p: np.ndarray, case: ElasticCase):
         out = [ctx.sensitivities(i) for i in range(len(P))]
     finally:
         ctx.close()
-    assert list(SENS_NAMES) == ["E_bond", "kn_ks", "bond_radius", "E", "rho"]
+    assert list(SENS_NAMES) == ["E_bond", "kn_ks", "bond_radius", "E", "mu"]
     vals = np.array([[s["E_secant"], s["nu_secant"]] for s in out])
     jac = np.stack([np.stack([s["dE"], s["dnu"]]) for s in out])
     return vals, jac

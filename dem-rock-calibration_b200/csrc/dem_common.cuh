@@ -92,6 +92,21 @@ __device__ __forceinline__ double4 mk4(double a, double b, double c, double d) {
 __device__ __forceinline__ void acc3(float4* p, float x, float y, float z) {
   atomicAdd(p, make_float4(x, y, z, 0.0f));
 }
+// Deterministic accumulation (dem_options.deterministic, FP32): contributions
+// as 64-bit fixed point with a resolution of 2^-40 (an FP32 value of magnitude
+// 2^-16 or more converts exactly, smaller ones round to the nearest 2^-40) added
+// with integer atomics, so a particle's sum is exact and does not depend on the
+// order in which its pairs are processed.  Range +-8.4e6 in engine units.
+constexpr float kFixScale = 1099511627776.0f;        // 2^40
+constexpr double kFixInv = 1.0 / 1099511627776.0;
+__device__ __forceinline__ long long to_fix(float x) { return __float2ll_rn(x * kFixScale); }
+__device__ __forceinline__ long long to_fix(double x) { return __double2ll_rn(x * (double)kFixScale); }
+__device__ __forceinline__ void acc3q(long long* q, float x, float y, float z) {
+  unsigned long long* u = reinterpret_cast<unsigned long long*>(q);
+  atomicAdd(u + 0, (unsigned long long)to_fix(x));
+  atomicAdd(u + 1, (unsigned long long)to_fix(y));
+  atomicAdd(u + 2, (unsigned long long)to_fix(z));
+}
 __device__ __forceinline__ void acc3(double4* p, double x, double y, double z) {
   double* q = reinterpret_cast<double*>(p);
   atomicAdd(q + 0, x);

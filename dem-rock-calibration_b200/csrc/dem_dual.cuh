@@ -15,7 +15,7 @@
 namespace dem {
 
 // Parameters of the sensitivity build (derivative slots; DEM_SENS_* in b200dem.h).
-enum SensParam : int { kSensEBond = 0, kSensKnKs = 1, kSensBondRadius = 2, kSensE = 3, kSensRho = 4, kSensCount = 5 };
+enum SensParam : int { kSensEBond = 0, kSensKnKs = 1, kSensBondRadius = 2, kSensE = 3, kSensMu = 4, kSensCount = 5 };
 
 template <int K>
 struct Dual {

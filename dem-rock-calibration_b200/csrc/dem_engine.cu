@@ -134,6 +134,8 @@ class Engine final : public EngineBase {
     // warps per SM, measured 3% faster than 3 x 256 threads at 80 registers
     // and than 64 registers with spills), 2 for FP64, 1 for the sensitivity
     // build.
+    // deterministic force accumulation: FP32 only (FP64 keeps double atomics)
+    det_ = opt_.deterministic != 0 && sizeof(Real) == 4 && !DualK<Real>::K;
     opt_.pair_block = 256;
     constexpr bool kSmallBlocks = sizeof(Real) == 4 && !DualK<Real>::K;
     if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > (kSmallBlocks ? 8u : 4u))
@@ -200,10 +202,6 @@ class Engine final : public EngineBase {
         hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
         homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
         hmass[p] = (Real)m;
-        // sensitivity build: mass and dt/m, dt/I against the density
-        set_d(hmass[p], kSensRho, m / s.mat.rho);
-        set_d(hvel[p].w, kSensRho, -dtm / s.mat.rho);
-        set_d(homg[p].w, kSensRho, -dtI / s.mat.rho);
         hsid[p] = si;
         horig[p] = q;
       }
@@ -213,6 +211,10 @@ class Engine final : public EngineBase {
     CK(omg_.alloc(np_));
     CK(frc_.alloc(np_));
     CK(mom_.alloc(np_));
+    if (det_) {
+      CK(frcq_.alloc(4 * (size_t)np_));   // zero-filled
+      CK(momq_.alloc(4 * (size_t)np_));
+    }
     CK(wallO_.alloc(np_));
     CK(pos_ref_.alloc(np_));
     CK(mass_.alloc(np_));
@@ -448,6 +450,7 @@ class Engine final : public EngineBase {
       }
       p.pA = (Real)s.pot.p_A;
       p.mu = (Real)m.mu;
+      set_d(p.mu, kSensMu, 1.0);   // sensitivity build: sliding friction (pairs and platens)
       p.mur = (Real)m.mur;
       p.aa_far = (Real)s.pot.aa_farcut;
       const double skin = opt_.skin_factor * s.rmin;
@@ -817,6 +820,9 @@ class Engine final : public EngineBase {
     A.stat = stat_.p;
     A.lat = lat_.p;
     A.sfl_tan = sfl_tan_.p;
+    A.frcq = frcq_.p;
+    A.momq = momq_.p;
+    A.det = det_ ? 1 : 0;
     return A;
   }
 
@@ -931,6 +937,10 @@ class Engine final : public EngineBase {
     if (forces_dirty_) {
       CK(cudaMemsetAsync(frc_.p, 0, np_ * sizeof(V4), stream_));
       CK(cudaMemsetAsync(mom_.p, 0, np_ * sizeof(V4), stream_));
+      if (det_) {
+        CK(cudaMemsetAsync(frcq_.p, 0, 4 * (size_t)np_ * sizeof(long long), stream_));
+        CK(cudaMemsetAsync(momq_.p, 0, 4 * (size_t)np_ * sizeof(long long), stream_));
+      }
       forces_dirty_ = false;
     }
     if (contacts_dirty_) {
@@ -1492,6 +1502,8 @@ class Engine final : public EngineBase {
   uint32_t np_ = 0, nb_ = 0, nc_host_ = 0, ncell_ = 0;
 
   DBuf<V4> pos_, vel_, omg_, frc_, mom_, wallO_, pos_ref_;
+  DBuf<long long> frcq_, momq_;   // deterministic mode: fixed-point accumulators
+  bool det_ = false;
   DBuf<Real> mass_;
   DBuf<uint32_t> sid_, orig_;
   DBuf<uint2> b_ij_;

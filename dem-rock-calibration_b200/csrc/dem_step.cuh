@@ -56,7 +56,35 @@ struct StepArgs {
   float* stat;      // running maxima over blocks and steps (reset by the host)
   const uint8_t* lat;  // per particle: 1 = on the lateral surface near mid-height (or null)
   double* sfl_tan;     // sensitivity build only: per sample the platen-force tangents (see dem_dual.cuh)
+  // deterministic mode (FP32 only): fixed-point force and moment accumulators,
+  // 4 per particle (x, y, z, unused), used instead of frc / mom
+  long long* frcq;
+  long long* momq;
+  int det;
 };
+
+// Scatter of one contribution to a particle's force or moment accumulator:
+// a 128-bit float reduction, or in deterministic mode three fixed-point adds.
+template <class Real>
+__device__ __forceinline__ void acc_f(const StepArgs<Real>& A, uint32_t p, Real x, Real y, Real z) {
+  if constexpr (sizeof(Real) == 4) {
+    if (A.det) {
+      acc3q(A.frcq + 4 * (size_t)p, x, y, z);
+      return;
+    }
+  }
+  acc3(A.frc + p, x, y, z);
+}
+template <class Real>
+__device__ __forceinline__ void acc_m(const StepArgs<Real>& A, uint32_t p, Real x, Real y, Real z) {
+  if constexpr (sizeof(Real) == 4) {
+    if (A.det) {
+      acc3q(A.momq + 4 * (size_t)p, x, y, z);
+      return;
+    }
+  }
+  acc3(A.mom + p, x, y, z);
+}
 
 // Hooks of the sensitivity build (dem_dual.cuh overloads them for dual
 // numbers); for float and double they do nothing.
@@ -182,10 +210,10 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
 template <class Real>
 __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i, uint32_t j, const Real f[3],
                                              const Real mI[3], const Real mJ[3], bool dropI, bool dropJ) {
-  acc3(A.frc + i, f[0], f[1], f[2]);
-  acc3(A.frc + j, -f[0], -f[1], -f[2]);
-  if (!dropI) acc3(A.mom + i, mI[0], mI[1], mI[2]);
-  if (!dropJ) acc3(A.mom + j, mJ[0], mJ[1], mJ[2]);
+  acc_f(A, i, f[0], f[1], f[2]);
+  acc_f(A, j, -f[0], -f[1], -f[2]);
+  if (!dropI) acc_m(A, i, mI[0], mI[1], mI[2]);
+  if (!dropJ) acc_m(A, j, mJ[0], mJ[1], mJ[2]);
 }
 
 // One bond (i < j).  The arithmetic is that of d_CalculateForcesDEM_22 for the
@@ -284,10 +312,10 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, con
     const Real mu1 = half * (rz * ot0 - rx * ot2) * cef;
     const Real mu2 = half * (rx * ot1 - ry * ot0) * cef;
     // contributions: i gets (F, Mn+Mt+Mu), j gets (-F, -(Mn+Mt)+Mu)
-    acc3(A.frc + i, fn0 + ft0, fn1 + ft1, fn2 + ft2);
-    acc3(A.frc + j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2));
-    acc3(A.mom + i, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1, (tn2 + tt2) + mu2);
-    acc3(A.mom + j, mu0 - (tn0 + tt0), mu1 - (tn1 + tt1), mu2 - (tn2 + tt2));
+    acc_f(A, i, fn0 + ft0, fn1 + ft1, fn2 + ft2);
+    acc_f(A, j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2));
+    acc_m(A, i, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1, (tn2 + tt2) + mu2);
+    acc_m(A, j, mu0 - (tn0 + tt0), mu1 - (tn1 + tt1), mu2 - (tn2 + tt2));
     // break test (dd_CheckBreakConditionDEM_2)
     bool broke = false;
     if (!sp.nobreak) {
@@ -553,7 +581,25 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
     if (!C.done) {
       const SampleParams<Real>& sp = A.sp[s];
       V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
-      V4 f = A.frc[p], m = A.mom[p];
+      V4 f, m;
+      if constexpr (sizeof(Real) == 4) {
+        if (A.det) {
+          const longlong2 q0 = *reinterpret_cast<const longlong2*>(A.frcq + 4 * (size_t)p);
+          const long long q2 = A.frcq[4 * (size_t)p + 2];
+          const longlong2 u0 = *reinterpret_cast<const longlong2*>(A.momq + 4 * (size_t)p);
+          const long long u2 = A.momq[4 * (size_t)p + 2];
+          f = mk4((Real)((double)q0.x * kFixInv), (Real)((double)q0.y * kFixInv), (Real)((double)q2 * kFixInv),
+                  Real(0));
+          m = mk4((Real)((double)u0.x * kFixInv), (Real)((double)u0.y * kFixInv), (Real)((double)u2 * kFixInv),
+                  Real(0));
+        } else {
+          f = A.frc[p];
+          m = A.mom[p];
+        }
+      } else {
+        f = A.frc[p];
+        m = A.mom[p];
+      }
       Real F[3] = {f.x, f.y, f.z}, M[3] = {m.x, m.y, m.z};
       if (sp.axis >= 0) {
         // d_UniaxialCompression_hm / d_BrazilCompression_hm (md_compression_hm.cu:167-239)
@@ -619,9 +665,13 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       if (A.keep_forces) {
         A.frc[p] = mk4(F[0], F[1], F[2], z);
         A.mom[p] = mk4(M[0], M[1], M[2], z);
-      } else {
+      } else if (!A.det) {
         A.frc[p] = mk4(z, z, z, z);
         A.mom[p] = mk4(z, z, z, z);
+      }
+      if (A.det) {
+        *reinterpret_cast<longlong4*>(A.frcq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
+        *reinterpret_cast<longlong4*>(A.momq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
       }
       // neighbour-list validity: displacement since the last build.  A parked
       // particle interacts with nothing (all parked particles coincide, and
@@ -644,7 +694,32 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       }
     }
     // per-sample double sums: a full warp of one sample reduces with shuffles and
-    // issues one atomic; otherwise each contributing lane adds its own value
+    // issues one atomic; otherwise each contributing lane adds its own value.  In
+    // deterministic mode every particle's terms are first rounded to fixed point
+    // and summed as integers (exact, independent of the warp a particle falls in).
+    if (A.det) {
+      long long qb = to_fix(sb), qt = to_fix(st), ql = to_fix(sl);
+      const unsigned fm = __activemask();
+      bool uni = false;
+      if (fm == 0xFFFFFFFFu) {
+        const uint32_t s0 = __shfl_sync(fm, s, 0);
+        uni = __all_sync(fm, s == s0);
+      }
+      if (uni) {
+        for (int off = 16; off > 0; off >>= 1) {
+          qb += __shfl_xor_sync(fm, qb, off);
+          qt += __shfl_xor_sync(fm, qt, off);
+          ql += __shfl_xor_sync(fm, ql, off);
+        }
+      }
+      if (!uni || (threadIdx.x & 31) == 0) {
+        unsigned long long* q = reinterpret_cast<unsigned long long*>(A.ctl[s].sFLq);
+        if (qb) atomicAdd(q + 0, (unsigned long long)qb);
+        if (qt) atomicAdd(q + 1, (unsigned long long)qt);
+        if (ql) atomicAdd(reinterpret_cast<unsigned long long*>(&A.ctl[s].lat_q), (unsigned long long)ql);
+      }
+      continue;
+    }
     const unsigned full = __activemask();
     bool uniform = false;
     if (full == 0xFFFFFFFFu) {
@@ -703,6 +778,11 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
     SampleCtl& C = A.ctl[s];
     if (!C.done) {
+      // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
+      C.sFL[0] += (double)C.sFLq[0] * kFixInv;
+      C.sFL[1] += (double)C.sFLq[1] * kFixInv;
+      C.lat_sum += (double)C.lat_q * kFixInv;
+      C.sFLq[0] = C.sFLq[1] = C.lat_q = 0;
       tangent_step_end(A, C, s);
       controller_step(C);
     }

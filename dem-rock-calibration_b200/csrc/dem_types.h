@@ -67,6 +67,11 @@ struct SampleCtl {
   double* rec_lat;          // Nsave: mean radial distance of the marked particles
   uint32_t lat_count;       // marked particles (0: no lateral record)
   uint32_t lat_pad;
+  // deterministic mode: the platen and lateral sums of the step in 2^-40 fixed
+  // point, folded into sFL / lat_sum by the controller
+  long long sFLq[2];
+  long long lat_q;
+  long long q_pad;
 };
 
 }  // namespace dem

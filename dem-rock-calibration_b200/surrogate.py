@@ -427,14 +427,17 @@ PROPS = ("UCS", "E", "nu")
 class UniaxialJudge:
     """Uniaxial tests of one packed cylinder (about n spheres) under many
     parameter sets (rows in the order of sweep.SWEEP_SPACE) in one batched
-    context.  Every case draws its bond strengths with the same seed, so the
-    macro properties are a deterministic function of the parameters.  Returns
-    rows (UCS GPa, chord modulus GPa, Poisson ratio)."""
+    context.  Every case draws its bond strengths with the same seed, and the
+    context runs in deterministic mode (exact fixed-point force sums), so the
+    macro properties are a reproducible function of the parameters alone - the
+    same in a batch as in a plain one-sample run.  Returns rows (UCS GPa, chord
+    modulus GPa, Poisson ratio)."""
 
     def __init__(self, n: int = 2000, seed: int = 5, velocity_m_s: float = 0.1, max_steps: int = 400000,
-                 device: int = 0):
+                 device: int = 0, deterministic: bool = True):
         from . import sweep
         self.sweep, self.seed, self.device = sweep, seed, device
+        self.deterministic = deterministic
         self.velocity, self.max_steps = velocity_m_s, max_steps
         self.xyz, self.rad, _, self.box, self.size_real, self.center_real = sweep.cylinder(n, seed, device=device)
         self.keys = list(sweep.SWEEP_SPACE)
@@ -445,7 +448,7 @@ class UniaxialJudge:
         from . import TEST_UNIAXIAL, VELOCITY, Context, loading
         P = np.atleast_2d(np.asarray(P, np.float64))
         r_min, r_mean = float(self.rad.min()), float(self.rad.mean())
-        ctx = Context(device=self.device)
+        ctx = Context(device=self.device, deterministic=self.deterministic)
         try:
             for row in P:
                 p = dict(zip(self.keys, row))

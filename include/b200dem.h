@@ -68,7 +68,10 @@ typedef struct {
   uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
                                (1..4 of 256 threads, FP32 also 5..8 of 128 threads;
                                0: 7 for FP32, 2 for FP64, 1 for the sensitivity build) */
-  uint32_t reserved;
+  uint32_t deterministic; /* 1: FP32 force and platen sums in exact 64-bit fixed point
+                             (2^-40 resolution), so a run is bit-reproducible and a
+                             sample's results do not depend on the other samples of
+                             its context; 0: floating-point atomics (faster) */
 } dem_options;
 
 /* Micro-parameters of one specimen.  The first block is the reference's
@@ -180,7 +183,7 @@ int dem_get_record(dem_ctx* ctx, int32_t sample, double* rec, uint32_t* bonds, u
 #define DEM_SENS_KN_KS 1         /* dem_material.kn_ks */
 #define DEM_SENS_BOND_RADIUS 2   /* bond_radius_factor (or the absolute b_r when b_r > 0) */
 #define DEM_SENS_E 3             /* particle E (contacts, platens) */
-#define DEM_SENS_RHO 4           /* density */
+#define DEM_SENS_MU 4            /* sliding friction coefficient mu (pairs and platens) */
 #define DEM_SENS_COUNT 5
 typedef struct {
   double strain;                 /* axial strain at the last step, compression positive */

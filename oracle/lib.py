@@ -171,6 +171,8 @@ def _declare_ref(L):
     L.refh_cg_start_parameters.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp]
     L.refh_cg_new_parameters2.argtypes = [_vp] * 7 + [C.c_int, C.c_double, _vp, _vp]
     L.refh_run_test.argtypes = [C.c_int, C.c_char_p, C.c_char_p, C.POINTER(TestParams), C.POINTER(TestResult)]
+    L.refh_time_bpm_cpu.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp, _u32] + [C.c_float] * 5 + [
+        C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
 
 
 def sfx(a) -> str:

@@ -12,10 +12,13 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
+#include <fcntl.h>
 #include <unistd.h>
 #include <sys/stat.h>
 
@@ -83,6 +86,15 @@ void setup_task(md_task_data& td, uint32_t N, float a, uint32_t nx, uint32_t ny,
 }
 
 }  // namespace
+
+// The definition in md_calculateforcesbpm_cpu.cu:20-24 (per directed slot, with
+// the slot and particle indices and the bond type) differs from the overload
+// md.h:134 declares (never defined); this prototype matches the definition.
+void h_CalculateForceElastic(const float* R, const float* V, const float* W, float* F, float* M, const float* ab_r,
+                             const float* _1d_iL, const float* AxialMoment, float3* Rij, float3* OverlapTau,
+                             float3* Mijn, float3* Mijt, float3* Fij, const uint N, const uint idx, const uint jdx,
+                             const uint kdx, const float dt, const float m_E, const float m_G, const float m_Gcritn,
+                             const float m_Gcritt, uint type);
 
 extern "C" {
 
@@ -562,6 +574,69 @@ int refh_cg_new_parameters2(const double* params, double* variation, const doubl
     ddfun[i] = t.ddFunctional[i];
   }
   for (int j = 0; j < 4; ++j) functional[j] = t.Functional[j];
+  return 0;
+}
+
+// Times the reference's CPU BPM routine h_CalculateForceElastic
+// (md_calculateforcesbpm_cpu.cu:20-262, declared md.h:134) on one host thread:
+// one call per directed bonded slot (i -> j and j -> i for every bond of bi/bj),
+// repeated over the bond list until at least min_seconds have passed.  The
+// routine prints several lines per call (printf and std::cerr), so stdout and
+// stderr are sent to /dev/null for the timed loop and restored afterwards.  Slot state starts as a fresh bond:
+// previous direction = current direction, 1/L0 from the positions, zero
+// histories; br is the bond radius per bond, the axial moment pi br^4 / 2.
+// Returns the directed-slot evaluations per second and the seconds spent.
+int refh_time_bpm_cpu(const float* R, const float* V, const float* W, uint32_t N, const uint32_t* bi,
+                      const uint32_t* bj, const float* br, uint32_t nb, float dt, float m_E, float m_G, float Gcn,
+                      float Gct, double min_seconds, double* evals_per_s, double* seconds) {
+  if (!R || !V || !W || !bi || !bj || !br || nb == 0 || N == 0) return -1;
+  const size_t ns = 2 * (size_t)nb;
+  std::vector<float> F(3 * (size_t)N, 0.f), M(3 * (size_t)N, 0.f), ab_r(ns), inv_l(ns), axial(ns);
+  std::vector<float3> Rij(ns), Ot(ns), Mn(ns), Mt(ns), Fij(ns);
+  std::vector<uint32_t> idx(ns), jdx(ns);
+  for (size_t b = 0; b < nb; ++b) {
+    for (int d = 0; d < 2; ++d) {
+      const size_t k = 2 * b + d;
+      const uint32_t i = d ? bj[b] : bi[b], j = d ? bi[b] : bj[b];
+      idx[k] = i;
+      jdx[k] = j;
+      const float x = R[j] - R[i], y = R[j + N] - R[i + N], z = R[j + 2 * N] - R[i + 2 * N];
+      const float r = std::sqrt(x * x + y * y + z * z);
+      const float ir = r > 0.f ? 1.f / r : 0.f;
+      Rij[k] = make_float3(x * ir, y * ir, z * ir);
+      inv_l[k] = ir;
+      ab_r[k] = br[b];
+      axial[k] = 0.5f * 3.14159265f * br[b] * br[b] * br[b] * br[b];
+      Ot[k] = Mn[k] = Mt[k] = Fij[k] = make_float3(0.f, 0.f, 0.f);
+    }
+  }
+  fflush(stdout);
+  fflush(stderr);
+  const int saved = dup(1), saved2 = dup(2);
+  const int devnull = open("/dev/null", O_WRONLY);
+  if (saved < 0 || saved2 < 0 || devnull < 0) return -2;
+  dup2(devnull, 1);
+  dup2(devnull, 2);
+  size_t calls = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  double el = 0.0;
+  do {
+    for (size_t k = 0; k < ns; ++k)
+      h_CalculateForceElastic(R, V, W, F.data(), M.data(), ab_r.data(), inv_l.data(), axial.data(), Rij.data(),
+                              Ot.data(), Mn.data(), Mt.data(), Fij.data(), N, idx[k], jdx[k], (uint)k, dt, m_E,
+                              m_G, Gcn, Gct, 1u);
+    calls += ns;
+    el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  } while (el < min_seconds);
+  fflush(stdout);
+  fflush(stderr);
+  dup2(saved, 1);
+  dup2(saved2, 2);
+  close(saved);
+  close(saved2);
+  close(devnull);
+  *evals_per_s = (double)calls / el;
+  *seconds = el;
   return 0;
 }
 

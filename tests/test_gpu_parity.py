@@ -42,8 +42,8 @@ def _loading(c: T.RefCase, test=None, **kw):
                        cond_fracture=k["condfract"], **kw)
 
 
-def engine_for(c: T.RefCase, test=None, precision=0, **ext):
-    ctx = dem.Context(precision=precision)
+def engine_for(c: T.RefCase, test=None, precision=0, deterministic=False, **ext):
+    ctx = dem.Context(precision=precision, deterministic=deterministic)
     sid = ctx.add_sample(_material(c, **ext), _loading(c, test), c.R)
     ctx.setup()
     return ctx, sid
@@ -184,8 +184,9 @@ def compare_pairs_to_slots(pr, st: sim.RefState, bitwise: bool, tol_rel=1e-4):
     return n_cmp, worst
 
 
+@pytest.mark.parametrize("det", [False, True], ids=["float-atomics", "deterministic"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_step_matches_oracle_and_reference(name):
+def test_step_matches_oracle_and_reference(name, det):
     c = T.ref_case(**SMALL, **CASES[name])
     g = load(f"step_{name}")
     c.sc.wall_top = float(g["wall_top"])
@@ -196,7 +197,7 @@ def test_step_matches_oracle_and_reference(name):
     orc = st_in.copy()
     out = sim.oracle_step(orc, c.sc, want_abs=True)
     # engine
-    ctx, sid = engine_for(c)
+    ctx, sid = engine_for(c, deterministic=det)
     load_state(ctx, sid, c, st_in)
     ctx.set_platens(sid, c.sc.wall_top, c.sc.wall_bot, c.sc.wall_V)
     ctx.step_stages(dem.STAGE_PAIRS | dem.STAGE_PARTICLES | dem.STAGE_KEEP_FORCES)

@@ -320,6 +320,9 @@ def run_sweep(args, ws, rank, local):
     for c in sw.cases:
         ctx.add_sample(c.material, c.loading, c.xyz, c.radii)
     ctx.setup()
+    # launch schedules chosen by the engine's autotuner on this workload (the
+    # tuning steps advance the run like any other steps)
+    tune = ctx.autotune(max(20, min(args.steps, 100))) if args.pair_min_blocks == 0 else None
     ctx.run_timed(args.warmup)
     D.barrier()
     clk = Clocks(local)
@@ -352,6 +355,7 @@ def run_sweep(args, ws, rank, local):
                                   "device_ms": seq["device_ms"],
                                   "note": "the same cases one context at a time (device time summed)"},
                    "batched_over_sequential": value / D.sum(seq_rate),
+                   "autotune": tune,
                    "l2": "inputs larger than L2, no flush"},
         "gpu_launches": 2 * args.steps, "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

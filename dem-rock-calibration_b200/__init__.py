@@ -101,6 +101,12 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_int), ("pair_min_blocks", C.c_uint32 * 16), ("particle_block", C.c_uint32 * 16),
+                ("ms_per_step", C.c_double * 16), ("chosen_pair_min_blocks", C.c_uint32),
+                ("chosen_particle_block", C.c_uint32), ("chosen_ms_per_step", C.c_double)]
+
+
 _LIB = None
 _vp, _u32, _i32, _u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
 
@@ -131,6 +137,7 @@ def _declare(L):
     L.dem_rebuild_contacts.argtypes = [_vp]
     L.dem_run_timed.argtypes = [_vp, _u64, P(C.c_double)]
     L.dem_profile.argtypes = [_vp, _u32, P(C.c_double), P(C.c_double), P(C.c_double)]
+    L.dem_autotune.argtypes = [_vp, _u32, P(TuneReport)]
     L.dem_create_cylinder_sample.argtypes = [P(PackParams), _vp, _vp, _u32, P(_u32), P(PackReport)]
     L.dem_last_error_detail.restype = C.c_char_p
     L.dem_last_error_detail.argtypes = []
@@ -425,6 +432,16 @@ class Context:
         ms = C.c_double()
         _ck(_lib().dem_run_timed(self._h, nsteps, C.byref(ms)), "dem_run_timed")
         return ms.value
+
+    def autotune(self, steps: int = 200) -> dict:
+        """Times the launch-schedule candidates on the next steps of this run
+        (steps per candidate; the simulation advances) and keeps the fastest."""
+        r = TuneReport()
+        _ck(_lib().dem_autotune(self._h, steps, C.byref(r)), "dem_autotune")
+        n = r.candidates
+        return dict(candidates=[(r.pair_min_blocks[k], r.particle_block[k], r.ms_per_step[k]) for k in range(n)],
+                    pair_min_blocks=r.chosen_pair_min_blocks, particle_block=r.chosen_particle_block,
+                    ms_per_step=r.chosen_ms_per_step)
 
     def profile(self, nsteps: int) -> dict:
         a, b, t = C.c_double(), C.c_double(), C.c_double()

@@ -41,6 +41,7 @@ class ElasticCase:
     dt: float
     fixed: dict | None = None
     device: int = 0
+    deterministic: bool = True     # exact fixed-point force sums: repeatable values and derivatives
 
 
 def _material(case: ElasticCase, row):
@@ -55,7 +56,7 @@ def _material(case: ElasticCase, row):
 def elastic_run(p: np.ndarray, case: ElasticCase):
     """(values (B, 2), Jacobians (B, 2, 5)) of (E_secant, nu_secant)."""
     P = np.atleast_2d(np.asarray(p, np.float64))
-    ctx = Context(precision=2, device=case.device)
+    ctx = Context(precision=2, device=case.device, deterministic=case.deterministic)
     try:
         ld = Loading.from_buffer_copy(case.loading)
         ld.max_steps = case.steps

@@ -149,6 +149,7 @@ struct PairSearch {
   uint32_t* out_j;        // fill: partner indices (kModeRefSet: np*cap slots)
   uint32_t cap;           // max pairs per particle kept in registers / slots
   uint32_t* overflow;     // number of particles whose pairs exceeded cap
+  const uint32_t* done;   // kModeContact, optional: per sample 1 = finished (its contacts are not listed)
 };
 
 template <class Real>
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
     const auto xi = ld4(S.pos + i);
     const uint32_t s = S.sid[i];
     const Grid<Real> g = S.grids[s];
-    if (at_hidden(g, xi)) {
+    if (at_hidden(g, xi) || (S.done && S.done[s])) {
       if (!kFill) S.count[i] = 0;
       continue;
     }

@@ -154,6 +154,9 @@ int dem_run_timed(dem_ctx* ctx, uint64_t nsteps, double* ms) { CTX_CALL(ctx->e->
 int dem_profile(dem_ctx* ctx, uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching) {
   CTX_CALL(ctx->e->profile(nsteps, pair_ms, particle_ms, touching));
 }
+int dem_autotune(dem_ctx* ctx, uint32_t steps, dem_tune_report* report) {
+  CTX_CALL(ctx->e->autotune(steps, report));
+}
 
 int dem_ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
                   uint32_t* CIs, uint32_t* pnC) {

@@ -107,11 +107,28 @@ __device__ __forceinline__ void acc3q(long long* q, float x, float y, float z) {
   atomicAdd(u + 1, (unsigned long long)to_fix(y));
   atomicAdd(u + 2, (unsigned long long)to_fix(z));
 }
+// FP64 and sensitivity builds: the same scheme with 2^-50 resolution (range
+// +-8192), stored in place of the double accumulators (same width; a zero
+// double is a zero integer, so the accumulators reset as before).
+constexpr double kFixScaleD = 1125899906842624.0;    // 2^50
+constexpr double kFixInvD = 1.0 / 1125899906842624.0;
+__device__ __forceinline__ void fix_add(double* slot, double x) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(slot), (unsigned long long)__double2ll_rn(x * kFixScaleD));
+}
+__device__ __forceinline__ double fix_val(double slot) { return (double)__double_as_longlong(slot) * kFixInvD; }
 __device__ __forceinline__ void acc3(double4* p, double x, double y, double z) {
   double* q = reinterpret_cast<double*>(p);
   atomicAdd(q + 0, x);
   atomicAdd(q + 1, y);
   atomicAdd(q + 2, z);
+}
+__device__ __forceinline__ void acc3_fix(double4* p, double x, double y, double z) {
+  fix_add(&p->x, x);
+  fix_add(&p->y, y);
+  fix_add(&p->z, z);
+}
+__device__ __forceinline__ double4 unfix4(const double4& a) {
+  return make_double4(fix_val(a.x), fix_val(a.y), fix_val(a.z), 0.0);
 }
 
 // Counter-based normal deviates for per-bond properties: splitmix64 mixing of

@@ -184,6 +184,30 @@ __device__ __forceinline__ void acc3(Dual4<K>* p, const Dual<K>& a, const Dual<K
   acc1(&p->y, b);
   acc1(&p->z, c);
 }
+// deterministic mode: every value and derivative slot in 2^-50 fixed point
+template <int K>
+__device__ __forceinline__ void acc1_fix(Dual<K>* p, const Dual<K>& a) {
+  fix_add(&p->v, a.v);
+  for (int k = 0; k < K; ++k)
+    if (a.d[k] != 0.0) fix_add(&p->d[k], a.d[k]);
+}
+template <int K>
+__device__ __forceinline__ void acc3_fix(Dual4<K>* p, const Dual<K>& a, const Dual<K>& b, const Dual<K>& c) {
+  acc1_fix(&p->x, a);
+  acc1_fix(&p->y, b);
+  acc1_fix(&p->z, c);
+}
+template <int K>
+__device__ __forceinline__ Dual<K> unfix1(const Dual<K>& a) {
+  Dual<K> r;
+  r.v = fix_val(a.v);
+  for (int k = 0; k < K; ++k) r.d[k] = fix_val(a.d[k]);
+  return r;
+}
+template <int K>
+__device__ __forceinline__ Dual4<K> unfix4(const Dual4<K>& a) {
+  return Dual4<K>{unfix1(a.x), unfix1(a.y), unfix1(a.z), Dual<K>(0.0)};
+}
 template <int K>
 __host__ __device__ __forceinline__ Dual<K> norm3(const Dual<K>& x, const Dual<K>& y, const Dual<K>& z) {
   return sqrt((x * x + y * y) + z * z);
@@ -196,13 +220,18 @@ template <int K>
 __device__ __forceinline__ void tangent_wall(const StepArgs<Dual<K>>& A, uint32_t s, int which, const Dual<K>& f) {
   double* t = A.sfl_tan + (size_t)s * (4 * K + 2) + which * K;
   for (int k = 0; k < K; ++k)
-    if (f.d[k] != 0.0) atomicAdd(t + k, -f.d[k]);
+    if (f.d[k] != 0.0) {
+      if (A.det)
+        fix_add(t + k, -f.d[k]);
+      else
+        atomicAdd(t + k, -f.d[k]);
+    }
 }
 template <int K>
 __device__ __forceinline__ void tangent_step_end(const StepArgs<Dual<K>>& A, const SampleCtl& C, uint32_t s) {
   double* t = A.sfl_tan + (size_t)s * (4 * K + 2);
   for (int k = 0; k < 2 * K; ++k) {
-    t[2 * K + k] = t[k];
+    t[2 * K + k] = A.det ? fix_val(t[k]) : t[k];
     t[k] = 0.0;
   }
   t[4 * K] = C.sFL[0];

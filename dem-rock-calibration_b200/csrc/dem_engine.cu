@@ -134,19 +134,11 @@ class Engine final : public EngineBase {
     // warps per SM, measured 3% faster than 3 x 256 threads at 80 registers
     // and than 64 registers with spills), 2 for FP64, 1 for the sensitivity
     // build.
-    // deterministic force accumulation: FP32 only (FP64 keeps double atomics)
-    det_ = opt_.deterministic != 0 && sizeof(Real) == 4 && !DualK<Real>::K;
-    opt_.pair_block = 256;
-    constexpr bool kSmallBlocks = sizeof(Real) == 4 && !DualK<Real>::K;
-    if (opt_.pair_min_blocks == 0 || opt_.pair_min_blocks > (kSmallBlocks ? 8u : 4u))
-      opt_.pair_min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 7 : 2);
-    if (opt_.pair_min_blocks > 4) opt_.pair_block = 128;
-    pair_kernel_ = pair_kernel_ptr(opt_.pair_min_blocks);
-    if (!opt_.pair_grid) {
-      int per_sm = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel_, (int)opt_.pair_block, 0));
-      opt_.pair_grid = (uint32_t)num_sms_ * (uint32_t)std::max(per_sm, 1);
-    }
+    // deterministic force accumulation: fixed point (FP32: separate 64-bit
+    // accumulators; FP64 and the sensitivity build: in place of the doubles)
+    det_ = opt_.deterministic != 0;
+    user_grid_ = opt_.pair_grid != 0;
+    RC(set_pair_config(opt_.pair_min_blocks));
     if (!opt_.particle_block) opt_.particle_block = 256;
     if (!opt_.graph_steps) opt_.graph_steps = 100;
     if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.25;
@@ -211,7 +203,7 @@ class Engine final : public EngineBase {
     CK(omg_.alloc(np_));
     CK(frc_.alloc(np_));
     CK(mom_.alloc(np_));
-    if (det_) {
+    if (det_ && sizeof(Real) == 4) {
       CK(frcq_.alloc(4 * (size_t)np_));   // zero-filled
       CK(momq_.alloc(4 * (size_t)np_));
     }
@@ -648,6 +640,66 @@ class Engine final : public EngineBase {
     CK(cudaMemcpyAsync(hc.data(), counts.p, S_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     for (uint32_t si = 0; si < S_; ++si) samples_[si].bonds_initial = hc[si];
+    // bond range of every sample (bonds are stored in particle order, and the
+    // particles of a sample are contiguous)
+    std::vector<uint32_t> row(np_ + 1);
+    CK(cudaMemcpy(row.data(), b_row_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    sb_begin_.assign(S_, 0);
+    sb_end_.assign(S_, 0);
+    for (uint32_t si = 0; si < S_; ++si) {
+      sb_begin_[si] = row[samples_[si].p_begin];
+      sb_end_[si] = row[samples_[si].p_begin + samples_[si].n];
+    }
+    tiles_.release();
+    ntiles_.release();
+    tiles_on_ = false;
+    ndone_seen_ = 0;
+    return DEM_OK;
+  }
+
+  // Batched runs: finished samples stop costing work.  Their contacts are left
+  // out of the next contact-list builds, and once their bonds make up an
+  // eighth of all bonds the pair kernel visits only the bond tiles that hold a
+  // bond of an unfinished sample (a tile list read through one indirection;
+  // the graph is captured again with it).  A finished sample's state no longer
+  // changes either way (its pairs and particles are skipped), so results are
+  // unchanged.  Called after read_flags, with the stream idle.
+  int update_tiles() {
+    const uint32_t S = (uint32_t)samples_.size();
+    uint32_t nd = 0;
+    size_t done_bonds = 0;
+    for (uint32_t si = 0; si < S; ++si)
+      if (hctl_[si].done) {
+        ++nd;
+        if (si < sb_end_.size()) done_bonds += sb_end_[si] - sb_begin_[si];
+      }
+    if (nd == ndone_seen_) return DEM_OK;
+    ndone_seen_ = nd;
+    if (!sdone_.p) CK(sdone_.alloc(S));
+    std::vector<uint32_t> hd(S);
+    for (uint32_t si = 0; si < S; ++si) hd[si] = hctl_[si].done ? 1u : 0u;
+    CK(cudaMemcpy(sdone_.p, hd.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (nb_ == 0 || 8 * done_bonds < (size_t)nb_) return DEM_OK;
+    const uint32_t tile = opt_.pair_block, T = (nb_ + tile - 1) / tile;
+    std::vector<uint8_t> act(T, 0);
+    for (uint32_t si = 0; si < S; ++si)
+      if (!hd[si] && sb_end_[si] > sb_begin_[si])
+        for (uint32_t t = sb_begin_[si] / tile; t <= (sb_end_[si] - 1) / tile; ++t) act[t] = 1;
+    std::vector<uint32_t> list;
+    list.reserve(T);
+    for (uint32_t t = 0; t < T; ++t)
+      if (act[t]) list.push_back(t);
+    if (!tiles_.p) {
+      CK(tiles_.alloc(T));
+      CK(ntiles_.alloc(1));
+    }
+    const uint32_t cnt = (uint32_t)list.size();
+    if (cnt) CK(cudaMemcpy(tiles_.p, list.data(), cnt * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ntiles_.p, &cnt, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!tiles_on_) {
+      tiles_on_ = true;
+      invalidate_graph();
+    }
     return DEM_OK;
   }
 
@@ -657,6 +709,7 @@ class Engine final : public EngineBase {
     RC(bin_cells());
     PairSearch<Real> S = search_args(kModeContact);
     S.gap = skin_.p;
+    S.done = sdone_.p;
     S.b_row = b_row_.p;
     S.b_ij = b_ij_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
@@ -823,7 +876,77 @@ class Engine final : public EngineBase {
     A.frcq = frcq_.p;
     A.momq = momq_.p;
     A.det = det_ ? 1 : 0;
+    A.tiles = tiles_on_ ? tiles_.p : nullptr;
+    A.ntiles = tiles_on_ ? ntiles_.p : nullptr;
     return A;
+  }
+
+  // Pair-kernel variant (register budget and block size) and its grid: all
+  // co-resident blocks unless the caller fixed the grid.  Changing it drops
+  // the captured graph and the bond-tile list (tiles are blocks).
+  int set_pair_config(uint32_t min_blocks) {
+    constexpr bool kSmallBlocks = sizeof(Real) == 4 && !DualK<Real>::K;
+    if (min_blocks == 0 || min_blocks > (kSmallBlocks ? 8u : 4u))
+      min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 7 : 2);
+    opt_.pair_min_blocks = min_blocks;
+    opt_.pair_block = min_blocks > 4 ? 128 : 256;
+    pair_kernel_ = pair_kernel_ptr(min_blocks);
+    if (!user_grid_) {
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel_, (int)opt_.pair_block, 0));
+      opt_.pair_grid = (uint32_t)num_sms_ * (uint32_t)std::max(per_sm, 1);
+    }
+    invalidate_graph();
+    tiles_on_ = false;
+    ndone_seen_ = 0;
+    return DEM_OK;
+  }
+
+  // Launch-schedule autotuner: advances the run by `steps` steps per candidate
+  // (real steps of the simulation: the state moves on exactly as under a plain
+  // run), timing each candidate's steps with CUDA events, and keeps the
+  // fastest.  Candidates: the pair kernel's register budgets (FP32: 3 x 256
+  // threads, 7, 6, 5 x 128 threads and 4 x 256 threads; FP64: 2, 1, 3) crossed
+  // with particle-kernel blocks of 128 and 256 threads.
+  int autotune(uint32_t steps, dem_tune_report* rep) override {
+    if (!setup_done_ || steps == 0 || !rep) return DEM_ERR_ARG;
+    std::vector<uint32_t> pairs;
+    if (DualK<Real>::K)
+      pairs = {1, 2};
+    else if (sizeof(Real) == 4)
+      pairs = {7, 3, 6, 5, 4};
+    else
+      pairs = {2, 1, 3};
+    const uint32_t parts[2] = {256, 128};
+    std::memset(rep, 0, sizeof(*rep));
+    double best = 1e300;
+    uint32_t bp = opt_.pair_min_blocks, bq = opt_.particle_block;
+    int k = 0;
+    for (uint32_t pm : pairs)
+      for (uint32_t pb : parts) {
+        RC(set_pair_config(pm));
+        opt_.particle_block = pb;
+        double ms = 0.0;
+        RC(run_timed(std::min<uint64_t>(steps, opt_.graph_steps), &ms));   // warm-up and capture
+        RC(run_timed(steps, &ms));
+        if (k < DEM_TUNE_MAX) {
+          rep->pair_min_blocks[k] = pm;
+          rep->particle_block[k] = pb;
+          rep->ms_per_step[k] = ms / steps;
+        }
+        ++k;
+        if (ms < best) {
+          best = ms;
+          bp = pm;
+          bq = pb;
+        }
+      }
+    rep->candidates = std::min(k, (int)DEM_TUNE_MAX);
+    rep->chosen_pair_min_blocks = bp;
+    rep->chosen_particle_block = bq;
+    rep->chosen_ms_per_step = best / steps;
+    opt_.particle_block = bq;
+    return set_pair_config(bp);
   }
 
   static const void* pair_kernel_ptr(uint32_t min_blocks) {
@@ -937,7 +1060,7 @@ class Engine final : public EngineBase {
     if (forces_dirty_) {
       CK(cudaMemsetAsync(frc_.p, 0, np_ * sizeof(V4), stream_));
       CK(cudaMemsetAsync(mom_.p, 0, np_ * sizeof(V4), stream_));
-      if (det_) {
+      if (det_ && frcq_.p) {
         CK(cudaMemsetAsync(frcq_.p, 0, 4 * (size_t)np_ * sizeof(long long), stream_));
         CK(cudaMemsetAsync(momq_.p, 0, 4 * (size_t)np_ * sizeof(long long), stream_));
       }
@@ -955,6 +1078,7 @@ class Engine final : public EngineBase {
     uint64_t steps = 0;
     Flags f{};
     RC(read_flags(f));
+    RC(update_tiles());
     while (true) {
       if (f.stale) ++stale_events_;
       if (f.rebuild || f.stale || (double)f.d2max > 0.0625 * min_skin_ * min_skin_) {
@@ -976,6 +1100,7 @@ class Engine final : public EngineBase {
       steps += chunk;
       CK(cudaGetLastError());
       RC(read_flags(f));
+      RC(update_tiles());
     }
     total_steps_ += steps;
     if (done_steps) *done_steps = steps;
@@ -1503,6 +1628,11 @@ class Engine final : public EngineBase {
 
   DBuf<V4> pos_, vel_, omg_, frc_, mom_, wallO_, pos_ref_;
   DBuf<long long> frcq_, momq_;   // deterministic mode: fixed-point accumulators
+  std::vector<uint32_t> sb_begin_, sb_end_;   // per sample: bond range
+  DBuf<uint32_t> tiles_, ntiles_, sdone_;     // active bond tiles; per-sample finished flags
+  bool tiles_on_ = false;
+  uint32_t ndone_seen_ = 0;
+  bool user_grid_ = false;
   bool det_ = false;
   DBuf<Real> mass_;
   DBuf<uint32_t> sid_, orig_;

@@ -51,6 +51,7 @@ class EngineBase {
   // nsteps steps launched one by one with events around each kernel: average
   // per-launch durations and the mean number of touching contacts per step
   virtual int profile(uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching) = 0;
+  virtual int autotune(uint32_t steps, dem_tune_report* rep) = 0;
 };
 
 EngineBase* make_engine(const dem_options& o, int* err);

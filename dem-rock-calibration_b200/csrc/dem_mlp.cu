@@ -76,17 +76,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 // GELU in the tanh form of Hendrycks & Gimpel (2016),
 //   gelu(z) = z/2 (1 + tanh(u)) = z s,  s = 1 / (1 + exp(-2u)),
 //   u = sqrt(2/pi) (z + 0.044715 z^3),
-// evaluated as z s with the hardware exponential (__expf), which keeps its
-// relative accuracy in both tails (the form 1 + tanh(u) cancels for large
-// negative z); its derivative
+// evaluated as z s with the hardware exponential (__expf) and reciprocal
+// (rcp.approx), which keep their relative accuracy in both tails (the form
+// 1 + tanh(u) cancels for large negative z); its derivative
 //   gelu'(z) = s + 2 z s (1 - s) sqrt(2/pi) (1 + 3 0.044715 z^2).
 // ReLU takes 0 as its derivative at 0, as sklearn's MLPRegressor does
 // (NN_MP.py:374 uses its default activation).
 constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2/pi)
 constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float rcp_hw(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu_s(float z) {
   const float u = kGeluC * __fmaf_rn(kGeluA * z * z, z, z);
-  return __frcp_rn(1.f + __expf(-2.f * u));
+  return rcp_hw(1.f + __expf(-2.f * u));
 }
 __device__ __forceinline__ float gelu(float z) { return z * gelu_s(z); }
 __device__ __forceinline__ float gelu_grad(float z) {

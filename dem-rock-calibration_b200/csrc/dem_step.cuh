@@ -61,27 +61,35 @@ struct StepArgs {
   long long* frcq;
   long long* momq;
   int det;
+  // batched runs: when set, the pair kernel visits only the listed bond tiles
+  // (tiles holding a bond of an unfinished sample); ntiles on the device
+  const uint32_t* tiles;
+  const uint32_t* ntiles;
 };
 
 // Scatter of one contribution to a particle's force or moment accumulator:
 // a 128-bit float reduction, or in deterministic mode three fixed-point adds.
 template <class Real>
-__device__ __forceinline__ void acc_f(const StepArgs<Real>& A, uint32_t p, Real x, Real y, Real z) {
-  if constexpr (sizeof(Real) == 4) {
-    if (A.det) {
+__device__ __forceinline__ void acc_f(const StepArgs<Real>& A, uint32_t p, const Real& x, const Real& y,
+                                      const Real& z) {
+  if (A.det) {
+    if constexpr (sizeof(Real) == 4)
       acc3q(A.frcq + 4 * (size_t)p, x, y, z);
-      return;
-    }
+    else
+      acc3_fix(A.frc + p, x, y, z);
+    return;
   }
   acc3(A.frc + p, x, y, z);
 }
 template <class Real>
-__device__ __forceinline__ void acc_m(const StepArgs<Real>& A, uint32_t p, Real x, Real y, Real z) {
-  if constexpr (sizeof(Real) == 4) {
-    if (A.det) {
+__device__ __forceinline__ void acc_m(const StepArgs<Real>& A, uint32_t p, const Real& x, const Real& y,
+                                      const Real& z) {
+  if (A.det) {
+    if constexpr (sizeof(Real) == 4)
       acc3q(A.momq + 4 * (size_t)p, x, y, z);
-      return;
-    }
+    else
+      acc3_fix(A.mom + p, x, y, z);
+    return;
   }
   acc3(A.mom + p, x, y, z);
 }
@@ -412,9 +420,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) 
   using V4 = typename RT<Real>::V4;
   const uint32_t nb = A.nb;
   const uint32_t tile = blockDim.x, stride = gridDim.x * tile;
-  for (uint32_t base = blockIdx.x * tile; base < nb; base += stride) {
-    if (threadIdx.x == 0 && base + stride < nb) {
-      const size_t nx = base + stride;
+  const uint32_t ntl = A.tiles ? *A.ntiles : (nb + tile - 1) / tile;
+  for (uint32_t k = blockIdx.x; k < ntl; k += gridDim.x) {
+    const uint32_t base = (A.tiles ? A.tiles[k] : k) * tile;
+    if (threadIdx.x == 0 && k + gridDim.x < ntl) {
+      const size_t nx = A.tiles ? (size_t)A.tiles[k + gridDim.x] * tile : (size_t)base + stride;
       l2_prefetch(A.b_ij + nx, tile * sizeof(uint2));
       l2_prefetch(A.b_par + nx, tile * sizeof(V4));
       l2_prefetch(A.b_s0 + nx, tile * sizeof(V4));
@@ -596,6 +606,9 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
           f = A.frc[p];
           m = A.mom[p];
         }
+      } else if (A.det) {
+        f = unfix4(A.frc[p]);    // FP64 / sensitivity build: fixed point in place
+        m = unfix4(A.mom[p]);
       } else {
         f = A.frc[p];
         m = A.mom[p];
@@ -665,13 +678,15 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       if (A.keep_forces) {
         A.frc[p] = mk4(F[0], F[1], F[2], z);
         A.mom[p] = mk4(M[0], M[1], M[2], z);
-      } else if (!A.det) {
-        A.frc[p] = mk4(z, z, z, z);
+      } else if (!A.det || sizeof(Real) != 4) {
+        A.frc[p] = mk4(z, z, z, z);   // (a zero double is also a zero fixed-point value)
         A.mom[p] = mk4(z, z, z, z);
       }
-      if (A.det) {
-        *reinterpret_cast<longlong4*>(A.frcq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
-        *reinterpret_cast<longlong4*>(A.momq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
+      if constexpr (sizeof(Real) == 4) {
+        if (A.det) {
+          *reinterpret_cast<longlong4*>(A.frcq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
+          *reinterpret_cast<longlong4*>(A.momq + 4 * (size_t)p) = make_longlong4(0, 0, 0, 0);
+        }
       }
       // neighbour-list validity: displacement since the last build.  A parked
       // particle interacts with nothing (all parked particles coincide, and

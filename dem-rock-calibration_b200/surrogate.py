@@ -144,8 +144,9 @@ class MLP:
             "dem_mlp_gemm_tn")
 
     # ---- passes --------------------------------------------------------
-    def _forward(self, bufs, x, idx=None):
-        """x: FP32 (rows, n_in) device tensor, rows selected by idx when given."""
+    def _forward(self, bufs, x, idx=None, keep_z: bool = True):
+        """x: FP32 (rows, n_in) device tensor, rows selected by idx when given;
+        keep_z stores the hidden pre-activations (needed by a backward pass)."""
         P, B = self._ptr, bufs["B"]
         _ck(self.L.dem_mlp_pack_bf16(P(x), None if idx is None else P(idx), B, self.n_in, self.kp[0],
                                      P(bufs["h"][0]), self._s()), "dem_mlp_pack_bf16")
@@ -153,7 +154,7 @@ class MLP:
         for l in range(len(self.W)):
             if l < last:
                 self._gemm(bufs["h"][l], self.Wh[l], B, self.np_[l], self.kp[l], self.b[l], self.mode,
-                           bufs["z"][l], bufs["h"][l + 1])
+                           bufs["z"][l] if keep_z else None, bufs["h"][l + 1])
             else:
                 self._gemm(bufs["h"][l], self.Wh[l], B, self.n_out, self.kp[l], self.b[l], BIAS, bufs["y"], None)
         return bufs["y"]
@@ -243,7 +244,7 @@ class MLP:
         for a in range(0, X.shape[0], chunk):
             xd = torch.from_numpy(X[a:a + chunk]).to(self.dev)
             bufs = self._buffers(xd.shape[0])
-            self._forward(bufs, xd)
+            self._forward(bufs, xd, keep_z=False)
             out[a:a + chunk] = bufs["y"].cpu().numpy()
         self.check()
         return out
@@ -251,7 +252,7 @@ class MLP:
     def predict_device(self, xd):
         """Forward pass of a device FP32 (rows, n_in) tensor; returns the device output buffer."""
         bufs = self._buffers(int(xd.shape[0]))
-        return self._forward(bufs, xd)
+        return self._forward(bufs, xd, keep_z=False)
 
     def gradients(self, X: np.ndarray, T: np.ndarray, input_grad: bool = False):
         """(loss, dW, db, dX) of mean((y - t)^2) at the current weights (no update)."""

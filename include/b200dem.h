@@ -230,6 +230,22 @@ int dem_run_timed(dem_ctx* ctx, uint64_t nsteps, double* ms);
  * events around each: average per-launch times of the pair kernel and the
  * particle kernel, and the mean number of touching contacts per step. */
 int dem_profile(dem_ctx* ctx, uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching);
+/* Launch-schedule autotuner (no counterpart in the reference): after
+ * dem_setup, advances the run by `steps` steps per candidate schedule (real
+ * steps: the state moves on as under dem_run), times each with CUDA events
+ * and keeps the fastest for the rest of the context's life.  Candidates: the
+ * pair kernel's register budget / block size (dem_options.pair_min_blocks)
+ * crossed with particle-kernel blocks of 128 and 256 threads. */
+#define DEM_TUNE_MAX 16
+typedef struct {
+  int candidates;
+  uint32_t pair_min_blocks[DEM_TUNE_MAX];
+  uint32_t particle_block[DEM_TUNE_MAX];
+  double ms_per_step[DEM_TUNE_MAX];
+  uint32_t chosen_pair_min_blocks, chosen_particle_block;
+  double chosen_ms_per_step;
+} dem_tune_report;
+int dem_autotune(dem_ctx* ctx, uint32_t steps, dem_tune_report* report);
 
 /* --- reference-layout parity exports (stateless, run on the current device) --- */
 /* CellDistribution: CI[n], CIs[2n] (sorted keys then particle indices), pnC[2*nx*ny*nz]. */

@@ -1,5 +1,6 @@
-"""Deterministic mode (dem_options.deterministic): FP32 force, moment and
-platen sums in exact 64-bit fixed point.
+"""Deterministic mode (dem_options.deterministic): force, moment and platen
+sums in exact 64-bit fixed point (FP32: separate accumulators with 2^-40
+resolution; FP64 and the sensitivity build: 2^-50, in place).
 
   * the same context run twice gives bit-identical results and records;
   * a case run inside a batch of four equals the same case run alone, bit for
@@ -8,7 +9,10 @@ platen sums in exact 64-bit fixed point.
   * one step's forces match the oracle and the reference kernels as in the
     float-atomic mode (test_gpu_parity.py runs its step cases in both modes);
   * whole loading tests agree with the float-atomic mode within the latter's
-    own run-to-run scatter (UCS 10%, E and nu 3%).
+    own run-to-run scatter (UCS 10%, E and nu 3%);
+  * FP64 runs and sensitivity runs (values and derivatives) repeat exactly;
+  * a run that starts with the launch-schedule autotuner equals one that does
+    not.
 """
 from __future__ import annotations
 
@@ -70,3 +74,54 @@ def test_deterministic_mode_agrees_with_float_atomics():
         assert rd["FractureStress"] == pytest.approx(rf["FractureStress"], rel=0.10)
         assert rd["E_chord"] == pytest.approx(rf["E_chord"], rel=0.03)
         assert rd["nu"] == pytest.approx(rf["nu"], rel=0.03, abs=2e-3)
+
+
+def test_fp64_and_sensitivity_runs_repeat_exactly():
+    J = S.UniaxialJudge(n=2000, seed=5)
+    r_min, r_mean = float(J.rad.min()), float(J.rad.mean())
+    P = _params(2)
+    for precision in (1, 2):
+        outs = []
+        for _ in range(2):
+            ctx = dem.Context(precision=precision, deterministic=True)
+            for row in P:
+                ld = dem.loading(dem.TEST_UNIAXIAL, J.box, J.size_real, J.center_real, velocity=-0.1 / dem.VELOCITY,
+                                 min_stress=0.010, max_strain=0.01, cond_fracture=0.7, dNsave=100, max_steps=3000,
+                                 p_r_platen=r_mean)
+                ctx.add_sample(sweep.material_for(dict(zip(J.keys, row)), r_min, r_mean, 7), ld, J.xyz, J.rad)
+            ctx.setup()
+            ctx.run(3000)
+            outs.append([(ctx.result(i), ctx.sensitivities(i)) for i in range(len(P))])
+            ctx.close()
+        for (ra, sa), (rb, sb) in zip(*outs):
+            assert all(ra[k] == rb[k] for k in KEYS)
+            assert sa["E_secant"] == sb["E_secant"] and sa["nu_secant"] == sb["nu_secant"]
+            assert np.array_equal(sa["dE"], sb["dE"]) and np.array_equal(sa["dnu"], sb["dnu"])
+
+
+def test_autotuned_run_equals_plain_run():
+    """The autotuner's steps are ordinary steps of the run: in deterministic
+    mode a run that starts with an autotune gives bit-identical results to
+    one that does not, and the tuner reports its timed candidates."""
+    J = S.UniaxialJudge(n=2000, seed=5)
+    r_min, r_mean = float(J.rad.min()), float(J.rad.mean())
+    P = _params(3)
+    res = []
+    for tune in (False, True):
+        ctx = dem.Context(deterministic=True)
+        for row in P:
+            ld = dem.loading(dem.TEST_UNIAXIAL, J.box, J.size_real, J.center_real, velocity=-0.1 / dem.VELOCITY,
+                             min_stress=0.010, max_strain=0.01, cond_fracture=0.7, dNsave=100, max_steps=400000,
+                             p_r_platen=r_mean)
+            ctx.add_sample(sweep.material_for(dict(zip(J.keys, row)), r_min, r_mean, 7), ld, J.xyz, J.rad)
+        ctx.setup()
+        if tune:
+            t = ctx.autotune(40)
+            assert len(t["candidates"]) >= 4 and t["ms_per_step"] > 0
+            assert (t["pair_min_blocks"], t["particle_block"]) in [(c[0], c[1]) for c in t["candidates"]]
+        ctx.run(400000)
+        res.append([ctx.result(i) for i in range(len(P))])
+        ctx.close()
+    for ra, rb in zip(*res):
+        assert all(ra[k] == rb[k] for k in KEYS)
+

@@ -420,16 +420,16 @@ def run_surrogate(args, ws, rank, local):
     value = D.sum(float(rows)) * epochs / (ms_max * 1e-3)
     flops = surrogate_flops(sizes, rows) * epochs
     ep.close()
-    # inference GEMM of a 65,536-candidate proposal batch (hidden layer 256 x 256), alone
+    # inference GEMM of a 65,536-candidate proposal batch (hidden layer 256 x 256:
+    # bias + GELU, BF16 out, no pre-activation kept), alone
     M, N, K = 65536, 256, 256
     A = torch.randn(M, K, device=net.dev).to(torch.bfloat16)
     Bm = torch.randn(N, K, device=net.dev).to(torch.bfloat16)
     bias = torch.zeros(N, device=net.dev)
-    zf = torch.empty(M, N, device=net.dev)
     zh = torch.empty(M, N, dtype=torch.bfloat16, device=net.dev)
     P = lambda t: C.c_void_p(t.data_ptr())
     st = torch.cuda.current_stream(net.dev)
-    call = lambda: net.L.dem_mlp_gemm_tn(P(A), P(Bm), M, N, K, P(bias), S.BIAS_GELU, P(zf), P(zh),
+    call = lambda: net.L.dem_mlp_gemm_tn(P(A), P(Bm), M, N, K, P(bias), S.BIAS_GELU, None, P(zh),
                                          C.c_void_p(st.cuda_stream))
     for _ in range(5):
         call()
@@ -443,6 +443,12 @@ def run_surrogate(args, ws, rank, local):
     gemm_ms = g0.elapsed_time(g1) / reps
     net.check()
     gemm_tf = 2.0 * M * N * K / (gemm_ms * 1e-3) / 1e12
+    # algorithmic bytes: A and B read once, BF16 output written once; at width
+    # 256 the arithmetic intensity (about 130 flop/byte) is below the B200
+    # ridge (measured bf16 peak / measured HBM bandwidth, about 250), so HBM
+    # bounds this layer
+    gemm_bytes = 2.0 * M * K + 2.0 * N * K + 2.0 * M * N
+    hbm_peak, _ = peaks()
     # end to end through the public API: host arrays in, a fitted network and host predictions out
     t0 = time.perf_counter()
     net2 = S.MLP(sizes, seed=rank + 100, device=local)
@@ -462,10 +468,16 @@ def run_surrogate(args, ws, rank, local):
                    "l2": "dataset and weights inside the L2 (the whole job is 10 MB)"},
         "gpu_launches": epochs * len(ep.sizes) * net.launches_per_step(),
         "clocks": clocks,
-        "roofline": {"bound": "tensor", "achieved": gemm_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": gemm_tf / peak_tf, "traffic": None,
-                     "kernel": f"k_gemm_tn<256> forward layer {M} x {N} x {K} (bias + GELU epilogue)",
-                     "gemm_us": gemm_ms * 1e3, "peak_kind": peak_kind},
+        "roofline": (lambda ai, ridge, gbs: {
+            "bound": "hbm" if ai < ridge else "tensor",
+            "achieved": gbs if ai < ridge else gemm_tf, "peak": hbm_peak if ai < ridge else peak_tf,
+            "unit": "GB/s" if ai < ridge else "TFLOP/s",
+            "frac": gbs / hbm_peak if ai < ridge else gemm_tf / peak_tf, "traffic": None,
+            "kernel": f"k_gemm_tn<256> forward layer {M} x {N} x {K} (bias + GELU epilogue, BF16 out)",
+            "gemm_us": gemm_ms * 1e3, "tflops": gemm_tf, "tensor_frac": gemm_tf / peak_tf,
+            "arithmetic_intensity": ai, "ridge": ridge, "algorithmic_bytes": gemm_bytes,
+            "peak_kind": peak_kind})(2.0 * M * N * K / gemm_bytes, peak_tf * 1e12 / (hbm_peak * 1e9),
+                                     gemm_bytes / (gemm_ms * 1e-3) / 1e9),
         "e2e": {"value": rows * epochs / t_e2e, "unit": "samples/s",
                 "h2d_bytes_per_step": (X.nbytes + Y.nbytes) / epochs, "d2h_bytes_per_step": 4.0 * 2,
                 "seconds": t_e2e, "note": "MLP.fit from host arrays (upload, eager first epoch, graph capture, "
@@ -549,6 +561,8 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="contact-list skin as a multiple of the smallest radius (0: the engine default, 0.1)")
     ap.add_argument("--deterministic", action="store_true",
                     help="exact fixed-point force sums (bit-reproducible runs) instead of float atomics")
     ap.add_argument("--specimens", type=int, default=2,
@@ -569,7 +583,7 @@ def main() -> int:
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
     spec = specs[0]
     ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
-                      deterministic=args.deterministic)
+                      deterministic=args.deterministic, skin_factor=args.skin)
     sids = [ctx.add_sample(sp.material, sp.loading, sp.xyz, sp.radii) for sp in specs]
     ctx.setup()
     cnt = ctx.counts()

@@ -141,7 +141,7 @@ class Engine final : public EngineBase {
     RC(set_pair_config(opt_.pair_min_blocks));
     if (!opt_.particle_block) opt_.particle_block = 256;
     if (!opt_.graph_steps) opt_.graph_steps = 100;
-    if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.25;
+    if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.1;
     return DEM_OK;
   }
 

@@ -3,24 +3,26 @@
 // FP32 accumulation on the 5th-generation tensor cores.
 //
 //   k_gemm_tn   C[M x N] = A[M x K] . B[N x K]^T, A and B row-major BF16 (both
-//               "K-major"), accumulator in tensor memory.  A 128-row tile of A
-//               and an N-tile (32..256, narrowed for small grids) of B stream
-//               through a 2-4 stage cp.async pipeline (64 of K per stage) into
-//               shared memory in the canonical no-swizzle core-matrix layout
-//               (8 rows x 16 bytes per core matrix); one thread issues
-//               tcgen05.mma (M = 128, K = 16 per instruction, kind::f16) and
-//               commits each stage to its mbarrier, which frees the stage for
-//               the next load.  The eight warps then read the accumulator with
-//               tcgen05.ld (warps w and w + 4 share lanes 32 (w % 4) and split
-//               the columns), stage 32 x 32 chunks in shared memory and store
-//               whole rows: + bias and GELU or ReLU to BF16 (hidden layers,
-//               pre-activation kept in FP32), + bias to FP32 (output layer), or
-//               plain FP32 (weight and activation gradients).
+//               "K-major"), accumulator in tensor memory.  Warp-specialised:
+//               one thread streams 128-row tiles of A and TN-row tiles of B
+//               (TN 32..256, narrowed for small grids), 64 of K per stage, with
+//               the TMA into a 2-4 stage ring in the 128-byte swizzled layout;
+//               one thread issues tcgen05.mma (M = 128, K = 16 per
+//               instruction, kind::f16) as each stage lands and commits it
+//               back to the producer; the eight warps then read the
+//               accumulator with tcgen05.ld (warps w and w + 4 share lanes
+//               32 (w % 4) and split the columns) and apply the epilogue in
+//               registers: + bias and GELU or ReLU to BF16 (hidden layers,
+//               pre-activation kept in FP32 when asked), + bias to FP32
+//               (output layer), or plain FP32 (weight and activation
+//               gradients), written with 16-byte stores.
 //   small kernels: input packing, transposes, activation backward, column
 //               sums, MSE gradient, Adam.
 //
 // All waits are bounded: a commit that does not arrive within the poll limit
 // sets *err, the block waits once more (bounded) and frees its tensor memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -65,12 +67,31 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 // Shared-memory matrix descriptor (sm_100): start address, leading-dimension
 // byte offset (between the two core matrices along K of one instruction),
 // stride byte offset (between 8-row groups), descriptor version 1, no swizzle.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzled layout the TMA writes: rows of 64 BF16 (128 bytes), 8-row atoms of
+// 1024 bytes one after another (stride byte offset 1024; the leading byte
+// offset is unused for swizzled K-major operands and set to 16), descriptor
+// version 1, layout type 2 (SWIZZLE_128B).  The K = 16 slices of a row start
+// 32 bytes apart inside the atom.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
   d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
   return d;
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+// TMA load of one box (x = K element, y = row) of a 2-D tensor map into shared
+// memory, completing on the mbarrier; no multicast
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(saddr(bar))
+      : "memory");
 }
 
 // GELU in the tanh form of Hendrycks & Gimpel (2016),
@@ -100,106 +121,94 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return __fmaf_rn(2.f * z * s * (1.f - s), du, s);
 }
 
-// Pipeline geometry of a TN-column tile: a stage holds 64 of K (32 for the
-// 256-column tile) as 16-byte groups of 8 BF16 per row, for the 128 rows of A
-// and the TN rows of B; as many stages as fit in about 100 KB (2..4), so that
-// two blocks share an SM and one block's epilogue overlaps the other's main
-// loop.
+// Pipeline geometry of a TN-column tile: a stage holds 64 of K (one 128-byte
+// swizzled row) for the 128 rows of A and the TN rows of B; as many stages as
+// fit in about 100 KB (2..4), so that two blocks share an SM and one block's
+// epilogue overlaps the other's main loop.
+constexpr int kSK = 64;
 template <int TN>
 struct GemmCfg {
-  static constexpr int kSK = TN >= 256 ? 32 : 64;   // K per stage (narrower stages for the widest tile)
-  static constexpr int kGroups = kSK / 8;           // 16-byte K groups per row and stage
-  static constexpr int kStageBytes = (kTM + TN) * kGroups * 16;
+  static constexpr int kABytes = kTM * 128;
+  static constexpr int kStageBytes = (kTM + TN) * 128;
   static constexpr int kStages = (100 * 1024 / kStageBytes) < 2 ? 2 : ((100 * 1024 / kStageBytes) > 4 ? 4 : (100 * 1024 / kStageBytes));
-  static constexpr int kBars = 8 * kStages;                      // one mbarrier (8 bytes) per stage
-  static constexpr int kSmem = kStages * kStageBytes + kBars + 16 + 128;   // + tmem slot + alignment slack
+  static constexpr int kSmem = kStages * kStageBytes + 1024 /* alignment */ + 8 * (2 * kStages + 1) + 16;
   static constexpr uint32_t kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256));
 };
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// Stage s of round c: rows of A (kTM) then rows of B (TN), each as kGroups
-// core-matrix columns: group g of row r at byte (g * rows + r) * 16, so the
-// 8-row core matrices are 128 bytes apart (SBO) and the K groups rows * 16
-// bytes apart (LBO).  Rows beyond M / N and K beyond the end are zero-filled
-// (source size 0, address clamped to the operand's base).
+// Warp-specialised: warp 0 lane 0 streams the stages with the TMA (A box
+// 64 x 128 rows, B box 64 x TN rows, 128-byte swizzle, zero fill past the
+// edges), warp 1 allocates the accumulator and its lane 0 issues the MMAs of
+// each stage once its bytes have landed and commits the stage back to the
+// producer; all eight warps then drain the accumulator.
 template <int TN>
-__device__ __forceinline__ void load_stage(uint32_t st, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N,
-                                           int K, int m0, int n0, int k0, int tid) {
-  using Cfg = GemmCfg<TN>;
-  for (int q = tid; q < Cfg::kGroups * (kTM + TN); q += kThreads) {
-    const int g = q % Cfg::kGroups, r = q / Cfg::kGroups;
-    const int k = k0 + 8 * g;
-    const __nv_bfloat16* src;
-    uint32_t dst, bytes;
-    if (r < kTM) {
-      const bool in = (m0 + r < M) && (k < K);
-      src = in ? A + (size_t)(m0 + r) * K + k : A;
-      bytes = in ? 16u : 0u;
-      dst = st + (uint32_t)(g * kTM + r) * 16u;
-    } else {
-      const int rb = r - kTM;
-      const bool in = (n0 + rb < N) && (k < K);
-      src = in ? B + (size_t)(n0 + rb) * K + k : B;
-      bytes = in ? 16u : 0u;
-      dst = st + (uint32_t)(kTM * Cfg::kGroups * 16) + (uint32_t)(g * TN + rb) * 16u;
-    }
-    cp_async16(dst, src, bytes);
-  }
-}
-
-template <int TN>
-__global__ void __launch_bounds__(kThreads) k_gemm_tn(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B,
-                                                 int M, int N, int K, const float* __restrict__ bias, int mode,
-                                                 float* __restrict__ outf, __nv_bfloat16* __restrict__ outh,
-                                                 unsigned int* err) {
+__global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ CUtensorMap tmA,
+                                                 const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
+                                                 const float* __restrict__ bias, int mode, float* __restrict__ outf,
+                                                 __nv_bfloat16* __restrict__ outh, unsigned int* err) {
   using Cfg = GemmCfg<TN>;
   constexpr int S = Cfg::kStages;
   extern __shared__ uint8_t smem_raw[];
-  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * Cfg::kStageBytes);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + S * Cfg::kStageBytes + Cfg::kBars);
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + S * Cfg::kStageBytes);
+  uint64_t* empty = full + S;
+  uint64_t* accum = empty + S;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(accum + 1);
   const uint32_t sbase = saddr(base);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * TN;
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
                  "r"(Cfg::kCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0)
-    for (int s = 0; s < S; ++s) bar_init(&bars[s]);
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      bar_init(&full[s]);
+      bar_init(&empty[s]);
+    }
+    bar_init(accum);
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  // instruction descriptor: F32 accumulate, BF16 A and B, both K-major, N, M = 128
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
-  const int rounds = (K + Cfg::kSK - 1) / Cfg::kSK;
-  // prologue: stages 0 .. S-2 in flight
-  for (int s = 0; s < S - 1; ++s) {
-    if (s < rounds) load_stage<TN>(sbase + s * Cfg::kStageBytes, A, B, M, N, K, m0, n0, s * Cfg::kSK, tid);
-    cp_async_commit();
-  }
+  const int rounds = (K + kSK - 1) / kSK;
   bool ok = true;
-  int issued = 0;                                             // rounds whose MMAs have been committed
-  for (int c = 0; c < rounds; ++c) {
-    const int s = c % S;
-    cp_async_wait<S - 2>();                                   // this thread's copies of round c have landed
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core's proxy
-    __syncthreads();
-    if (tid == 0) {
+  if (warp == 0 && lane == 0) {
+    // producer
+    int issued = 0;
+    for (int c = 0; c < rounds; ++c) {
+      const int s = c % S;
+      if (c >= S && !bar_wait(&empty[s], (uint32_t)((c / S - 1) & 1))) {
+        ok = false;
+        break;
+      }
+      const uint32_t st = sbase + s * Cfg::kStageBytes;
+      bar_expect_tx(&full[s], (uint32_t)Cfg::kStageBytes);
+      tma_load_2d(st, &tmA, c * kSK, m0, &full[s]);
+      tma_load_2d(st + Cfg::kABytes, &tmB, c * kSK, n0, &full[s]);
+      issued = c + 1;
+    }
+    // no load may still be writing shared memory when the block ends
+    for (int c = (issued > S ? issued - S : 0); c < issued; ++c)
+      if (!bar_wait(&full[c % S], (uint32_t)((c / S) & 1))) ok = false;
+    if (!ok) atomicOr(err, 1u);
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    int committed = 0;
+    for (int c = 0; c < rounds; ++c) {
+      const int s = c % S;
+      if (!bar_wait(&full[s], (uint32_t)((c / S) & 1))) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
       const uint32_t st = sbase + s * Cfg::kStageBytes;
-      for (int kk = 0; kk < Cfg::kSK / 16; ++kk) {
-        const uint64_t da = smem_desc(st + (uint32_t)(2 * kk * kTM * 16), kTM * 16, 128);
-        const uint64_t db = smem_desc(st + (uint32_t)(kTM * Cfg::kGroups * 16 + 2 * kk * TN * 16), TN * 16, 128);
+      for (int kk = 0; kk < kSK / 16; ++kk) {
+        const uint64_t da = smem_desc_sw128(st + (uint32_t)(kk * 32));
+        const uint64_t db = smem_desc_sw128(st + (uint32_t)(Cfg::kABytes + kk * 32));
         const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -209,33 +218,22 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __nv_bfloat16* __res
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       saddr(&bars[s]))
+                       saddr(&empty[s]))
                    : "memory");
+      committed = c + 1;
     }
-    issued = c + 1;
-    // refill the stage that round c - 1 read, once its MMAs have completed
-    const int cn = c + S - 1;
-    if (c >= 1) {
-      const int sp = (c - 1) % S;
-      ok = bar_wait(&bars[sp], (uint32_t)(((c - 1) / S) & 1));
-      if (__syncthreads_or(!ok)) break;
-    }
-    if (cn < rounds) load_stage<TN>(sbase + (cn % S) * Cfg::kStageBytes, A, B, M, N, K, m0, n0, cn * Cfg::kSK, tid);
-    cp_async_commit();
+    if (ok)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       saddr(accum))
+                   : "memory");
+    else if (committed > 0)
+      bar_wait(&empty[(committed - 1) % S], (uint32_t)(((committed - 1) / S) & 1));
+    if (!ok) atomicOr(err, 1u);
   }
-  if (ok && rounds > 0) {
-    const int cl = rounds - 1;
-    ok = bar_wait(&bars[cl % S], (uint32_t)((cl / S) & 1));
-    ok = !__syncthreads_or(!ok);
-  }
-  cp_async_wait<0>();
-  if (!ok) {
-    if (tid == 0) atomicOr(err, 1u);
-    // one more bounded wait for the last commit, so that no MMA is left reading
-    // shared memory or writing the accumulator when the block frees them
-    if (issued > 0) bar_wait(&bars[(issued - 1) % S], (uint32_t)(((issued - 1) / S) & 1));
-  }
-  __syncthreads();
+  // everyone: the accumulator is complete when the last commit arrives
+  if (rounds > 0) ok = ok && bar_wait(accum, 0u);
+  ok = !__syncthreads_or(!ok);
+  if (!ok && tid == 0) atomicOr(err, 1u);
   if (ok && rounds > 0) {
     tc_fence_after();
     // epilogue: warp w reads accumulator lanes 32 (w % 4) .. +31 (the lanes its
@@ -306,7 +304,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __nv_bfloat16* __res
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols) : "memory");
 }
 
@@ -444,6 +442,35 @@ int err_flag(unsigned int** out) {
 
 uint32_t blocks(size_t n) { return (uint32_t)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+// Tensor maps of the two operands: row-major BF16 [rows x K], box 64 x rows
+// of the tile, 128-byte swizzle, zero fill outside.  cuTensorMapEncodeTiled
+// comes from the driver through the runtime (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+int make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return DEM_ERR_CUDA;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kSK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? DEM_OK : DEM_ERR_CUDA;
+}
+
 // the pipeline needs more than the default 48 KB of dynamic shared memory: the
 // limit is raised once per device and tile width (before any graph capture,
 // since the first call of every shape comes from eager code)
@@ -460,7 +487,9 @@ int launch_gemm(unsigned gx, unsigned gy, cudaStream_t st, const __nv_bfloat16* 
       return DEM_ERR_CUDA;
     raised[dev] = true;
   }
-  k_gemm_tn<TN><<<dim3(gx, gy), kThreads, GemmCfg<TN>::kSmem, st>>>(a, b, M, N, K, bias, mode, outf, oh, err);
+  CUtensorMap ma, mb;
+  if (make_map(&ma, a, M, K, kTM) || make_map(&mb, b, N, K, TN)) return DEM_ERR_CUDA;
+  k_gemm_tn<TN><<<dim3(gx, gy), kThreads, GemmCfg<TN>::kSmem, st>>>(ma, mb, M, N, K, bias, mode, outf, oh, err);
   return DEM_OK;
 }
 

@@ -96,6 +96,9 @@ class Packer {
     CKP(pos.alloc(n));
     CKP(vel.alloc(n));
     CKP(frc.alloc(n));
+    CKP(frcq.alloc(4 * (size_t)n));
+    CKP(cudaMemset(frcq.p, 0, 4 * (size_t)n * sizeof(long long)));
+    CKP(part.alloc(3 * (size_t)nsm * 8));
     CKP(ref.alloc(n));
     CKP(sid.alloc(n));
     CKP(cudaMemcpy(pos.p, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
@@ -267,6 +270,7 @@ class Packer {
     CKP(cudaMemcpy(pos.p, hp.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
     CKP(cudaMemcpy(vel.p, hv.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
     CKP(cudaMemset(frc.p, 0, n * sizeof(float4)));
+    CKP(cudaMemset(frcq.p, 0, 4 * (size_t)n * sizeof(long long)));
     return DEM_OK;
   }
 
@@ -330,6 +334,8 @@ class Packer {
     A.pos = pos.p;
     A.vel = vel.p;
     A.frc = frc.p;
+    A.frcq = frcq.p;
+    A.part = part.p;
     A.ref = ref.p;
     A.sid = sid.p;
     A.np = n;
@@ -402,6 +408,8 @@ class Packer {
   float last_overlap = 0.f;
   uint32_t rebuilds = 0;
   Buf<float4> pos, vel, frc, ref;
+  Buf<long long> frcq;
+  Buf<double> part;
   Buf<uint32_t> sid, cell_of, cell_count, cell_start, cursor, cell_list, cnt, offs, brow, ovf, nc_dev, js, scan_tmp;
   Buf<uint2> cij;
   Buf<Grid<float>> grid;

@@ -58,6 +58,11 @@ struct PackArgs {
   unsigned int* blocks_done;
   int viscous;         // 1: viscous step of the pre-relaxation instead of FIRE
   Real vis;            // viscous coefficient (reference Po.vism)
+  // Determinism: pair forces in exact fixed point (4 per particle, see acc3q),
+  // and the FIRE power / norms as per-block partial sums (3 per block) that the
+  // last block adds in block order; a seeded packing then repeats exactly.
+  long long* frcq;
+  double* part;
 };
 
 template <class Real>
@@ -84,8 +89,8 @@ __global__ void __launch_bounds__(256) k_soft_pairs(PackArgs<Real> A) {
       const Real r = RT<Real>::sqrt_rn(rr);
       fm = -A.D[s] * (a - r) / r;
     }
-    acc3(A.frc + i, fm * dx, fm * dy, fm * dz);
-    acc3(A.frc + j, -fm * dx, -fm * dy, -fm * dz);
+    acc3q(A.frcq + 4 * (size_t)i, fm * dx, fm * dy, fm * dz);
+    acc3q(A.frcq + 4 * (size_t)j, -fm * dx, -fm * dy, -fm * dz);
     const float ov = (float)((a - RT<Real>::sqrt_rn(rr)) / a);
     worst = fmaxf(worst, ov);
     if (A.povl && ov > 0.f) {
@@ -134,7 +139,10 @@ __global__ void __launch_bounds__(256) k_fire_power(PackArgs<Real> A) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     const uint32_t s = A.sid[p];
     const V4 x = A.pos[p], v = A.vel[p];
-    V4 f = A.frc[p];
+    long long* q = A.frcq + 4 * (size_t)p;
+    V4 f = mk4((Real)((double)q[0] * kFixInv), (Real)((double)q[1] * kFixInv), (Real)((double)q[2] * kFixInv),
+               Real(0));
+    q[0] = q[1] = q[2] = 0;
     // walls: radius R - r_i, caps at +-(H - r_i), force D * penetration
     const Real* c = A.cyl + 5 * s;
     const Real r = A.scale[s] * x.w, D = A.D[s];
@@ -157,10 +165,8 @@ __global__ void __launch_bounds__(256) k_fire_power(PackArgs<Real> A) {
       f.z += D * (-H0 - dz);
       pen = fmax(pen, -H0 - dz);
     }
-    if (pen > Real(0)) {
-      A.frc[p] = f;
-      worst = fmaxf(worst, (float)(pen / (Real(2) * r)));
-    }
+    A.frc[p] = f;
+    if (pen > Real(0)) worst = fmaxf(worst, (float)(pen / (Real(2) * r)));
     pw += (double)((f.x * v.x + f.y * v.y) + f.z * v.z);
     vv += (double)((v.x * v.x + v.y * v.y) + v.z * v.z);
     ff += (double)((f.x * f.x + f.y * f.y) + f.z * f.z);
@@ -172,15 +178,20 @@ __global__ void __launch_bounds__(256) k_fire_power(PackArgs<Real> A) {
   FireCtl& F = A.fire[0];
   if (A.viscous) return;
   if (threadIdx.x == 0) {
-    if (pw != 0.0) atomicAdd(&F.P, pw);
-    if (vv != 0.0) atomicAdd(&F.vv, vv);
-    if (ff != 0.0) atomicAdd(&F.ff, ff);
+    A.part[3 * blockIdx.x + 0] = pw;
+    A.part[3 * blockIdx.x + 1] = vv;
+    A.part[3 * blockIdx.x + 2] = ff;
     __threadfence();
     s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
   }
   __syncthreads();
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
+  for (uint32_t b = 0; b < gridDim.x; ++b) {
+    F.P += __ldcg(A.part + 3 * b);
+    F.vv += __ldcg(A.part + 3 * b + 1);
+    F.ff += __ldcg(A.part + 3 * b + 2);
+  }
   // md_createcylindersample.cu:374-397 (the same adaptation drives FIRE 2.0)
   if (F.P > 0) {
     ++F.Npos;

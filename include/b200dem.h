@@ -64,7 +64,7 @@ typedef struct {
   uint32_t pair_grid;     /* blocks of the pair kernel (0: all co-resident blocks) */
   uint32_t particle_block;/* threads per block of the particle kernel (0: 256) */
   uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
-  double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.25) */
+  double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.1) */
   uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
                                (1..4 of 256 threads, FP32 also 5..8 of 128 threads;
                                0: 7 for FP32, 2 for FP64, 1 for the sensitivity build) */

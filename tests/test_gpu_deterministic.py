@@ -12,7 +12,8 @@ resolution; FP64 and the sensitivity build: 2^-50, in place).
     own run-to-run scatter (UCS 10%, E and nu 3%);
   * FP64 runs and sensitivity runs (values and derivatives) repeat exactly;
   * a run that starts with the launch-schedule autotuner equals one that does
-    not.
+    not;
+  * a seeded packing repeats exactly.
 """
 from __future__ import annotations
 
@@ -124,4 +125,12 @@ def test_autotuned_run_equals_plain_run():
         ctx.close()
     for ra, rb in zip(*res):
         assert all(ra[k] == rb[k] for k in KEYS)
+
+
+def test_seeded_packing_repeats_exactly():
+    """The packer sums pair forces in fixed point and the FIRE power in block
+    order, so a seeded specimen is the same on every run."""
+    a = sweep.cylinder(1500, 21)
+    b = sweep.cylinder(1500, 21)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 

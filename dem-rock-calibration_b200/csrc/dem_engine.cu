@@ -116,7 +116,7 @@ class Engine final : public EngineBase {
 
   explicit Engine(const dem_options& o) : opt_(o) {}
   ~Engine() override {
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    invalidate_graph();
     if (stream_) cudaStreamDestroy(stream_);
   }
 
@@ -985,26 +985,51 @@ class Engine final : public EngineBase {
   void invalidate_graph() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     graph_exec_ = nullptr;
+    for (auto& g : small_graphs_) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   }
 
-  int capture_graph() {
-    invalidate_graph();
+  int capture_steps(uint32_t steps, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     StepArgs<Real> A = args();
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    for (uint32_t k = 0; k < opt_.graph_steps; ++k) launch_step(A, 3);
+    for (uint32_t k = 0; k < steps; ++k) launch_step(A, 3);
     cudaError_t e = cudaStreamEndCapture(stream_, &g);
     if (e != cudaSuccess) {
       last_cuda_ = e;
       return DEM_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&graph_exec_, g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
       last_cuda_ = e;
-      graph_exec_ = nullptr;
+      *out = nullptr;
       return DEM_ERR_CUDA;
     }
+    return DEM_OK;
+  }
+
+  int capture_graph() {
+    invalidate_graph();
+    return capture_steps(opt_.graph_steps, &graph_exec_);
+  }
+
+  // A chunk shorter than graph_steps (fast particles or a thin skin shorten
+  // them) runs as graphs of 64, 16 and 4 steps (captured on first use) and
+  // single steps, instead of two kernel launches per step.
+  int run_short_chunk(uint64_t chunk) {
+    static constexpr uint32_t kSizes[3] = {64, 16, 4};
+    for (int k = 0; k < 3; ++k) {
+      while (chunk >= kSizes[k] && kSizes[k] < opt_.graph_steps) {
+        if (!small_graphs_[k]) RC(capture_steps(kSizes[k], &small_graphs_[k]));
+        CK(cudaGraphLaunch(small_graphs_[k], stream_));
+        chunk -= kSizes[k];
+      }
+    }
+    StepArgs<Real> A = args();
+    for (uint64_t s = 0; s < chunk; ++s) launch_step(A, 3);
     return DEM_OK;
   }
 
@@ -1094,8 +1119,7 @@ class Engine final : public EngineBase {
         if (!graph_exec_) RC(capture_graph());
         CK(cudaGraphLaunch(graph_exec_, stream_));
       } else {
-        StepArgs<Real> A = args();
-        for (uint64_t k = 0; k < chunk; ++k) launch_step(A, 3);
+        RC(run_short_chunk(chunk));
       }
       steps += chunk;
       CK(cudaGetLastError());
@@ -1614,6 +1638,7 @@ class Engine final : public EngineBase {
   dem_options opt_;
   cudaStream_t stream_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
+  cudaGraphExec_t small_graphs_[3] = {nullptr, nullptr, nullptr};   // 64, 16 and 4 steps
   int num_sms_ = 148;
   const void* pair_kernel_ = nullptr;
   bool setup_done_ = false, forces_dirty_ = false, contacts_dirty_ = false, stale_ = false;

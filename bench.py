@@ -589,11 +589,13 @@ def main() -> int:
     cnt = ctx.counts()
     n_gpu = cnt["particles"]
     ctx.run_timed(args.warmup)
+    rb0 = ctx.result(sids[0])["rebuilds"]
     D.barrier()
     clk = Clocks(local)
     ms = ctx.run_timed(args.steps)
     clocks = clk.stop()
     D.barrier()
+    rb1 = ctx.result(sids[0])["rebuilds"]
     ms_max = D.max(ms)
     n_total = D.sum(float(n_gpu))
     value = n_total * args.steps / (ms_max * 1e-3)
@@ -619,15 +621,16 @@ def main() -> int:
     # end to end through the public API with host buffers: positions uploaded,
     # set-up (Morton sort, bonds, contact list), K steps, results and records read back
     t0 = time.perf_counter()
-    e2 = dem.Context(device=local, graph_steps=200)
+    e2 = dem.Context(device=local, graph_steps=200, skin_factor=args.skin, deterministic=args.deterministic)
     for sp in specs:
         ld = dem.Loading.from_buffer_copy(sp.loading)
         ld.max_steps = args.steps
         e2.add_sample(sp.material, ld, sp.xyz, sp.radii)
     e2.setup()
+    t_setup = time.perf_counter() - t0
     e2.run(args.steps)
     recs = [e2.record(k) for k in range(len(specs))]
-    _ = [e2.result(k) for k in range(len(specs))]
+    res2 = [e2.result(k) for k in range(len(specs))]
     e2.close()
     t_e2e = time.perf_counter() - t0
     e2e_val = D.sum(n_gpu * args.steps / t_e2e)
@@ -654,6 +657,7 @@ def main() -> int:
                    "l2": f"inputs larger than L2: state {state_mb:.0f} MB per GPU vs 126 MB L2, no flush",
                    "packing": spec.pack, "stale_lists": stale,
                    "force_sums": "fixed point (deterministic)" if args.deterministic else "float atomics",
+                   "contact_list_builds_timed": rb1 - rb0,
                    "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
                                        "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
                                        "note": "state inside the L2"}},
@@ -667,7 +671,8 @@ def main() -> int:
                      "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
                      "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e,
+                "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e, "setup_seconds": t_setup,
+                "contact_list_builds": res2[0]["rebuilds"],
                 "note": "public API from host positions: upload, set-up, steps, results and records read back"},
         "cpu_baseline": cpu,
         "cpu_baseline_reference_bpm": cpu_bpm,

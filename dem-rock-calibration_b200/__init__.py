@@ -94,7 +94,7 @@ class Result(C.Structure):
                 ("Stress", C.c_double), ("dt", C.c_double), ("platen_top", C.c_double),
                 ("platen_bottom", C.c_double), ("platen_velocity", C.c_double), ("steps", C.c_uint64),
                 ("stepsave", C.c_uint32), ("bonds_initial", C.c_uint32), ("bonds_now", C.c_uint32),
-                ("fracture", C.c_int), ("done", C.c_int), ("stale", C.c_int), ("reserved", C.c_int),
+                ("fracture", C.c_int), ("done", C.c_int), ("stale", C.c_int), ("rebuilds", C.c_int),
                 ("E_chord", C.c_double), ("nu", C.c_double)]
 
     def as_dict(self) -> dict:

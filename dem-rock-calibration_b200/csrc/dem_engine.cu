@@ -654,6 +654,25 @@ class Engine final : public EngineBase {
     ntiles_.release();
     tiles_on_ = false;
     ndone_seen_ = 0;
+    return tile_samples();
+  }
+
+  // Sample of every bond tile of the current pair-kernel block size (~0u for
+  // a tile spanning two samples).
+  int tile_samples() {
+    tile_s_.release();
+    const uint32_t S = (uint32_t)sb_begin_.size();
+    if (nb_ == 0 || S == 0) return DEM_OK;
+    const uint32_t tile = opt_.pair_block, T = (nb_ + tile - 1) / tile;
+    std::vector<uint32_t> h(T, ~0u);
+    uint32_t si = 0;
+    for (uint32_t t = 0; t < T; ++t) {
+      const uint32_t b0 = t * tile, b1 = std::min(nb_, b0 + tile) - 1;
+      while (si < S && sb_end_[si] <= b0) ++si;
+      if (si < S && sb_begin_[si] <= b0 && b1 < sb_end_[si]) h[t] = si;
+    }
+    CK(tile_s_.alloc(T));
+    CK(tile_s_.upload(h.data(), T));
     return DEM_OK;
   }
 
@@ -878,6 +897,7 @@ class Engine final : public EngineBase {
     A.det = det_ ? 1 : 0;
     A.tiles = tiles_on_ ? tiles_.p : nullptr;
     A.ntiles = tiles_on_ ? ntiles_.p : nullptr;
+    A.tile_s = tile_s_.p;
     return A;
   }
 
@@ -899,7 +919,7 @@ class Engine final : public EngineBase {
     invalidate_graph();
     tiles_on_ = false;
     ndone_seen_ = 0;
-    return DEM_OK;
+    return setup_done_ ? tile_samples() : DEM_OK;
   }
 
   // Launch-schedule autotuner: advances the run by `steps` steps per candidate
@@ -1182,6 +1202,7 @@ class Engine final : public EngineBase {
     out->fracture = (int)C.Fracture;
     out->done = (int)C.done;
     out->stale = (int)stale_events_;
+    out->rebuilds = (int)std::min<uint64_t>(rebuilds_, INT32_MAX);
     // host post-processing of the record (CalculateLinearityDeviation, CalculateDestruction)
     std::vector<double> rec;
     std::vector<uint32_t> rb;
@@ -1655,6 +1676,7 @@ class Engine final : public EngineBase {
   DBuf<long long> frcq_, momq_;   // deterministic mode: fixed-point accumulators
   std::vector<uint32_t> sb_begin_, sb_end_;   // per sample: bond range
   DBuf<uint32_t> tiles_, ntiles_, sdone_;     // active bond tiles; per-sample finished flags
+  DBuf<uint32_t> tile_s_;                     // per bond tile: its sample (~0u: two samples)
   bool tiles_on_ = false;
   uint32_t ndone_seen_ = 0;
   bool user_grid_ = false;

@@ -65,6 +65,10 @@ struct StepArgs {
   // (tiles holding a bond of an unfinished sample); ntiles on the device
   const uint32_t* tiles;
   const uint32_t* ntiles;
+  // per bond tile (blockDim.x bonds): the sample all its bonds belong to, or
+  // ~0u when the tile spans two samples; lets a bond find its sample's state
+  // without first loading the sample id of its particle
+  const uint32_t* tile_s;
 };
 
 // Scatter of one contribution to a particle's force or moment accumulator:
@@ -231,7 +235,7 @@ __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i
 template <class Real>
 __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
                                         typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
-                                        typename RT<Real>::V4 s1, typename RT<Real>::V4 s2) {
+                                        typename RT<Real>::V4 s1, typename RT<Real>::V4 s2, uint32_t ts) {
   using T = RT<Real>;
   using V4 = typename T::V4;
   // the gathers depend only on (i, j): all issued before the first branch
@@ -239,7 +243,7 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, con
   const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
   const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
   const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
-  const uint32_t s = A.sid[i];
+  const uint32_t s = ts != ~0u ? ts : A.sid[i];
   if (A.ctl[s].done) return;
   const SampleParams<Real>& sp = A.sp[s];
   const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
@@ -432,9 +436,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) 
       l2_prefetch(A.b_s2 + nx, tile * sizeof(V4));
     }
     const uint32_t b = base + threadIdx.x;
+    const uint32_t ts = A.tile_s ? __ldg(A.tile_s + base / tile) : ~0u;
     if (b < nb)
       do_bond<Real>(A, b, __ldcs(A.b_ij + b), ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b),
-                    ld4_cs(A.b_s2 + b));
+                    ld4_cs(A.b_s2 + b), ts);
   }
   const uint32_t nc = *A.nc;
   for (uint32_t c = blockIdx.x * tile + threadIdx.x; c < nc; c += stride) do_contact<Real>(A, c);

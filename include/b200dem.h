@@ -134,7 +134,7 @@ typedef struct {
   uint32_t stepsave;         /* number of records */
   uint32_t bonds_initial, bonds_now;  /* intact undirected bonds */
   int fracture, done, stale;
-  int reserved;
+  int rebuilds;              /* contact-list builds of the context so far (all samples) */
   /* extensions (the reference outputs neither): chord Young modulus (GPa)
    * between 10% and 50% of the peak stress, and the Poisson ratio over the
    * same interval from the lateral record; NaN when undefined */

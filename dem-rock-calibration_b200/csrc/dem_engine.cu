@@ -994,10 +994,24 @@ class Engine final : public EngineBase {
     cudaLaunchKernel(pair_kernel_, g, b, params, 0, stream_);
   }
 
+  // Particle kernel grid: the blocks that are resident at once (a grid-stride
+  // loop covers the rest), at most 8 per SM (the block-statistics buffer).
+  uint32_t particle_grid() {
+    if (part_occ_block_ != opt_.particle_block) {
+      int occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_particles<Real>, (int)opt_.particle_block, 0) !=
+          cudaSuccess)
+        occ = 8;
+      part_occ_ = (uint32_t)std::min(std::max(occ, 1), 8);
+      part_occ_block_ = opt_.particle_block;
+    }
+    return std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * part_occ_));
+  }
+
   void launch_step(const StepArgs<Real>& A, int stages) {
     if (stages & 1) launch_pairs(A);
     if (stages & 2) {
-      const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
+      const uint32_t g = particle_grid();
       k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
     }
   }
@@ -1014,6 +1028,7 @@ class Engine final : public EngineBase {
   int capture_steps(uint32_t steps, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     StepArgs<Real> A = args();
+    (void)particle_grid();   // occupancy query outside the capture
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     for (uint32_t k = 0; k < steps; ++k) launch_step(A, 3);
     cudaError_t e = cudaStreamEndCapture(stream_, &g);
@@ -1619,7 +1634,7 @@ class Engine final : public EngineBase {
     CK(cnt.alloc(1));
     StepArgs<Real> A = args();
     A.touching = cnt.p;
-    const uint32_t g = std::max(1u, std::min(ceil_div(np_, opt_.particle_block), (uint32_t)num_sms_ * 8));
+    const uint32_t g = particle_grid();
     for (uint32_t k = 0; k < nsteps; ++k) {
       CK(cudaEventRecord(ev[4 * k], stream_));
       launch_pairs(A);
@@ -1680,6 +1695,7 @@ class Engine final : public EngineBase {
   bool tiles_on_ = false;
   uint32_t ndone_seen_ = 0;
   bool user_grid_ = false;
+  uint32_t part_occ_ = 8, part_occ_block_ = 0;
   bool det_ = false;
   DBuf<Real> mass_;
   DBuf<uint32_t> sid_, orig_;

@@ -590,12 +590,14 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   // flushed with one double atomic per (sample, warp) run
   float my_v2 = 0.f, my_d2 = 0.f;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
+    // the particle's own state is loaded before its sample's flags arrive (the
+    // loads do not depend on them; a finished sample's values go unused)
+    V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
     double sb = 0.0, st = 0.0, sl = 0.0;
     if (!C.done) {
       const SampleParams<Real>& sp = A.sp[s];
-      V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
       V4 f, m;
       if constexpr (sizeof(Real) == 4) {
         if (A.det) {

@@ -561,6 +561,8 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="0: FP32 (default), 1: FP64 build (the Brazilian configuration's FP64 case)")
     ap.add_argument("--skin", type=float, default=0.0,
                     help="contact-list skin as a multiple of the smallest radius (0: the engine default, 0.1)")
     ap.add_argument("--deterministic", action="store_true",
@@ -582,7 +584,7 @@ def main() -> int:
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
     spec = specs[0]
-    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
+    ctx = dem.Context(precision=args.precision, device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
                       deterministic=args.deterministic, skin_factor=args.skin)
     sids = [ctx.add_sample(sp.material, sp.loading, sp.xyz, sp.radii) for sp in specs]
     ctx.setup()
@@ -603,15 +605,17 @@ def main() -> int:
     prof = ctx.profile(min(args.steps, 300))
     res = [ctx.result(s) for s in sids]
     bonds = sum(r["bonds_now"] for r in res)
-    A = algorithmic_bytes(n_gpu, bonds, prof["touching"])
+    A = algorithmic_bytes(n_gpu, bonds, prof["touching"], fp64=args.precision == 1)
     achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    state_mb = (n_gpu * (7 * 16 + 8) + cnt["bonds"] * (8 + 4 * 16) + cnt["contacts"] * 24) / 1e6
+    w = 2 if args.precision == 1 else 1
+    state_mb = (n_gpu * (7 * 16 * w + 8) + cnt["bonds"] * (8 + 4 * 16 * w) + cnt["contacts"] * 24 * w) / 1e6
     stale = sum(r["stale"] for r in res)
     pairs0 = ctx.pairs(sids[0]) if rank == 0 and ws == 1 and not args.no_cpu else None
     ctx.close()
     # the same pipeline on one specimen alone (state inside the L2), for reference
-    one = dem.Context(device=local, graph_steps=200)
+    one = dem.Context(precision=args.precision, device=local, graph_steps=200, skin_factor=args.skin,
+                      deterministic=args.deterministic)
     one.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
     one.setup()
     one.run_timed(args.warmup)
@@ -621,7 +625,8 @@ def main() -> int:
     # end to end through the public API with host buffers: positions uploaded,
     # set-up (Morton sort, bonds, contact list), K steps, results and records read back
     t0 = time.perf_counter()
-    e2 = dem.Context(device=local, graph_steps=200, skin_factor=args.skin, deterministic=args.deterministic)
+    e2 = dem.Context(precision=args.precision, device=local, graph_steps=200, skin_factor=args.skin,
+                     deterministic=args.deterministic)
     for sp in specs:
         ld = dem.Loading.from_buffer_copy(sp.loading)
         ld.max_steps = args.steps
@@ -643,11 +648,12 @@ def main() -> int:
                "sample": f"{args.cpu_steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
                          f"integration) of the {spec.n}-sphere specimen"}
         cpu_bpm = reference_bpm_cpu(spec, pairs0)
-    default_disc = args.workload == "brazilian_disc" and args.specimens == 2
+    default_disc = (args.workload == "brazilian_disc" and args.specimens == 2 and args.precision == 0
+                    and not args.deterministic and args.skin in (0.0, 0.1))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
+        "dtype": "f64" if args.precision == 1 else "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
         "config": {"workload": f"{args.specimens} x {args.workload} ({spec.n} spheres each, radii "
                                f"U[0.18,0.30] mm, Brazilian platens at 0.02 m/s) advanced together"
                                if args.workload == "brazilian_disc" else

@@ -163,7 +163,8 @@ __device__ __forceinline__ bool pair_pred(const PairSearch<Real>& S, uint32_t i,
   if (j <= i) return false;
   if (S.mode == kModeBond) {
     const double r = (double)xi.w + (double)xj.w + (double)S.gap[s];
-    return !(rr < Real(1e-10)) && rr < Real(r * r);
+    // (a gap below -(r_i + r_j) bonds nothing; squaring would bond again)
+    return r > 0.0 && !(rr < Real(1e-10)) && rr < Real(r * r);
   }
   // contact: not bonded
   const Real cut = xi.w + xj.w + (Real)S.gap[s];

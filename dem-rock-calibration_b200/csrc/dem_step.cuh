@@ -582,7 +582,7 @@ __device__ inline void controller_step(SampleCtl& C) {
 }
 
 template <class Real>
-__global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(StepArgs<Real> A) {
   using T = RT<Real>;
   using V4 = typename T::V4;
   __shared__ int s_last;
@@ -592,13 +592,23 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < A.np; p += gridDim.x * blockDim.x) {
     // the particle's own state is loaded before its sample's flags arrive (the
     // loads do not depend on them; a finished sample's values go unused)
-    V4 x = A.pos[p], v = A.vel[p], w = A.omg[p];
+    // (FP32 only: the wider types would hold too many registers across the wait)
+    V4 x, v, w, f, m, xref;
+    if constexpr (sizeof(Real) == 4) {
+      x = A.pos[p];
+      v = A.vel[p];
+      w = A.omg[p];
+      xref = ld4_rw(A.pos_ref + p);
+      if (!A.det) {
+        f = A.frc[p];
+        m = A.mom[p];
+      }
+    }
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
     double sb = 0.0, st = 0.0, sl = 0.0;
     if (!C.done) {
       const SampleParams<Real>& sp = A.sp[s];
-      V4 f, m;
       if constexpr (sizeof(Real) == 4) {
         if (A.det) {
           const longlong2 q0 = *reinterpret_cast<const longlong2*>(A.frcq + 4 * (size_t)p);
@@ -609,16 +619,19 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
                   Real(0));
           m = mk4((Real)((double)u0.x * kFixInv), (Real)((double)u0.y * kFixInv), (Real)((double)u2 * kFixInv),
                   Real(0));
+        }
+      } else {
+        x = A.pos[p];
+        v = A.vel[p];
+        w = A.omg[p];
+        xref = ld4_rw(A.pos_ref + p);
+        if (A.det) {
+          f = unfix4(A.frc[p]);    // FP64 / sensitivity build: fixed point in place
+          m = unfix4(A.mom[p]);
         } else {
           f = A.frc[p];
           m = A.mom[p];
         }
-      } else if (A.det) {
-        f = unfix4(A.frc[p]);    // FP64 / sensitivity build: fixed point in place
-        m = unfix4(A.mom[p]);
-      } else {
-        f = A.frc[p];
-        m = A.mom[p];
       }
       Real F[3] = {f.x, f.y, f.z}, M[3] = {m.x, m.y, m.z};
       if (sp.axis >= 0) {
@@ -706,7 +719,7 @@ __global__ void __launch_bounds__(256) k_particles(StepArgs<Real> A) {
       if (parked) {
         A.pos_ref[p] = x;
       } else {
-        const V4 x0 = ld4_rw(A.pos_ref + p);
+        const V4 x0 = xref;
         const Real e0 = x.x - x0.x, e1 = x.y - x0.y, e2 = x.z - x0.z;
         const Real d2s = (e0 * e0 + e1 * e1) + e2 * e2;
         if (d2s > Real(0.25) * sp.skin_half2) C.rebuild = 1;  // past a quarter of the skin: rebuild soon

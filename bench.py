@@ -377,25 +377,51 @@ def surrogate_flops(sizes, rows: int) -> float:
     return 2.0 * rows * (2 * sum(mm) + sum(mm[1:]))
 
 
+def S_space():
+    return importlib.import_module("dem-rock-calibration_b200.sweep").SWEEP_SPACE
+
+
 def run_surrogate(args, ws, rank, local):
     """Surrogate MLP 6-256-256-256-4 (GELU, BF16 operands, FP32 accumulation in
     tensor memory) trained by mini-batch Adam (batch 256) on 8192 samples, one
     CUDA-graph replay per epoch; every rank trains its own network (weak
     scaling).  Inputs are the six sweep micro-parameters scaled to [-1, 1],
     targets a seeded smooth four-output map standing in for (UCS, E, nu,
-    tensile strength) of simulated specimens.  Also times the forward GEMM of
-    a 65,536-candidate proposal batch."""
+    tensile strength) of simulated specimens - or, with --sim-data N, the
+    properties of N Latin-hypercube parameter sets simulated first by the
+    batched engine (uniaxial and Brazilian tests of 2,000-sphere specimens,
+    deterministic mode), reported with the simulation rate and the held-out
+    error of the trained network.  Also times the forward GEMM of a
+    65,536-candidate proposal batch."""
     import torch
     S = importlib.import_module("dem-rock-calibration_b200.surrogate")
     D = Dist(ws)
     torch.cuda.set_device(local)
     sizes = (6, 256, 256, 256, 4)
-    n, batch = 8192, 256
-    rng = np.random.default_rng(17 + rank)
-    X = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
-    Y = np.stack([np.sin(2 * X[:, 0]) + X[:, 1] ** 2 - X[:, 3], X[:, 2] * X[:, 3] + 0.5 * X[:, 0],
-                  np.exp(0.5 * X[:, 4]) - X[:, 5] * X[:, 1], X[:, 0] * X[:, 5] + 0.3 * X[:, 2]], 1)
-    Y = ((Y - Y.mean(0)) / Y.std(0)).astype(np.float32)
+    batch = 256
+    sim = None
+    if args.sim_data > 0:
+        Xs, Ys, t_sim = S.simulate_dataset(args.sim_data, seed=1 + rank, uni=S.UniaxialJudge(device=local),
+                                           braz=S.BrazilJudge(device=local))
+        ok = np.all(np.isfinite(Ys), axis=1) & (Ys[:, 0] > 0) & (Ys[:, 3] > 0)
+        Xs, Ys = Xs[ok], Ys[ok]
+        lo = np.array([v[0] for v in S_space().values()])
+        hi = np.array([v[1] for v in S_space().values()])
+        Xn = (2.0 * (Xs - lo) / (hi - lo) - 1.0).astype(np.float32)
+        mu_y, sd_y = Ys.mean(0), Ys.std(0) + 1e-30
+        Yn = ((Ys - mu_y) / sd_y).astype(np.float32)
+        n_test = max(1, len(Xn) // 10)
+        X, Y = Xn[n_test:], Yn[n_test:]
+        sim = dict(cases=int(args.sim_data), kept=int(ok.sum()), seconds=t_sim,
+                   solves_per_hour=2 * args.sim_data / t_sim * 3600.0,
+                   test=(Xn[:n_test], Yn[:n_test], sd_y))
+    else:
+        n = 8192
+        rng = np.random.default_rng(17 + rank)
+        X = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+        Y = np.stack([np.sin(2 * X[:, 0]) + X[:, 1] ** 2 - X[:, 3], X[:, 2] * X[:, 3] + 0.5 * X[:, 0],
+                      np.exp(0.5 * X[:, 4]) - X[:, 5] * X[:, 1], X[:, 0] * X[:, 5] + 0.3 * X[:, 2]], 1)
+        Y = ((Y - Y.mean(0)) / Y.std(0)).astype(np.float32)
     net = S.MLP(sizes, seed=rank, device=local)
     ep = S.Epochs(net, X, Y, batch, seed=rank)
     loss0 = ep.run()
@@ -420,6 +446,13 @@ def run_surrogate(args, ws, rank, local):
     value = D.sum(float(rows)) * epochs / (ms_max * 1e-3)
     flops = surrogate_flops(sizes, rows) * epochs
     ep.close()
+    if sim is not None:
+        # held-out error of the trained network, per property, in units of that
+        # property's spread over the dataset, and relative to its mean magnitude
+        Xt, Yt, sd_y = sim.pop("test")
+        pred = net.predict(Xt)
+        rmse = np.sqrt(np.mean((pred - Yt) ** 2, axis=0))
+        sim["test_rmse_in_sd"] = dict(zip(("UCS", "E", "nu", "sigma_t"), map(float, rmse)))
     # inference GEMM of a 65,536-candidate proposal batch (hidden layer 256 x 256:
     # bias + GELU, BF16 out, no pre-activation kept), alone
     M, N, K = 65536, 256, 256
@@ -460,10 +493,11 @@ def run_surrogate(args, ws, rank, local):
         "metric": "surrogate training samples/s", "value": value, "unit": "samples/s", "n_gpus": ws,
         "steps": epochs, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / epochs, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 operands, f32 accumulation",
-        "data": "synthetic (seeded inputs in the sweep box, smooth 4-output targets)",
+        "data": ("simulated: batched uniaxial + Brazilian solves of Latin-hypercube parameter sets"
+                 if sim is not None else "synthetic (seeded inputs in the sweep box, smooth 4-output targets)"),
         "config": {"workload": f"surrogate MLP {'-'.join(map(str, sizes))} GELU, {rows} samples per epoch, "
                                f"batch {batch}, Adam", "step": "one epoch (one CUDA-graph replay)",
-                   "loss_first_epoch": loss0, "loss_last_epoch": loss1,
+                   "loss_first_epoch": loss0, "loss_last_epoch": loss1, "simulated_dataset": sim,
                    "train_tflops": flops / (ms_max * 1e-3) / 1e12,
                    "l2": "dataset and weights inside the L2 (the whole job is 10 MB)"},
         "gpu_launches": epochs * len(ep.sizes) * net.launches_per_step(),
@@ -561,6 +595,8 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sim-data", type=int, default=0,
+                    help="surrogate: train on this many simulated parameter sets instead of synthetic targets")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
                     help="0: FP32 (default), 1: FP64 build (the Brazilian configuration's FP64 case)")
     ap.add_argument("--skin", type=float, default=0.0,

@@ -468,6 +468,64 @@ class UniaxialJudge:
         return np.array([[r["FractureStress"], r["E_chord"], r["nu"]] for r in res])
 
 
+class BrazilJudge:
+    """Brazilian tests of one packed disc (about n spheres, thickness half the
+    diameter, axis z, platens across the diameter) under many parameter sets,
+    in one batched context, deterministic mode; returns the tensile strength
+    (GPa) per row (the reference's sigma_B = F / (pi R t), md_data_types.h:395)."""
+
+    def __init__(self, n: int = 2000, seed: int = 6, velocity_m_s: float = 0.1, max_steps: int = 400000,
+                 device: int = 0, deterministic: bool = True):
+        from . import sweep
+        self.sweep, self.seed, self.device = sweep, seed, device
+        self.deterministic = deterministic
+        self.velocity, self.max_steps = velocity_m_s, max_steps
+        self.xyz, self.rad, _, self.box, self.size_real, self.center_real = sweep.cylinder(n, seed, aspect=0.5,
+                                                                                           device=device)
+        self.keys = list(sweep.SWEEP_SPACE)
+
+    def __call__(self, P: np.ndarray) -> np.ndarray:
+        from . import TEST_BRAZIL, VELOCITY, Context, loading
+        P = np.atleast_2d(np.asarray(P, np.float64))
+        r_min, r_mean = float(self.rad.min()), float(self.rad.mean())
+        ctx = Context(device=self.device, deterministic=self.deterministic)
+        try:
+            for row in P:
+                p = dict(zip(self.keys, row))
+                ld = loading(TEST_BRAZIL, self.box, self.size_real, self.center_real,
+                             velocity=-self.velocity / VELOCITY, min_stress=0.0021, max_strain=0.03,
+                             cond_fracture=0.1, dNsave=1000, max_steps=self.max_steps, p_r_platen=r_mean)
+                ctx.add_sample(self.sweep.material_for(p, r_min, r_mean, self.seed * 7919 + 1), ld, self.xyz,
+                               self.rad)
+            ctx.setup()
+            ctx.run(self.max_steps)
+            out = np.array([ctx.result(i)["FractureStress"] for i in range(len(P))])
+        finally:
+            ctx.close()
+        return out
+
+
+def simulate_dataset(n: int, seed: int = 0, uni: "UniaxialJudge | None" = None, braz: "BrazilJudge | None" = None,
+                     batch: int = 256, space=None):
+    """n Latin-hypercube parameter sets of the sweep box and their simulated
+    macro properties: columns (UCS, E, nu) from uniaxial tests, plus the
+    tensile strength from Brazilian tests when braz is given; batch cases per
+    context.  Returns (X (n x 6), Y (n x 3 or 4), seconds)."""
+    import time
+
+    from . import sweep
+    space = space or sweep.SWEEP_SPACE
+    lo = np.array([v[0] for v in space.values()])
+    hi = np.array([v[1] for v in space.values()])
+    X = latin_box(n, lo, hi, seed)
+    uni = uni or UniaxialJudge()
+    t0 = time.perf_counter()
+    cols = [np.vstack([uni(X[a:a + batch]) for a in range(0, n, batch)])]
+    if braz is not None:
+        cols.append(np.concatenate([braz(X[a:a + batch]) for a in range(0, n, batch)])[:, None])
+    return X, np.hstack(cols), time.perf_counter() - t0
+
+
 @dataclass
 class CalibrationRun:
     target: np.ndarray

@@ -670,10 +670,13 @@ def main() -> int:
     e2.setup()
     t_setup = time.perf_counter() - t0
     e2.run(args.steps)
+    t_run = time.perf_counter() - t0 - t_setup
     recs = [e2.record(k) for k in range(len(specs))]
     res2 = [e2.result(k) for k in range(len(specs))]
-    e2.close()
     t_e2e = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    e2.close()
+    t_close = time.perf_counter() - t1
     e2e_val = D.sum(n_gpu * args.steps / t_e2e)
     h2d = sum(sp.xyz.nbytes + sp.radii.nbytes for sp in specs)
     d2h = sum(r.nbytes + b.nbytes for r, b in recs) + len(specs) * 160
@@ -714,6 +717,7 @@ def main() -> int:
                      "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e, "setup_seconds": t_setup,
+                "run_seconds": t_run, "close_seconds_untimed": t_close,
                 "contact_list_builds": res2[0]["rebuilds"],
                 "note": "public API from host positions: upload, set-up, steps, results and records read back"},
         "cpu_baseline": cpu,

@@ -401,8 +401,8 @@ def run_surrogate(args, ws, rank, local):
     batch = 256
     sim = None
     if args.sim_data > 0:
-        Xs, Ys, t_sim = S.simulate_dataset(args.sim_data, seed=1 + rank, uni=S.UniaxialJudge(device=local),
-                                           braz=S.BrazilJudge(device=local))
+        Xs, Ys, t_sim = S.simulate_dataset(args.sim_data, seed=1 + rank, uni=S.UniaxialSolver(device=local),
+                                           braz=S.BrazilSolver(device=local))
         ok = np.all(np.isfinite(Ys), axis=1) & (Ys[:, 0] > 0) & (Ys[:, 3] > 0)
         Xs, Ys = Xs[ok], Ys[ok]
         lo = np.array([v[0] for v in S_space().values()])
@@ -539,7 +539,7 @@ def run_solves(args, ws, rank, local):
     sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
     D = Dist(ws)
     torch.cuda.set_device(local)
-    J = S.UniaxialJudge(n=2000, seed=5 + rank, device=local)
+    J = S.UniaxialSolver(n=2000, seed=5 + rank, device=local)
     lo = np.array([v[0] for v in sweep.SWEEP_SPACE.values()])
     hi = np.array([v[1] for v in sweep.SWEEP_SPACE.values()])
     X = S.latin_box(args.cases, lo, hi, 1 + rank)

@@ -18,8 +18,8 @@ MLP            the network: forward, backward, Adam, fit, predict, input gradien
 Surrogate      normalisation of parameters and properties around an MLP
 propose        batched multi-start inversion: the parameter sets whose predicted
                properties are closest to a target
-calibrate      the loop of the reference workflow with the batched simulator as
-               the judge: fit, propose, simulate the proposals, accept a
+calibrate      the loop of the reference workflow with the batched simulator
+               deciding: fit, propose, simulate the proposals, accept a
                proposal only when the simulator confirms it, else add the new
                simulations to the data and refit
 """
@@ -420,12 +420,12 @@ class Surrogate:
         return params, self.predict(params)
 
 
-# ---- the plain simulator as the judge, and the calibration loop ----------
+# ---- the plain simulator that decides, and the calibration loop ----------
 
 PROPS = ("UCS", "E", "nu")
 
 
-class UniaxialJudge:
+class UniaxialSolver:
     """Uniaxial tests of one packed cylinder (about n spheres) under many
     parameter sets (rows in the order of sweep.SWEEP_SPACE) in one batched
     context.  Every case draws its bond strengths with the same seed, and the
@@ -468,7 +468,7 @@ class UniaxialJudge:
         return np.array([[r["FractureStress"], r["E_chord"], r["nu"]] for r in res])
 
 
-class BrazilJudge:
+class BrazilSolver:
     """Brazilian tests of one packed disc (about n spheres, thickness half the
     diameter, axis z, platens across the diameter) under many parameter sets,
     in one batched context, deterministic mode; returns the tensile strength
@@ -505,7 +505,7 @@ class BrazilJudge:
         return out
 
 
-def simulate_dataset(n: int, seed: int = 0, uni: "UniaxialJudge | None" = None, braz: "BrazilJudge | None" = None,
+def simulate_dataset(n: int, seed: int = 0, uni: "UniaxialSolver | None" = None, braz: "BrazilSolver | None" = None,
                      batch: int = 256, space=None):
     """n Latin-hypercube parameter sets of the sweep box and their simulated
     macro properties: columns (UCS, E, nu) from uniaxial tests, plus the
@@ -518,7 +518,7 @@ def simulate_dataset(n: int, seed: int = 0, uni: "UniaxialJudge | None" = None, 
     lo = np.array([v[0] for v in space.values()])
     hi = np.array([v[1] for v in space.values()])
     X = latin_box(n, lo, hi, seed)
-    uni = uni or UniaxialJudge()
+    uni = uni or UniaxialSolver()
     t0 = time.perf_counter()
     cols = [np.vstack([uni(X[a:a + batch]) for a in range(0, n, batch)])]
     if braz is not None:
@@ -557,10 +557,10 @@ def score(props, target, tol) -> np.ndarray:
     return np.where(np.isfinite(out), out, np.inf)
 
 
-def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_round: int = 16, tol=0.01,
+def calibrate(solve, target, lo, hi, n_init: int = 64, rounds: int = 3, per_round: int = 16, tol=0.01,
               epochs: int = 300, seed: int = 0, X0=None, Y0=None, device: int = 0) -> CalibrationRun:
     """The reference's surrogate loop (NN_MP.py:766-930) with the simulator as
-    the judge: simulate a Latin-hypercube start set (or take X0, Y0), then per
+    the arbiter: simulate a Latin-hypercube start set (or take X0, Y0), then per
     round fit the surrogate to everything simulated so far, propose per_round
     parameter sets whose predicted properties are closest to target (errors
     weighted by 1 / tol^2), simulate them in one batched context, and stop
@@ -573,7 +573,7 @@ def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_roun
     tol = np.broadcast_to(np.asarray(tol, np.float64), target.shape).copy()
     if X0 is None:
         X = latin_box(n_init, lo, hi, seed)
-        Y = judge(X)
+        Y = solve(X)
     else:
         X, Y = np.asarray(X0, np.float64), np.asarray(Y0, np.float64)
     sims = len(X)
@@ -592,7 +592,7 @@ def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_roun
             i = int(np.argmin(cand))
             if cand[i] > 1.0:
                 return
-            again = judge(X[i:i + 1])[0]
+            again = solve(X[i:i + 1])[0]
             sims += 1
             if score(again, target, tol)[0] <= 1.0:
                 accepted, confirmed = True, again
@@ -605,7 +605,7 @@ def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_roun
         ok = np.all(np.isfinite(Y), axis=1)
         sur.fit(X[ok], Y[ok], epochs=epochs, batch=min(256, int(ok.sum())))
         P, _ = sur.propose(target, k=per_round, weights=w, seed=seed + r)
-        Yp = judge(P)
+        Yp = solve(P)
         sims += len(P)
         X, Y = np.vstack([X, P]), np.vstack([Y, Yp])
         rejected = np.concatenate([rejected, np.zeros(len(P), bool)])
@@ -616,7 +616,7 @@ def calibrate(judge, target, lo, hi, n_init: int = 64, rounds: int = 3, per_roun
     return CalibrationRun(target, tol, X, Y, X[i], Y[i], float(sc[i]), accepted, confirmed, r, sims, scores)
 
 
-def random_search(judge, target, lo, hi, budget: int, tol=0.01, seed: int = 0, X0=None, Y0=None,
+def random_search(solve, target, lo, hi, budget: int, tol=0.01, seed: int = 0, X0=None, Y0=None,
                   batch: int = 16) -> CalibrationRun:
     """The method without the network at the same simulator budget: further
     Latin-hypercube points after the start set, the best simulated case kept
@@ -628,7 +628,7 @@ def random_search(judge, target, lo, hi, budget: int, tol=0.01, seed: int = 0, X
     extra = latin_box(budget - len(X), lo, hi, seed + 1000) if budget > len(X) else np.empty((0, len(lo)))
     for a in range(0, len(extra), batch):
         P = extra[a:a + batch]
-        X, Y = np.vstack([X, P]), np.vstack([Y, judge(P)])
+        X, Y = np.vstack([X, P]), np.vstack([Y, solve(P)])
         scores.append(float(score(Y, target, tol).min()))
     sc = score(Y, target, tol)
     i = int(np.argmin(sc))

@@ -53,7 +53,7 @@ def _run(J, P, det=True):
 
 
 def test_runs_are_bit_reproducible_and_independent_of_the_batch():
-    J = S.UniaxialJudge(n=2000, seed=5)
+    J = S.UniaxialSolver(n=2000, seed=5)
     P = _params(4)
     a = _run(J, P)
     b = _run(J, P)
@@ -67,7 +67,7 @@ def test_runs_are_bit_reproducible_and_independent_of_the_batch():
 
 
 def test_deterministic_mode_agrees_with_float_atomics():
-    J = S.UniaxialJudge(n=2000, seed=5)
+    J = S.UniaxialSolver(n=2000, seed=5)
     P = _params(4)
     d = _run(J, P, det=True)
     f = _run(J, P, det=False)
@@ -78,7 +78,7 @@ def test_deterministic_mode_agrees_with_float_atomics():
 
 
 def test_fp64_and_sensitivity_runs_repeat_exactly():
-    J = S.UniaxialJudge(n=2000, seed=5)
+    J = S.UniaxialSolver(n=2000, seed=5)
     r_min, r_mean = float(J.rad.min()), float(J.rad.mean())
     P = _params(2)
     for precision in (1, 2):
@@ -104,7 +104,7 @@ def test_autotuned_run_equals_plain_run():
     """The autotuner's steps are ordinary steps of the run: in deterministic
     mode a run that starts with an autotune gives bit-identical results to
     one that does not, and the tuner reports its timed candidates."""
-    J = S.UniaxialJudge(n=2000, seed=5)
+    J = S.UniaxialSolver(n=2000, seed=5)
     r_min, r_mean = float(J.rad.min()), float(J.rad.mean())
     P = _params(3)
     res = []

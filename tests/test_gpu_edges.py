@@ -28,7 +28,7 @@ KEYS = ("FractureStress", "FractureStrain", "E_chord", "nu", "steps", "bonds_now
 
 
 def _spec(n=2000, seed=5):
-    J = S.UniaxialJudge(n=n, seed=seed)
+    J = S.UniaxialSolver(n=n, seed=seed)
     return J
 
 

@@ -38,7 +38,7 @@ TOL = np.array([0.01, 0.01, 0.01])     # UCS, E, nu
 
 
 def test_surrogate_beats_latin_hypercube_at_equal_simulation_budget():
-    J = S.UniaxialJudge(n=2000, seed=5)
+    J = S.UniaxialSolver(n=2000, seed=5)
     lo = np.array([v[0] for v in sweep.SWEEP_SPACE.values()])
     hi = np.array([v[1] for v in sweep.SWEEP_SPACE.values()])
     X0 = S.latin_box(64, lo, hi, 1)

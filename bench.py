@@ -500,7 +500,7 @@ def run_surrogate(args, ws, rank, local):
                    "loss_first_epoch": loss0, "loss_last_epoch": loss1, "simulated_dataset": sim,
                    "train_tflops": flops / (ms_max * 1e-3) / 1e12,
                    "l2": "dataset and weights inside the L2 (the whole job is 10 MB)"},
-        "gpu_launches": epochs * len(ep.sizes) * net.launches_per_step(),
+        "gpu_launches": epochs * sum(net.launches_per_step(b) for b in ep.sizes),
         "clocks": clocks,
         "roofline": (lambda ai, ridge, gbs: {
             "bound": "hbm" if ai < ridge else "tensor",

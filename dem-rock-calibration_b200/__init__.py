@@ -165,6 +165,7 @@ def _declare(L):
     L.dem_mlp_mse_grad.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp]
     L.dem_mlp_adam.argtypes = [_vp, _vp, _vp, _vp, _sz, _f, _f, _f, _f, _f, _vp, _vp, _vp]
     L.dem_mlp_tick.argtypes = [_vp, _vp]
+    L.dem_mlp_adam_multi.argtypes = [_vp, C.c_int, _sz, _f, _f, _f, _f, _vp, _vp]
 
 
 def _lib():

@@ -421,6 +421,27 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
   }
 }
 
+// Adam over a list of arrays in one launch: block row y updates array y of
+// the descriptor list (grid-stride over its elements), with the same update as
+// k_adam.
+__global__ void k_adam_multi(const dem_mlp_tensor* __restrict__ list, float lr, float b1, float b2, float eps,
+                             const int* __restrict__ step) {
+  const dem_mlp_tensor T = list[blockIdx.y];
+  const float t = (float)max(*step, 1);
+  const float c1 = 1.f - powf(b1, t), c2 = 1.f - powf(b2, t);
+  __nv_bfloat16* wh = static_cast<__nv_bfloat16*>(T.w_bf16);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < T.n; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = T.g[i] + T.l2 * T.w[i];
+    const float mi = b1 * T.m[i] + (1.f - b1) * gi;
+    const float vi = b2 * T.v[i] + (1.f - b2) * gi * gi;
+    T.m[i] = mi;
+    T.v[i] = vi;
+    const float wi = T.w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    T.w[i] = wi;
+    if (wh) wh[i] = __float2bfloat16_rn(wi);
+  }
+}
+
 // per device: a flag set by a GEMM block whose tensor-core commit timed out
 constexpr int kMaxDev = 64;
 std::mutex g_mu;
@@ -569,10 +590,13 @@ int dem_mlp_act_backward(const float* dh, const float* z, size_t n, int act, voi
 
 int dem_mlp_colsum(const float* in, int rows, int cols, float* out, float* scratch, void* stream) {
   if (!in || !out || !scratch || rows <= 0 || cols <= 0) return DEM_ERR_ARG;
-  const int S = std::min(DEM_MLP_COLSUM_SPLIT, std::max(1, rows / 64));
+  // up to 2048 rows one pass writes the sums directly; beyond, partial sums of
+  // row slices are added in order by a second pass
+  const int S = rows <= 2048 ? 1 : std::min(DEM_MLP_COLSUM_SPLIT, rows / 256);
   k_colsum_part<<<dim3((unsigned)((cols + 31) / 32), (unsigned)S), dim3(32, 8), 0, (cudaStream_t)stream>>>(
-      in, rows, cols, scratch);
-  k_colsum_final<<<(unsigned)((cols + 127) / 128), 128, 0, (cudaStream_t)stream>>>(scratch, S, cols, out);
+      in, rows, cols, S == 1 ? out : scratch);
+  if (S > 1)
+    k_colsum_final<<<(unsigned)((cols + 127) / 128), 128, 0, (cudaStream_t)stream>>>(scratch, S, cols, out);
   return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 
@@ -593,6 +617,14 @@ int dem_mlp_mse_grad(const float* y, const float* t, size_t n, void* dy_bf16, fl
   if (!y || !t || !dy_bf16 || n == 0) return DEM_ERR_ARG;
   k_mse_grad<<<blocks(n), 256, 0, (cudaStream_t)stream>>>(y, t, n, static_cast<__nv_bfloat16*>(dy_bf16), dy_f32,
                                                          loss);
+  return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}
+
+int dem_mlp_adam_multi(const dem_mlp_tensor* list, int count, size_t max_n, float lr, float b1, float b2,
+                       float eps, const int* step, void* stream) {
+  if (!list || !step || count <= 0 || count > 65535 || max_n == 0) return DEM_ERR_ARG;
+  const dim3 g(std::min<uint32_t>((uint32_t)((max_n + 255) / 256), 148u * 4u), (unsigned)count);
+  k_adam_multi<<<g, 256, 0, (cudaStream_t)stream>>>(list, lr, b1, b2, eps, step);
   return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 

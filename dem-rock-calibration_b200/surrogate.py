@@ -99,6 +99,17 @@ class MLP:
         self.loss_acc = torch.zeros(1, dtype=torch.float64, device=self.dev)
         self.scratch = torch.zeros(COLSUM_SPLIT * max(self.np_ + self.kp), **f32)
         self._bufs = {}
+        # device descriptor list of every weight and bias array for the one-launch
+        # Adam step (dem_mlp_tensor: w, g, m, v, w_bf16, n, l2, pad)
+        nl = len(self.W)
+        rec = np.zeros(len(self.params), dtype=[("w", "<u8"), ("g", "<u8"), ("m", "<u8"), ("v", "<u8"),
+                                                  ("wh", "<u8"), ("n", "<u8"), ("l2", "<f4"), ("pad", "<f4")])
+        for i, (w, g, m, v) in enumerate(zip(self.params, self.grads, self.m, self.v)):
+            rec[i] = (w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
+                      self.Wh[i].data_ptr() if i < nl else 0, w.numel(),
+                      self.l2 if i < nl else 0.0, 0.0)      # sklearn penalises the weights, not the biases
+        self.adam_list = torch.from_numpy(rec.view(np.uint8).copy()).to(self.dev)
+        self.adam_max_n = int(max(p.numel() for p in self.params))
         self._graph = None
 
     # ---- buffers -------------------------------------------------------
@@ -193,21 +204,18 @@ class MLP:
     def _adam(self):
         P, L, s = self._ptr, self.L, self._s()
         _ck(L.dem_mlp_tick(P(self.step), s), "dem_mlp_tick")
-        nl = len(self.W)
-        for i, (w, g, m, v) in enumerate(zip(self.params, self.grads, self.m, self.v)):
-            wh = P(self.Wh[i]) if i < nl else None
-            l2 = self.l2 if i < nl else 0.0      # sklearn penalises the weights, not the biases
-            _ck(L.dem_mlp_adam(P(w), P(g), P(m), P(v), w.numel(), self.lr, self.b1, self.b2, self.eps, l2,
-                               P(self.step), wh, s), "dem_mlp_adam")
+        _ck(L.dem_mlp_adam_multi(P(self.adam_list), len(self.params), self.adam_max_n, self.lr, self.b1, self.b2,
+                                 self.eps, P(self.step), s), "dem_mlp_adam_multi")
 
-    def launches_per_step(self) -> int:
+    def launches_per_step(self, batch: int = 256) -> int:
         """Kernel launches of one train_step: gather + input pack + one GEMM per
         layer; MSE gradient + pack, per layer two transposes, the weight-gradient
-        GEMM and the two column-sum passes, per layer but the first a transpose,
-        the input-gradient GEMM and the activation backward; the step tick and
-        one Adam launch per weight and bias array."""
+        GEMM and the column sums (one pass up to 2048 rows, else two), per layer
+        but the first a transpose, the input-gradient GEMM and the activation
+        backward; the step tick and one Adam launch for all arrays."""
         nl = len(self.W)
-        return (2 + nl) + (2 + 5 * nl + 3 * (nl - 1)) + (1 + 2 * nl)
+        cs = 1 if batch <= 2048 else 2
+        return (2 + nl) + (2 + (4 + cs) * nl + 3 * (nl - 1)) + 2
 
     def train_step(self, x, t, idx):
         """One Adam step on the rows idx (device int32) of x / t (device FP32)."""

@@ -305,7 +305,7 @@ int dem_mlp_transpose_bf16(const void* in, int rows, int cols, int ldo, void* ou
 int dem_mlp_act_backward(const float* dh, const float* z, size_t n, int act, void* dz_bf16, float* dz_f32,
                          void* stream);
 /* out[c] = sum over rows of in[r][c] (FP32, a fixed summation order);
- * scratch holds DEM_MLP_COLSUM_SPLIT * cols floats */
+ * scratch holds DEM_MLP_COLSUM_SPLIT * cols floats (used above 2048 rows) */
 #define DEM_MLP_COLSUM_SPLIT 32
 int dem_mlp_colsum(const float* in, int rows, int cols, float* out, float* scratch, void* stream);
 /* dY = 2 (y - t) / n (BF16, and FP32 when given); *loss (double, device) += mean squared error */
@@ -316,6 +316,20 @@ int dem_mlp_mse_grad(const float* y, const float* t, size_t n, void* dy_bf16, fl
 int dem_mlp_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps,
                  float l2, const int* step, void* w_bf16, void* stream);
 int dem_mlp_tick(int* step, void* stream);
+/* The same Adam step over `count` arrays in one launch: `list` is a device
+ * array of descriptors (n elements each, at most max_n), per-array l2. */
+typedef struct {
+  float* w;
+  const float* g;
+  float* m;
+  float* v;
+  void* w_bf16;      /* BF16 copy to refresh, or NULL */
+  uint64_t n;
+  float l2;
+  float pad;
+} dem_mlp_tensor;
+int dem_mlp_adam_multi(const dem_mlp_tensor* list, int count, size_t max_n, float lr, float b1, float b2, float eps,
+                       const int* step, void* stream);
 
 /* --- reference entry points --- */
 /* One loading test of one specimen from host positions to macro results and

@@ -138,6 +138,32 @@ def test_small_kernels():
     assert int(step) == 3
     assert np.allclose(w.cpu().numpy(), wn, rtol=1e-5, atol=1e-6)
     assert torch.equal(wh, w.to(torch.bfloat16))
+    # the one-launch Adam over a descriptor list equals the per-array launches
+    arrs = []
+    for n_, l2 in ((700, 1e-3), (33, 0.0)):
+        w0 = torch.randn(n_, device="cuda", generator=g)
+        g0 = torch.randn(n_, device="cuda", generator=g)
+        arrs.append([(w0.clone(), g0, torch.zeros(n_, device="cuda"), torch.zeros(n_, device="cuda"),
+                      torch.zeros(n_, dtype=torch.bfloat16, device="cuda"), l2) for _ in range(2)])
+    st1 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st2 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rec = np.zeros(2, dtype=[("w", "<u8"), ("g", "<u8"), ("m", "<u8"), ("v", "<u8"), ("wh", "<u8"), ("n", "<u8"),
+                             ("l2", "<f4"), ("pad", "<f4")])
+    for k, pair in enumerate(arrs):
+        w_, g_, m_, v_, h_, l2 = pair[1]
+        rec[k] = (w_.data_ptr(), g_.data_ptr(), m_.data_ptr(), v_.data_ptr(), h_.data_ptr(), w_.numel(), l2, 0.0)
+    lst = torch.from_numpy(rec.view(np.uint8).copy()).cuda()
+    for it in range(3):
+        assert L.dem_mlp_tick(_p(st1), _s()) == 0 and L.dem_mlp_tick(_p(st2), _s()) == 0
+        for pair in arrs:
+            w_, g_, m_, v_, h_, l2 = pair[0]
+            assert L.dem_mlp_adam(_p(w_), _p(g_), _p(m_), _p(v_), w_.numel(), 1e-2, 0.9, 0.999, 1e-8, l2, _p(st1),
+                                  _p(h_), _s()) == 0
+        assert L.dem_mlp_adam_multi(_p(lst), 2, 700, 1e-2, 0.9, 0.999, 1e-8, _p(st2), _s()) == 0
+    torch.cuda.synchronize()
+    for pair in arrs:
+        for a, b in zip(pair[0][:5], pair[1][:5]):
+            assert torch.equal(a, b)
 
 
 def _rel(a, b):

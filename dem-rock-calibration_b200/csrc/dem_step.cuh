@@ -228,6 +228,42 @@ __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i
   if (!dropJ) acc_m(A, j, mJ[0], mJ[1], mJ[2]);
 }
 
+// The i-side force and moment of an intact bond.  FP32 float atomics: bonds
+// are stored sorted by i, so the lanes of a warp that share i are adjacent;
+// when the whole warp is here their contributions are first summed over each
+// run of equal i (a segmented suffix sum by shuffles) and the run's first lane
+// issues the two reductions, which cuts the vector reductions reaching L2 by
+// about a third.  Otherwise (deterministic mode, FP64, a partial warp) every
+// lane adds its own.
+template <class Real>
+__device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t i, Real f0, Real f1, Real f2,
+                                               Real m0, Real m1, Real m2) {
+  if constexpr (sizeof(Real) == 4) {
+    if (!A.det && __activemask() == 0xFFFFFFFFu) {
+      const uint32_t lane = threadIdx.x & 31;
+      float v[6] = {f0, f1, f2, m0, m1, m2};
+#pragma unroll
+      for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t io = __shfl_down_sync(0xFFFFFFFFu, i, d);
+        const bool same = lane + d < 32 && io == i;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const float o = __shfl_down_sync(0xFFFFFFFFu, v[k], d);
+          if (same) v[k] += o;
+        }
+      }
+      const uint32_t iu = __shfl_up_sync(0xFFFFFFFFu, i, 1);
+      if (lane == 0 || iu != i) {
+        acc3(A.frc + i, v[0], v[1], v[2]);
+        acc3(A.mom + i, v[3], v[4], v[5]);
+      }
+      return;
+    }
+  }
+  acc_f(A, i, f0, f1, f2);
+  acc_m(A, i, m0, m1, m2);
+}
+
 // One bond (i < j).  The arithmetic is that of d_CalculateForcesDEM_22 for the
 // slot i->j (md_calculateforcesdem3.cu:41-200, 427-486); the slot j->i of the
 // reference is its exact mirror (all vectors negated, the unsymmetric moment
@@ -324,10 +360,10 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, con
     const Real mu1 = half * (rz * ot0 - rx * ot2) * cef;
     const Real mu2 = half * (rx * ot1 - ry * ot0) * cef;
     // contributions: i gets (F, Mn+Mt+Mu), j gets (-F, -(Mn+Mt)+Mu)
-    acc_f(A, i, fn0 + ft0, fn1 + ft1, fn2 + ft2);
     acc_f(A, j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2));
-    acc_m(A, i, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1, (tn2 + tt2) + mu2);
     acc_m(A, j, mu0 - (tn0 + tt0), mu1 - (tn1 + tt1), mu2 - (tn2 + tt2));
+    scatter_i_warp<Real>(A, i, fn0 + ft0, fn1 + ft1, fn2 + ft2, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1,
+                         (tn2 + tt2) + mu2);
     // break test (dd_CheckBreakConditionDEM_2)
     bool broke = false;
     if (!sp.nobreak) {
@@ -416,30 +452,48 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
 // Pair kernel: one thread per bond, then one per contact-list pair, grid
 // stride.  A block's bonds of one pass are a contiguous tile of blockDim
 // bonds; while the block works on it, one thread asks the copy engine to
-// prefetch the block's next tile of bond state into L2 (five bulk prefetches),
-// so the next pass finds its streamed loads in L2.  Bond arrays are padded to
-// whole 256-bond tiles.
+// prefetch the block's next tile of bond state into L2 (four bulk prefetches),
+// so the next pass finds its streamed loads in L2, and every thread already
+// holds the next tile's pair indices.  Bond arrays are padded to whole
+// 256-bond tiles.
 template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2), int kBlock = 256>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) {
   using V4 = typename RT<Real>::V4;
   const uint32_t nb = A.nb;
   const uint32_t tile = blockDim.x, stride = gridDim.x * tile;
   const uint32_t ntl = A.tiles ? *A.ntiles : (nb + tile - 1) / tile;
-  for (uint32_t k = blockIdx.x; k < ntl; k += gridDim.x) {
-    const uint32_t base = (A.tiles ? A.tiles[k] : k) * tile;
-    if (threadIdx.x == 0 && k + gridDim.x < ntl) {
-      const size_t nx = A.tiles ? (size_t)A.tiles[k + gridDim.x] * tile : (size_t)base + stride;
-      l2_prefetch(A.b_ij + nx, tile * sizeof(uint2));
-      l2_prefetch(A.b_par + nx, tile * sizeof(V4));
-      l2_prefetch(A.b_s0 + nx, tile * sizeof(V4));
-      l2_prefetch(A.b_s1 + nx, tile * sizeof(V4));
-      l2_prefetch(A.b_s2 + nx, tile * sizeof(V4));
+  // software pipeline over the block's tiles: the pair indices and the sample
+  // of the next tile are loaded before this tile's gathers, so a pass starts
+  // its particle gathers at once instead of after an index round trip
+  uint32_t k = blockIdx.x;
+  uint32_t base = 0, ts = ~0u;
+  uint2 ij = make_uint2(0, 0);
+  if (k < ntl) {
+    base = (A.tiles ? A.tiles[k] : k) * tile;
+    if (A.tile_s) ts = __ldg(A.tile_s + base / tile);
+    if (base + threadIdx.x < nb) ij = __ldcs(A.b_ij + base + threadIdx.x);
+  }
+  for (; k < ntl; k += gridDim.x) {
+    const uint32_t kn = k + gridDim.x;
+    uint32_t nbase = 0, nts = ~0u;
+    uint2 nij = make_uint2(0, 0);
+    if (kn < ntl) {
+      nbase = (A.tiles ? A.tiles[kn] : kn) * tile;
+      if (threadIdx.x == 0) {
+        l2_prefetch(A.b_par + nbase, tile * sizeof(V4));
+        l2_prefetch(A.b_s0 + nbase, tile * sizeof(V4));
+        l2_prefetch(A.b_s1 + nbase, tile * sizeof(V4));
+        l2_prefetch(A.b_s2 + nbase, tile * sizeof(V4));
+      }
+      if (A.tile_s) nts = __ldg(A.tile_s + nbase / tile);
+      if (nbase + threadIdx.x < nb) nij = __ldcs(A.b_ij + nbase + threadIdx.x);
     }
     const uint32_t b = base + threadIdx.x;
-    const uint32_t ts = A.tile_s ? __ldg(A.tile_s + base / tile) : ~0u;
     if (b < nb)
-      do_bond<Real>(A, b, __ldcs(A.b_ij + b), ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b),
-                    ld4_cs(A.b_s2 + b), ts);
+      do_bond<Real>(A, b, ij, ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b), ld4_cs(A.b_s2 + b), ts);
+    base = nbase;
+    ts = nts;
+    ij = nij;
   }
   const uint32_t nc = *A.nc;
   for (uint32_t c = blockIdx.x * tile + threadIdx.x; c < nc; c += stride) do_contact<Real>(A, c);

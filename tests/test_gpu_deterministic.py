@@ -8,8 +8,8 @@ resolution; FP64 and the sensitivity build: 2^-50, in place).
     context), which the float-atomic mode does not give;
   * one step's forces match the oracle and the reference kernels as in the
     float-atomic mode (test_gpu_parity.py runs its step cases in both modes);
-  * whole loading tests agree with the float-atomic mode within the latter's
-    own run-to-run scatter (UCS 10%, E and nu 3%);
+  * whole loading tests agree with the float-atomic mode: within the range
+    of three float-atomic runs widened by 10% (UCS) or 3% (E, nu);
   * FP64 runs and sensitivity runs (values and derivatives) repeat exactly;
   * a run that starts with the launch-schedule autotuner equals one that does
     not;
@@ -70,11 +70,16 @@ def test_deterministic_mode_agrees_with_float_atomics():
     J = S.UniaxialSolver(n=2000, seed=5)
     P = _params(4)
     d = _run(J, P, det=True)
-    f = _run(J, P, det=False)
-    for (rd, _), (rf, _) in zip(d, f):
-        assert rd["FractureStress"] == pytest.approx(rf["FractureStress"], rel=0.10)
-        assert rd["E_chord"] == pytest.approx(rf["E_chord"], rel=0.03)
-        assert rd["nu"] == pytest.approx(rf["nu"], rel=0.03, abs=2e-3)
+    # float-atomic runs differ from one another (summation order): on this
+    # 2,000-sphere specimen the UCS of one case spans about 12% over five runs.
+    # The deterministic value must lie within the range of three float runs,
+    # widened by the stated margin.
+    fs = [_run(J, P, det=False) for _ in range(3)]
+    for i, (rd, _) in enumerate(d):
+        for key, rel, ab in (("FractureStress", 0.10, 0.0), ("E_chord", 0.03, 0.0), ("nu", 0.03, 2e-3)):
+            vals = [f[i][0][key] for f in fs]
+            m = float(np.mean(vals))
+            assert min(vals) - rel * m - ab <= rd[key] <= max(vals) + rel * m + ab, (i, key, rd[key], vals)
 
 
 def test_fp64_and_sensitivity_runs_repeat_exactly():

@@ -316,13 +316,24 @@ def run_sweep(args, ws, rank, local):
     sw = sweep.build_sweep(args.cases, sweep_sizes(16, 11 + rank), seed=1 + rank, device=local)
     n = sw.particles
     dem = importlib.import_module("dem-rock-calibration_b200")
-    ctx = dem.Context(device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks)
+    # launch schedule and contact-list skin chosen by the engine's autotuner on
+    # a scratch context of the same cases (its tuning steps advance that run),
+    # then applied to a fresh context, so the timed steps start from set-up
+    tune = None
+    if args.pair_min_blocks == 0:
+        scratch = dem.Context(device=local, graph_steps=200, skin_factor=args.skin)
+        for c in sw.cases:
+            scratch.add_sample(c.material, c.loading, c.xyz, c.radii)
+        scratch.setup()
+        tune = scratch.autotune(max(20, min(args.steps, 100)))
+        scratch.close()
+    ctx = dem.Context(device=local, graph_steps=200,
+                      pair_min_blocks=tune["pair_min_blocks"] if tune else args.pair_min_blocks,
+                      particle_block=tune["particle_block"] if tune else 0,
+                      skin_factor=tune["skin_factor"] if tune else args.skin)
     for c in sw.cases:
         ctx.add_sample(c.material, c.loading, c.xyz, c.radii)
     ctx.setup()
-    # launch schedules chosen by the engine's autotuner on this workload (the
-    # tuning steps advance the run like any other steps)
-    tune = ctx.autotune(max(20, min(args.steps, 100))) if args.pair_min_blocks == 0 else None
     ctx.run_timed(args.warmup)
     D.barrier()
     clk = Clocks(local)

@@ -104,7 +104,9 @@ class Result(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [("candidates", C.c_int), ("pair_min_blocks", C.c_uint32 * 16), ("particle_block", C.c_uint32 * 16),
                 ("ms_per_step", C.c_double * 16), ("chosen_pair_min_blocks", C.c_uint32),
-                ("chosen_particle_block", C.c_uint32), ("chosen_ms_per_step", C.c_double)]
+                ("chosen_particle_block", C.c_uint32), ("chosen_ms_per_step", C.c_double),
+                ("skin_candidates", C.c_int), ("skin_factor", C.c_double * 8), ("skin_ms_per_step", C.c_double * 8),
+                ("skin_rebuild_ms", C.c_double * 8), ("chosen_skin_factor", C.c_double)]
 
 
 _LIB = None
@@ -435,14 +437,18 @@ class Context:
         return ms.value
 
     def autotune(self, steps: int = 200) -> dict:
-        """Times the launch-schedule candidates on the next steps of this run
-        (steps per candidate; the simulation advances) and keeps the fastest."""
+        """Times the launch-schedule candidates and then the contact-list skins
+        on the next steps of this run (steps per candidate; the simulation
+        advances) and keeps the fastest."""
         r = TuneReport()
         _ck(_lib().dem_autotune(self._h, steps, C.byref(r)), "dem_autotune")
         n = r.candidates
         return dict(candidates=[(r.pair_min_blocks[k], r.particle_block[k], r.ms_per_step[k]) for k in range(n)],
                     pair_min_blocks=r.chosen_pair_min_blocks, particle_block=r.chosen_particle_block,
-                    ms_per_step=r.chosen_ms_per_step)
+                    ms_per_step=r.chosen_ms_per_step,
+                    skins=[(r.skin_factor[k], r.skin_ms_per_step[k], r.skin_rebuild_ms[k])
+                           for k in range(r.skin_candidates)],
+                    skin_factor=r.chosen_skin_factor)
 
     def profile(self, nsteps: int) -> dict:
         a, b, t = C.c_double(), C.c_double(), C.c_double()

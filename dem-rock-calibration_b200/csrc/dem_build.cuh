@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
           const uint32_t c = g.off + (uint32_t)cx + (uint32_t)cy * g.nx + (uint32_t)cz * g.ny * g.nx;
           for (uint32_t k = S.cell_start[c], e = S.cell_start[c + 1]; k < e; ++k) {
             const uint32_t j = S.cell_list[k];
+            if (S.mode != kModeRefSet && j <= i) continue;   // each pair once, from its lower index
             const auto xj = ld4(S.pos + j);
             if (at_hidden(g, xj) || !pair_pred<Real>(S, i, j, xi, xj, s)) continue;
             if (kFill && n < kMax && n < S.cap) buf[n] = j;

@@ -141,7 +141,8 @@ class Engine final : public EngineBase {
     RC(set_pair_config(opt_.pair_min_blocks));
     if (!opt_.particle_block) opt_.particle_block = 256;
     if (!opt_.graph_steps) opt_.graph_steps = 100;
-    if (!(opt_.skin_factor > 0)) opt_.skin_factor = 0.1;
+    skin_user_ = opt_.skin_factor > 0;
+    if (!skin_user_) opt_.skin_factor = 0.1;
     return DEM_OK;
   }
 
@@ -966,7 +967,64 @@ class Engine final : public EngineBase {
     rep->chosen_particle_block = bq;
     rep->chosen_ms_per_step = best / steps;
     opt_.particle_block = bq;
-    return set_pair_config(bp);
+    RC(set_pair_config(bp));
+    rep->chosen_skin_factor = opt_.skin_factor;
+    if (skin_user_) return DEM_OK;
+    // Contact-list skin.  A thin skin lists fewer separated pairs but must be
+    // rebuilt sooner (once a sphere has moved a quarter of it).  Each
+    // candidate runs 4 x `steps` steps with its rebuilds included, in two
+    // passes of 2 x `steps` (thin to thick, then thick to thin, so that a
+    // drift of the run's speed over the tuning charges all candidates alike);
+    // the list is rebuilt at the candidate's skin before each pass (that
+    // rebuild timed on its own and reported).
+    static constexpr double kSkins[4] = {0.1, 0.2, 0.3, 0.4};
+    double tot[4] = {0, 0, 0, 0};
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < 4; ++q) {
+        const int c = pass ? 3 - q : q;
+        float t_reb = 0.f;
+        RC(set_skin(kSkins[c], &t_reb));
+        if (pass == 0) rep->skin_rebuild_ms[c] = t_reb;
+        double ms = 0.0;
+        RC(run_timed(2 * (uint64_t)steps, &ms));
+        tot[c] += ms;
+      }
+    int bs = 0;
+    for (int c = 0; c < 4; ++c) {
+      rep->skin_factor[c] = kSkins[c];
+      rep->skin_ms_per_step[c] = tot[c] / (4.0 * steps);
+      if (tot[c] < tot[bs]) bs = c;
+    }
+    rep->skin_candidates = 4;
+    rep->chosen_skin_factor = kSkins[bs];
+    return set_skin(kSkins[bs], nullptr);
+  }
+
+  // Contact-list skin after set-up: new cell grids (their edge grows with the
+  // skin), per-sample skin parameters, and a list rebuild at the new skin
+  // (tangential histories carried over as in any rebuild).
+  int set_skin(double factor, float* rebuild_ms) {
+    if (!setup_done_ || !(factor > 0)) return DEM_ERR_ARG;
+    opt_.skin_factor = factor;
+    RC(make_grids());
+    RC(upload_params());
+    min_skin_ = 1e300;
+    for (auto& s : samples_) min_skin_ = std::min(min_skin_, factor * s.rmin);
+    invalidate_graph();
+    Flags f{};
+    RC(read_flags(f));
+    cudaEvent_t ea, eb;
+    CK(cudaEventCreate(&ea));
+    CK(cudaEventCreate(&eb));
+    CK(cudaEventRecord(ea, stream_));
+    const int rc = build_contacts(false);
+    CK(cudaEventRecord(eb, stream_));
+    CK(cudaEventSynchronize(eb));
+    if (rebuild_ms) CK(cudaEventElapsedTime(rebuild_ms, ea, eb));
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+    RC(rc);
+    return clear_rebuild_flags();
   }
 
   static const void* pair_kernel_ptr(uint32_t min_blocks) {
@@ -1695,6 +1753,7 @@ class Engine final : public EngineBase {
   bool tiles_on_ = false;
   uint32_t ndone_seen_ = 0;
   bool user_grid_ = false;
+  bool skin_user_ = false;  // skin_factor given at creation: the autotuner keeps it
   uint32_t part_occ_ = 8, part_occ_block_ = 0;
   bool det_ = false;
   DBuf<Real> mass_;

@@ -235,7 +235,11 @@ int dem_profile(dem_ctx* ctx, uint32_t nsteps, double* pair_ms, double* particle
  * steps: the state moves on as under dem_run), times each with CUDA events
  * and keeps the fastest for the rest of the context's life.  Candidates: the
  * pair kernel's register budget / block size (dem_options.pair_min_blocks)
- * crossed with particle-kernel blocks of 128 and 256 threads. */
+ * crossed with particle-kernel blocks of 128 and 256 threads; then the
+ * contact-list skin (dem_options.skin_factor 0.1, 0.2, 0.3, 0.4; only when
+ * the context was created with skin_factor 0), each run for 4 x `steps`
+ * steps with its list rebuilds included (two passes in opposite orders).
+ * The skin changes only which separated pairs are listed, not the forces. */
 #define DEM_TUNE_MAX 16
 typedef struct {
   int candidates;
@@ -244,6 +248,11 @@ typedef struct {
   double ms_per_step[DEM_TUNE_MAX];
   uint32_t chosen_pair_min_blocks, chosen_particle_block;
   double chosen_ms_per_step;
+  int skin_candidates;
+  double skin_factor[8];
+  double skin_ms_per_step[8];    /* measured step time at that skin, list rebuilds included */
+  double skin_rebuild_ms[8];     /* one contact-list rebuild at that skin */
+  double chosen_skin_factor;
 } dem_tune_report;
 int dem_autotune(dem_ctx* ctx, uint32_t steps, dem_tune_report* report);
 

@@ -106,7 +106,8 @@ def test_fp64_and_sensitivity_runs_repeat_exactly():
 
 
 def test_autotuned_run_equals_plain_run():
-    """The autotuner's steps are ordinary steps of the run: in deterministic
+    """The autotuner's steps are ordinary steps of the run and the skin it
+    picks changes only which separated pairs are listed: in deterministic
     mode a run that starts with an autotune gives bit-identical results to
     one that does not, and the tuner reports its timed candidates."""
     J = S.UniaxialSolver(n=2000, seed=5)
@@ -125,11 +126,27 @@ def test_autotuned_run_equals_plain_run():
             t = ctx.autotune(40)
             assert len(t["candidates"]) >= 4 and t["ms_per_step"] > 0
             assert (t["pair_min_blocks"], t["particle_block"]) in [(c[0], c[1]) for c in t["candidates"]]
+            assert [s[0] for s in t["skins"]] == [0.1, 0.2, 0.3, 0.4]
+            assert t["skin_factor"] in (0.1, 0.2, 0.3, 0.4) and all(s[1] > 0 and s[2] > 0 for s in t["skins"])
         ctx.run(400000)
         res.append([ctx.result(i) for i in range(len(P))])
         ctx.close()
     for ra, rb in zip(*res):
         assert all(ra[k] == rb[k] for k in KEYS)
+
+
+def test_autotuner_keeps_a_skin_set_at_creation():
+    J = S.UniaxialSolver(n=1000, seed=5)
+    r_min, r_mean = float(J.rad.min()), float(J.rad.mean())
+    ctx = dem.Context(skin_factor=0.25)
+    ld = dem.loading(dem.TEST_UNIAXIAL, J.box, J.size_real, J.center_real, velocity=-0.1 / dem.VELOCITY,
+                     min_stress=0.010, max_strain=0.01, cond_fracture=0.7, dNsave=100, max_steps=400000,
+                     p_r_platen=r_mean)
+    ctx.add_sample(sweep.material_for(dict(zip(J.keys, _params(1)[0])), r_min, r_mean, 7), ld, J.xyz, J.rad)
+    ctx.setup()
+    t = ctx.autotune(20)
+    assert t["skins"] == [] and t["skin_factor"] == 0.25
+    ctx.close()
 
 
 def test_seeded_packing_repeats_exactly():

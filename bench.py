@@ -46,7 +46,7 @@ METRIC = "BPM particle-steps/s"
 UNIT = "particle-steps/s"
 # DRAM bytes (read + write) of one k_pairs launch on the default workload (two
 # 245,098-sphere Brazilian discs), ncu --set full early in the loading
-PAIR_TRAFFIC_DISC_X2 = 198.6e6
+PAIR_TRAFFIC_DISC_X2 = 193.8e6
 
 
 def dist_env():

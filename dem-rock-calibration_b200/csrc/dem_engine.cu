@@ -209,6 +209,7 @@ class Engine final : public EngineBase {
       CK(momq_.alloc(4 * (size_t)np_));
     }
     CK(wallO_.alloc(np_));
+    CK(wflag_.alloc(np_));
     CK(pos_ref_.alloc(np_));
     CK(mass_.alloc(np_));
     CK(sid_.alloc(np_));
@@ -231,7 +232,6 @@ class Engine final : public EngineBase {
     RC(init_controllers());
     CK(blocks_done_.alloc(1));
     if (DualK<Real>::K) CK(sfl_tan_.alloc((size_t)S * (4 * DualK<Real>::K + 2)));
-    CK(blk_stat_.alloc(2 * (size_t)num_sms_ * 8 + 64));
     CK(stat_.alloc(2));
     min_skin_ = 1e300;
     max_dt_ = 0;
@@ -870,6 +870,7 @@ class Engine final : public EngineBase {
     A.frc = frc_.p;
     A.mom = mom_.p;
     A.wallO = wallO_.p;
+    A.wflag = wflag_.p;
     A.pos_ref = pos_ref_.p;
     A.mass = mass_.p;
     A.sid = sid_.p;
@@ -889,7 +890,6 @@ class Engine final : public EngineBase {
     A.blocks_done = blocks_done_.p;
     A.keep_forces = 0;
     A.touching = nullptr;
-    A.blk_stat = blk_stat_.p;
     A.stat = stat_.p;
     A.lat = lat_.p;
     A.sfl_tan = sfl_tan_.p;
@@ -1053,7 +1053,7 @@ class Engine final : public EngineBase {
   }
 
   // Particle kernel grid: the blocks that are resident at once (a grid-stride
-  // loop covers the rest), at most 8 per SM (the block-statistics buffer).
+  // loop covers the rest), at most 8 per SM.
   uint32_t particle_grid() {
     if (part_occ_block_ != opt_.particle_block) {
       int occ = 0;
@@ -1435,6 +1435,13 @@ class Engine final : public EngineBase {
     RC(put(vel_, V));
     RC(put(omg_, W));
     RC(put(wallO_, O));
+    if (O) {
+      // platen-history flags of the sample: set where the uploaded history is non-zero
+      std::vector<uint8_t> fl(s.n);
+      for (uint32_t k = 0; k < s.n; ++k)
+        fl[k] = (O[s.perm[k]] != 0.f || O[s.n + s.perm[k]] != 0.f || O[2 * s.n + s.perm[k]] != 0.f) ? 1 : 0;
+      CK(cudaMemcpy(wflag_.p + s.p_begin, fl.data(), s.n, cudaMemcpyHostToDevice));
+    }
     if (R) contacts_dirty_ = true;
     return DEM_OK;
   }
@@ -1746,6 +1753,7 @@ class Engine final : public EngineBase {
   uint32_t np_ = 0, nb_ = 0, nc_host_ = 0, ncell_ = 0;
 
   DBuf<V4> pos_, vel_, omg_, frc_, mom_, wallO_, pos_ref_;
+  DBuf<uint8_t> wflag_;
   DBuf<long long> frcq_, momq_;   // deterministic mode: fixed-point accumulators
   std::vector<uint32_t> sb_begin_, sb_end_;   // per sample: bond range
   DBuf<uint32_t> tiles_, ntiles_, sdone_;     // active bond tiles; per-sample finished flags
@@ -1771,7 +1779,7 @@ class Engine final : public EngineBase {
   DBuf<Grid<Real>> grids_;
   DBuf<uint32_t> cell_of_, cell_count_, cell_start_, cell_cursor_, cell_list_, cnt_, offs_, ovf_, scan_tmp_;
   DBuf<unsigned int> blocks_done_;
-  DBuf<float> blk_stat_, stat_;
+  DBuf<float> stat_;
   std::vector<std::unique_ptr<DBuf<double>>> rec_;
   std::vector<std::unique_ptr<DBuf<uint32_t>>> rec_bonds_;
   std::vector<std::unique_ptr<DBuf<double>>> rec_lat_;

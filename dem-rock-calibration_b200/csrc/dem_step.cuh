@@ -30,6 +30,7 @@ struct StepArgs {
   V4* frc;
   V4* mom;
   V4* wallO;
+  uint8_t* wflag;  // per particle: 1 = wallO may be non-zero (it touched the lower platen last step)
   V4* pos_ref;
   const Real* mass;
   const uint32_t* sid;
@@ -52,8 +53,7 @@ struct StepArgs {
   unsigned int* blocks_done;
   int keep_forces;  // 1: leave the step's total force/moment in frc/mom (parity checks)
   unsigned long long* touching;  // non-null: count touching contacts (algorithmic-byte accounting)
-  float* blk_stat;  // per block: max |v|^2 and max displacement^2 since the last list build
-  float* stat;      // running maxima over blocks and steps (reset by the host)
+  float* stat;      // running maxima of |v|^2 and displacement^2 over blocks and steps (reset by the host)
   const uint8_t* lat;  // per particle: 1 = on the lateral surface near mid-height (or null)
   double* sfl_tan;     // sensitivity build only: per sample the platen-force tangents (see dem_dual.cuh)
   // deterministic mode (FP32 only): fixed-point force and moment accumulators,
@@ -701,26 +701,37 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
           r[2] = x.z - Real(sp.wall_c[2]);
         }
         const Real lat = (ax == 2) ? (r[0] * r[0] + r[1] * r[1]) : (r[0] * r[0] + r[2] * r[2]);
+        // The history ends zero unless the sphere touches the lower platen (the
+        // branch of the platen it does not touch clears it), so a sphere of the
+        // platen zone that touches neither platen and had no history keeps a zero
+        // one: nothing to read or write.
         if (lat < Real(sp.wall_RR) && r[2] < Real(sp.zcut)) {
-          const Real wtop = Real((float)C.Top), wbot = Real((float)C.Bottom), wvel = Real((float)C.V);
-          V4 o4 = A.wallO[p];
-          Real o[3] = {o4.x, o4.y, o4.z};
-          const Real ri = x.w, mi = A.mass[p];
-          if (wtop - r[ax] < ri) {
-            const Real f = wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
-            st = -(double)f;
-            tangent_wall(A, s, 1, f);
-          } else {
-            o[0] = o[1] = o[2] = Real(0);
+          const Real wtop = Real((float)C.Top), wbot = Real((float)C.Bottom);
+          const bool top = wtop - r[ax] < x.w, bot = r[ax] - wbot < x.w;
+          const uint8_t had = A.wflag[p];
+          if (top || bot || had) {
+            const Real wvel = Real((float)C.V);
+            V4 o4 = had ? A.wallO[p] : mk4(Real(0), Real(0), Real(0), Real(0));
+            Real o[3] = {o4.x, o4.y, o4.z};
+            const Real ri = x.w, mi = A.mass[p];
+            if (top) {
+              const Real f = wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
+              st = -(double)f;
+              tangent_wall(A, s, 1, f);
+            } else {
+              o[0] = o[1] = o[2] = Real(0);
+            }
+            if (bot) {
+              const Real f =
+                  wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
+              sb = -(double)f;
+              tangent_wall(A, s, 0, f);
+            } else {
+              o[0] = o[1] = o[2] = Real(0);
+            }
+            A.wallO[p] = mk4(o[0], o[1], o[2], Real(0));
+            if (had != (uint8_t)bot) A.wflag[p] = bot ? 1 : 0;
           }
-          if (r[ax] - wbot < ri) {
-            const Real f = wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
-            sb = -(double)f;
-            tangent_wall(A, s, 0, f);
-          } else {
-            o[0] = o[1] = o[2] = Real(0);
-          }
-          A.wallO[p] = mk4(o[0], o[1], o[2], Real(0));
         }
       }
       // d_CalculateIncrementsDEM: v += F dt/m, x += v dt, w += M dt/I
@@ -854,8 +865,10 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
       a = fmaxf(a, s_v2[w]);
       b = fmaxf(b, s_d2[w]);
     }
-    A.blk_stat[2 * blockIdx.x] = a;
-    A.blk_stat[2 * blockIdx.x + 1] = b;
+    // running maxima since the host last reset them (non-negative floats order
+    // as their bit patterns)
+    atomicMax(reinterpret_cast<int*>(A.stat), __float_as_int(a));
+    atomicMax(reinterpret_cast<int*>(A.stat) + 1, __float_as_int(b));
   }
   // the last block to finish runs the controllers
   __threadfence();
@@ -876,32 +889,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
       controller_step(C);
     }
   }
-  float a = 0.f, b = 0.f;
-  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
-    a = fmaxf(a, __ldcg(A.blk_stat + 2 * k));
-    b = fmaxf(b, __ldcg(A.blk_stat + 2 * k + 1));
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    a = fmaxf(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
-    b = fmaxf(b, __shfl_xor_sync(0xFFFFFFFFu, b, o));
-  }
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-    s_v2[threadIdx.x >> 5] = a;
-    s_d2[threadIdx.x >> 5] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    a = A.stat[0];
-    b = A.stat[1];
-    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; ++w) {
-      a = fmaxf(a, s_v2[w]);
-      b = fmaxf(b, s_d2[w]);
-    }
-    A.stat[0] = a;
-    A.stat[1] = b;
-    *A.blocks_done = 0;
-  }
+  if (threadIdx.x == 0) *A.blocks_done = 0;
 }
 
 }  // namespace dem

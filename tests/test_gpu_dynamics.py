@@ -147,11 +147,14 @@ def test_uniaxial_elastic_record_matches_reference_driver(tmp_path, seed):
 def test_uniaxial_peak_statistics_match_reference_driver(tmp_path):
     """Breakable bonds (40 MPa) loaded past the peak (stop at 70% of it).  Bond
     breakage makes single runs chaotic: the engine's own repeated runs spread
-    by +-5% in peak stress and +-2% in chord modulus.  Compared are the means
-    over three specimens (reference once, engine three times each): peak
-    stress (UCS) within 8%, strain at peak within 8%, chord modulus within 3%,
-    and the engine's chord modulus from its own post-processing equal to the
-    one computed here from its record."""
+    by +-5% in peak stress and strain at peak and +-2% in chord modulus, and
+    one reference run per specimen is one draw of the same kind.  Compared
+    are the means over three specimens (reference once, engine three times
+    each), whose difference has a standard deviation of about
+    5% x sqrt(1/3 + 1/9) = 3.3% in UCS and strain: peak stress and strain at
+    peak within 10% (3 sigma), chord modulus within 3%, and the engine's chord
+    modulus from its own post-processing equal to the one computed here from
+    its record."""
     ucs_r, eps_r, E_r, ucs_m, eps_m, E_m = [], [], [], [], [], []
     for seed in (1, 2, 3):
         out, ref_rec, mine = _both_drivers(tmp_path / f"s{seed}", seed, 40e6, 40e6, 0.01, 0.7, runs=3)
@@ -165,8 +168,8 @@ def test_uniaxial_peak_statistics_match_reference_driver(tmp_path):
             assert res["E_chord"] == pytest.approx(_chord(rec), rel=1e-9)
             assert 0.0 < res["nu"] < 0.5
     m = {k: (np.mean(a), np.mean(b)) for k, a, b in (("ucs", ucs_m, ucs_r), ("eps", eps_m, eps_r), ("E", E_m, E_r))}
-    assert abs(m["ucs"][0] - m["ucs"][1]) <= 0.08 * m["ucs"][1], m
-    assert abs(m["eps"][0] - m["eps"][1]) <= 0.08 * m["eps"][1], m
+    assert abs(m["ucs"][0] - m["ucs"][1]) <= 0.10 * m["ucs"][1], m
+    assert abs(m["eps"][0] - m["eps"][1]) <= 0.10 * m["eps"][1], m
     assert abs(m["E"][0] - m["E"][1]) <= 0.03 * m["E"][1], m
 
 

@@ -112,8 +112,9 @@ __device__ __forceinline__ void acc3q(long long* q, float x, float y, float z) {
 // double is a zero integer, so the accumulators reset as before).
 constexpr double kFixScaleD = 1125899906842624.0;    // 2^50
 constexpr double kFixInvD = 1.0 / 1125899906842624.0;
+__device__ __forceinline__ long long fix_of(double x) { return __double2ll_rn(x * kFixScaleD); }
 __device__ __forceinline__ void fix_add(double* slot, double x) {
-  atomicAdd(reinterpret_cast<unsigned long long*>(slot), (unsigned long long)__double2ll_rn(x * kFixScaleD));
+  atomicAdd(reinterpret_cast<unsigned long long*>(slot), (unsigned long long)fix_of(x));
 }
 __device__ __forceinline__ double fix_val(double slot) { return (double)__double_as_longlong(slot) * kFixInvD; }
 __device__ __forceinline__ void acc3(double4* p, double x, double y, double z) {

@@ -228,34 +228,75 @@ __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i
   if (!dropJ) acc_m(A, j, mJ[0], mJ[1], mJ[2]);
 }
 
-// The i-side force and moment of an intact bond.  FP32 float atomics: bonds
-// are stored sorted by i, so the lanes of a warp that share i are adjacent;
-// when the whole warp is here their contributions are first summed over each
-// run of equal i (a segmented suffix sum by shuffles) and the run's first lane
-// issues the two reductions, which cuts the vector reductions reaching L2 by
-// about a third.  Otherwise (deterministic mode, FP64, a partial warp) every
-// lane adds its own.
+// Sum of v over the run of lanes of this warp that share key (keys sorted
+// along the lanes, all 32 lanes active): a segmented suffix sum by shuffles;
+// the run's first lane ends with the run's total.
+template <class T, int N>
+__device__ __forceinline__ void warp_run_sum(uint32_t key, T (&v)[N]) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (uint32_t d = 1; d < 32; d <<= 1) {
+    const uint32_t ko = __shfl_down_sync(0xFFFFFFFFu, key, d);
+    const bool same = lane + d < 32 && ko == key;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const T o = __shfl_down_sync(0xFFFFFFFFu, v[k], d);
+      if (same) v[k] += o;
+    }
+  }
+}
+
+// The i-side force and moment of an intact bond.  Bonds are stored sorted by
+// i, so the lanes of a warp that share i are adjacent: when the whole warp is
+// here their contributions are first summed over each run of equal i and the
+// run's first lane issues the atomics, which cuts the atomics reaching L2 by
+// about a third (float) or a half (fixed point, three per vector).  In
+// deterministic mode every lane's contribution is first rounded to fixed point
+// and the run is summed as integers, so the sum is the same exact value the
+// per-lane fixed-point atomics give.  Otherwise (a partial warp, the
+// sensitivity build) every lane adds its own.
 template <class Real>
 __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t i, Real f0, Real f1, Real f2,
                                                Real m0, Real m1, Real m2) {
-  if constexpr (sizeof(Real) == 4) {
-    if (!A.det && __activemask() == 0xFFFFFFFFu) {
+  if constexpr (sizeof(Real) == 4 || sizeof(Real) == 8) {
+    if (__activemask() == 0xFFFFFFFFu) {
       const uint32_t lane = threadIdx.x & 31;
-      float v[6] = {f0, f1, f2, m0, m1, m2};
-#pragma unroll
-      for (uint32_t d = 1; d < 32; d <<= 1) {
-        const uint32_t io = __shfl_down_sync(0xFFFFFFFFu, i, d);
-        const bool same = lane + d < 32 && io == i;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          const float o = __shfl_down_sync(0xFFFFFFFFu, v[k], d);
-          if (same) v[k] += o;
-        }
-      }
+      // every lane takes part in the shuffle (no short-circuit around it)
       const uint32_t iu = __shfl_up_sync(0xFFFFFFFFu, i, 1);
-      if (lane == 0 || iu != i) {
-        acc3(A.frc + i, v[0], v[1], v[2]);
-        acc3(A.mom + i, v[3], v[4], v[5]);
+      const bool head = lane == 0 || iu != i;
+      if (A.det) {
+        long long q[6];
+        if constexpr (sizeof(Real) == 4) {
+          q[0] = to_fix(f0); q[1] = to_fix(f1); q[2] = to_fix(f2);
+          q[3] = to_fix(m0); q[4] = to_fix(m1); q[5] = to_fix(m2);
+        } else {
+          q[0] = fix_of(f0); q[1] = fix_of(f1); q[2] = fix_of(f2);
+          q[3] = fix_of(m0); q[4] = fix_of(m1); q[5] = fix_of(m2);
+        }
+        warp_run_sum(i, q);
+        if (head) {
+          unsigned long long* uf;
+          unsigned long long* um;
+          if constexpr (sizeof(Real) == 4) {
+            uf = reinterpret_cast<unsigned long long*>(A.frcq + 4 * (size_t)i);
+            um = reinterpret_cast<unsigned long long*>(A.momq + 4 * (size_t)i);
+          } else {
+            uf = reinterpret_cast<unsigned long long*>(A.frc + i);
+            um = reinterpret_cast<unsigned long long*>(A.mom + i);
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            atomicAdd(uf + k, (unsigned long long)q[k]);
+            atomicAdd(um + k, (unsigned long long)q[3 + k]);
+          }
+        }
+      } else {
+        Real v[6] = {f0, f1, f2, m0, m1, m2};
+        warp_run_sum(i, v);
+        if (head) {
+          acc3(A.frc + i, v[0], v[1], v[2]);
+          acc3(A.mom + i, v[3], v[4], v[5]);
+        }
       }
       return;
     }

@@ -563,7 +563,7 @@ def run_solves(args, ws, rank, local):
     t_b = time.perf_counter() - t0
     clocks = clk.stop()
     t_b = D.max(t_b)
-    k = min(args.cases, 8)
+    k = min(args.cases, 32)
     t0 = time.perf_counter()
     Ys = np.vstack([J(X[i:i + 1]) for i in range(k)])
     t_s = time.perf_counter() - t0

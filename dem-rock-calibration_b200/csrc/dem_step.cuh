@@ -919,16 +919,18 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
   if (!s_last) return;
   __threadfence();
   for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
-    SampleCtl& C = A.ctl[s];
-    if (!C.done) {
-      // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
-      C.sFL[0] += (double)C.sFLq[0] * kFixInv;
-      C.sFL[1] += (double)C.sFLq[1] * kFixInv;
-      C.lat_sum += (double)C.lat_q * kFixInv;
-      C.sFLq[0] = C.sFLq[1] = C.lat_q = 0;
-      tangent_step_end(A, C, s);
-      controller_step(C);
-    }
+    if (A.ctl[s].done) continue;
+    // the controller works on a private copy (one load of the state, one store
+    // back) instead of a chain of dependent global reads and writes
+    SampleCtl C = A.ctl[s];
+    // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
+    C.sFL[0] += (double)C.sFLq[0] * kFixInv;
+    C.sFL[1] += (double)C.sFLq[1] * kFixInv;
+    C.lat_sum += (double)C.lat_q * kFixInv;
+    C.sFLq[0] = C.sFLq[1] = C.lat_q = 0;
+    tangent_step_end(A, C, s);
+    controller_step(C);
+    A.ctl[s] = C;
   }
   if (threadIdx.x == 0) *A.blocks_done = 0;
 }

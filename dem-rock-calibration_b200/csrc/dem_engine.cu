@@ -911,7 +911,7 @@ class Engine final : public EngineBase {
       min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 7 : 2);
     opt_.pair_min_blocks = min_blocks;
     opt_.pair_block = min_blocks > 4 ? 128 : 256;
-    pair_kernel_ = pair_kernel_ptr(min_blocks);
+    pair_kernel_ = pair_kernel_ptr(min_blocks, det_);
     if (!user_grid_) {
       int per_sm = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel_, (int)opt_.pair_block, 0));
@@ -1027,8 +1027,22 @@ class Engine final : public EngineBase {
     return clear_rebuild_flags();
   }
 
-  static const void* pair_kernel_ptr(uint32_t min_blocks) {
+  // Pair kernel variant for a register budget; deterministic FP32 contexts
+  // get the variants with the warp-summed j-side fixed-point atomics.
+  static const void* pair_kernel_ptr(uint32_t min_blocks, bool det) {
     if constexpr (sizeof(Real) == 4 && !DualK<Real>::K) {
+      if (det) {
+        switch (min_blocks) {
+          case 1: return (const void*)k_pairs<Real, 1, 256, true>;
+          case 2: return (const void*)k_pairs<Real, 2, 256, true>;
+          case 3: return (const void*)k_pairs<Real, 3, 256, true>;
+          case 5: return (const void*)k_pairs<Real, 5, 128, true>;
+          case 6: return (const void*)k_pairs<Real, 6, 128, true>;
+          case 7: return (const void*)k_pairs<Real, 7, 128, true>;
+          case 8: return (const void*)k_pairs<Real, 8, 128, true>;
+          default: return (const void*)k_pairs<Real, 4, 256, true>;
+        }
+      }
       switch (min_blocks) {
         case 5: return (const void*)k_pairs<Real, 5, 128>;
         case 6: return (const void*)k_pairs<Real, 6, 128>;

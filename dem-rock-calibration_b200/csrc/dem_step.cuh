@@ -305,11 +305,61 @@ __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t
   acc_m(A, i, m0, m1, m2);
 }
 
+// The j-side force and moment of an intact bond.  Deterministic FP32 mode with
+// the whole warp here: a contribution costs six 64-bit atomics, so the lanes
+// whose bonds share j (neighbours of nearby i; they need not be adjacent) are
+// found with a warp match and their fixed-point values summed by a shuffle tree
+// over their ranks (integer sums: the same exact total); the lowest of them
+// issues the atomics.  Float atomics cost too little for the match to pay
+// (measured), so every other case adds per lane.  The code is compiled only
+// into the pair kernels of deterministic FP32 contexts (kDetJ): its registers
+// slowed the float kernel by 12%.
+template <class Real, bool kDetJ>
+__device__ __forceinline__ void scatter_j_warp(const StepArgs<Real>& A, uint32_t j, Real f0, Real f1, Real f2,
+                                               Real m0, Real m1, Real m2) {
+  if constexpr (sizeof(Real) == 4 && kDetJ) {
+    if (A.det && __activemask() == 0xFFFFFFFFu) {
+      const uint32_t lane = threadIdx.x & 31;
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, j);
+      const uint32_t n = __popc(peers), r = __popc(peers & ((1u << lane) - 1u));
+      const uint32_t maxn = __reduce_max_sync(0xFFFFFFFFu, n);
+      long long q[6] = {to_fix(f0), to_fix(f1), to_fix(f2), to_fix(m0), to_fix(m1), to_fix(m2)};
+      // rank r adds rank r + s for r = 0 mod 2s; after the rounds rank 0 holds
+      // the sum.  Every lane runs every shuffle (maxn is the same in all lanes).
+      for (uint32_t s = 1; s < maxn; s <<= 1) {
+        uint32_t src = lane;
+        if (r % (2 * s) == 0 && r + s < n) {
+          unsigned above = lane < 31 ? peers & ~((2u << lane) - 1u) : 0u;
+          for (uint32_t t = 1; t < s; ++t) above &= above - 1u;
+          if (above) src = __ffs(above) - 1;
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const long long o = __shfl_sync(0xFFFFFFFFu, q[k], src);
+          if (src != lane) q[k] += o;
+        }
+      }
+      if (r == 0) {
+        unsigned long long* uf = reinterpret_cast<unsigned long long*>(A.frcq + 4 * (size_t)j);
+        unsigned long long* um = reinterpret_cast<unsigned long long*>(A.momq + 4 * (size_t)j);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          atomicAdd(uf + k, (unsigned long long)q[k]);
+          atomicAdd(um + k, (unsigned long long)q[3 + k]);
+        }
+      }
+      return;
+    }
+  }
+  acc_f(A, j, f0, f1, f2);
+  acc_m(A, j, m0, m1, m2);
+}
+
 // One bond (i < j).  The arithmetic is that of d_CalculateForcesDEM_22 for the
 // slot i->j (md_calculateforcesdem3.cu:41-200, 427-486); the slot j->i of the
 // reference is its exact mirror (all vectors negated, the unsymmetric moment
 // equal), so j receives -F, -(Mn + Mt) terms and the same unsymmetric moment.
-template <class Real>
+template <class Real, bool kDetJ>
 __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
                                         typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
                                         typename RT<Real>::V4 s1, typename RT<Real>::V4 s2, uint32_t ts) {
@@ -401,8 +451,8 @@ __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, con
     const Real mu1 = half * (rz * ot0 - rx * ot2) * cef;
     const Real mu2 = half * (rx * ot1 - ry * ot0) * cef;
     // contributions: i gets (F, Mn+Mt+Mu), j gets (-F, -(Mn+Mt)+Mu)
-    acc_f(A, j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2));
-    acc_m(A, j, mu0 - (tn0 + tt0), mu1 - (tn1 + tt1), mu2 - (tn2 + tt2));
+    scatter_j_warp<Real, kDetJ>(A, j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2), mu0 - (tn0 + tt0), mu1 - (tn1 + tt1),
+                         mu2 - (tn2 + tt2));
     scatter_i_warp<Real>(A, i, fn0 + ft0, fn1 + ft1, fn2 + ft2, (tn0 + tt0) + mu0, (tn1 + tt1) + mu1,
                          (tn2 + tt2) + mu2);
     // break test (dd_CheckBreakConditionDEM_2)
@@ -497,7 +547,7 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
 // so the next pass finds its streamed loads in L2, and every thread already
 // holds the next tile's pair indices.  Bond arrays are padded to whole
 // 256-bond tiles.
-template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2), int kBlock = 256>
+template <class Real, int kMinBlocks = (sizeof(Real) == 4 ? 4 : 2), int kBlock = 256, bool kDetJ = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) {
   using V4 = typename RT<Real>::V4;
   const uint32_t nb = A.nb;
@@ -531,7 +581,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) 
     }
     const uint32_t b = base + threadIdx.x;
     if (b < nb)
-      do_bond<Real>(A, b, ij, ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b), ld4_cs(A.b_s2 + b), ts);
+      do_bond<Real, kDetJ>(A, b, ij, ld4_cs(A.b_par + b), ld4_cs(A.b_s0 + b), ld4_cs(A.b_s1 + b), ld4_cs(A.b_s2 + b), ts);
     base = nbase;
     ts = nts;
     ij = nij;

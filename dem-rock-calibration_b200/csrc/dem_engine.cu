@@ -1028,7 +1028,7 @@ class Engine final : public EngineBase {
   }
 
   // Pair kernel variant for a register budget; deterministic FP32 contexts
-  // get the variants with the warp-summed j-side fixed-point atomics.
+  // and FP64 contexts get the variants with the warp-summed j side.
   static const void* pair_kernel_ptr(uint32_t min_blocks, bool det) {
     if constexpr (sizeof(Real) == 4 && !DualK<Real>::K) {
       if (det) {
@@ -1049,6 +1049,14 @@ class Engine final : public EngineBase {
         case 7: return (const void*)k_pairs<Real, 7, 128>;
         case 8: return (const void*)k_pairs<Real, 8, 128>;
         default: break;
+      }
+    }
+    if constexpr (sizeof(Real) == 8) {
+      switch (min_blocks) {
+        case 1: return (const void*)k_pairs<Real, 1, 256, true>;
+        case 2: return (const void*)k_pairs<Real, 2, 256, true>;
+        case 3: return (const void*)k_pairs<Real, 3, 256, true>;
+        default: return (const void*)k_pairs<Real, 4, 256, true>;
       }
     }
     switch (min_blocks) {

@@ -305,47 +305,79 @@ __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t
   acc_m(A, i, m0, m1, m2);
 }
 
-// The j-side force and moment of an intact bond.  Deterministic FP32 mode with
-// the whole warp here: a contribution costs six 64-bit atomics, so the lanes
-// whose bonds share j (neighbours of nearby i; they need not be adjacent) are
-// found with a warp match and their fixed-point values summed by a shuffle tree
-// over their ranks (integer sums: the same exact total); the lowest of them
-// issues the atomics.  Float atomics cost too little for the match to pay
-// (measured), so every other case adds per lane.  The code is compiled only
-// into the pair kernels of deterministic FP32 contexts (kDetJ): its registers
-// slowed the float kernel by 12%.
+// The j-side force and moment of an intact bond.  Deterministic FP32 mode and
+// FP64 with the whole warp here: a contribution costs six 64-bit atomics, so
+// the lanes whose bonds share j (neighbours of nearby i; they need not be
+// adjacent) are found with a warp match and their values summed by a shuffle
+// tree over their ranks (in deterministic mode as fixed-point integers: the
+// same exact total); the lowest of them issues the atomics.  FP32 float
+// atomics cost too little for the match to pay (measured), so every other case
+// adds per lane.  The code is compiled only into the pair kernels of
+// deterministic FP32 and of FP64 contexts (kDetJ): its registers slowed the
+// FP32 float kernel by 12%.
+// Sum of v over the lanes of this warp named in peers (this lane among them,
+// at rank r of n; maxn the largest n in the warp): a shuffle tree over the
+// ranks, rank r adding rank r + s for r = 0 mod 2s, so that rank 0 ends with
+// the sum.  Every lane runs every shuffle (maxn is the same in all lanes).
+template <class T, int N>
+__device__ __forceinline__ void warp_peer_sum(unsigned peers, uint32_t n, uint32_t r, uint32_t maxn, T (&v)[N]) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t s = 1; s < maxn; s <<= 1) {
+    uint32_t src = lane;
+    if (r % (2 * s) == 0 && r + s < n) {
+      unsigned above = lane < 31 ? peers & ~((2u << lane) - 1u) : 0u;
+      for (uint32_t t = 1; t < s; ++t) above &= above - 1u;
+      if (above) src = __ffs(above) - 1;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const T o = __shfl_sync(0xFFFFFFFFu, v[k], src);
+      if (src != lane) v[k] += o;
+    }
+  }
+}
+
 template <class Real, bool kDetJ>
 __device__ __forceinline__ void scatter_j_warp(const StepArgs<Real>& A, uint32_t j, Real f0, Real f1, Real f2,
                                                Real m0, Real m1, Real m2) {
-  if constexpr (sizeof(Real) == 4 && kDetJ) {
-    if (A.det && __activemask() == 0xFFFFFFFFu) {
+  if constexpr ((sizeof(Real) == 4 || sizeof(Real) == 8) && kDetJ) {
+    if ((sizeof(Real) == 8 || A.det) && __activemask() == 0xFFFFFFFFu) {
       const uint32_t lane = threadIdx.x & 31;
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, j);
       const uint32_t n = __popc(peers), r = __popc(peers & ((1u << lane) - 1u));
       const uint32_t maxn = __reduce_max_sync(0xFFFFFFFFu, n);
-      long long q[6] = {to_fix(f0), to_fix(f1), to_fix(f2), to_fix(m0), to_fix(m1), to_fix(m2)};
-      // rank r adds rank r + s for r = 0 mod 2s; after the rounds rank 0 holds
-      // the sum.  Every lane runs every shuffle (maxn is the same in all lanes).
-      for (uint32_t s = 1; s < maxn; s <<= 1) {
-        uint32_t src = lane;
-        if (r % (2 * s) == 0 && r + s < n) {
-          unsigned above = lane < 31 ? peers & ~((2u << lane) - 1u) : 0u;
-          for (uint32_t t = 1; t < s; ++t) above &= above - 1u;
-          if (above) src = __ffs(above) - 1;
+      if (A.det) {
+        long long q[6];
+        if constexpr (sizeof(Real) == 4) {
+          q[0] = to_fix(f0); q[1] = to_fix(f1); q[2] = to_fix(f2);
+          q[3] = to_fix(m0); q[4] = to_fix(m1); q[5] = to_fix(m2);
+        } else {
+          q[0] = fix_of(f0); q[1] = fix_of(f1); q[2] = fix_of(f2);
+          q[3] = fix_of(m0); q[4] = fix_of(m1); q[5] = fix_of(m2);
         }
+        warp_peer_sum(peers, n, r, maxn, q);
+        if (r == 0) {
+          unsigned long long* uf;
+          unsigned long long* um;
+          if constexpr (sizeof(Real) == 4) {
+            uf = reinterpret_cast<unsigned long long*>(A.frcq + 4 * (size_t)j);
+            um = reinterpret_cast<unsigned long long*>(A.momq + 4 * (size_t)j);
+          } else {
+            uf = reinterpret_cast<unsigned long long*>(A.frc + j);
+            um = reinterpret_cast<unsigned long long*>(A.mom + j);
+          }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          const long long o = __shfl_sync(0xFFFFFFFFu, q[k], src);
-          if (src != lane) q[k] += o;
+          for (int k = 0; k < 3; ++k) {
+            atomicAdd(uf + k, (unsigned long long)q[k]);
+            atomicAdd(um + k, (unsigned long long)q[3 + k]);
+          }
         }
-      }
-      if (r == 0) {
-        unsigned long long* uf = reinterpret_cast<unsigned long long*>(A.frcq + 4 * (size_t)j);
-        unsigned long long* um = reinterpret_cast<unsigned long long*>(A.momq + 4 * (size_t)j);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          atomicAdd(uf + k, (unsigned long long)q[k]);
-          atomicAdd(um + k, (unsigned long long)q[3 + k]);
+      } else {
+        Real v[6] = {f0, f1, f2, m0, m1, m2};
+        warp_peer_sum(peers, n, r, maxn, v);
+        if (r == 0) {
+          acc3(A.frc + j, v[0], v[1], v[2]);
+          acc3(A.mom + j, v[3], v[4], v[5]);
         }
       }
       return;

@@ -34,6 +34,10 @@ from . import DemError, lib
 
 PLAIN, BIAS, BIAS_GELU, BIAS_RELU = 0, 1, 2, 3
 COLSUM_SPLIT = 32
+# one entry of the device list that dem_mlp_adam_multi reads (dem_mlp_tensor:
+# weights, gradient, moments, BF16 copy, element count, L2 penalty, padding)
+ADAM_TENSOR_DTYPE = np.dtype([("w", "<u8"), ("g", "<u8"), ("m", "<u8"), ("v", "<u8"), ("w_bf16", "<u8"),
+                              ("n", "<u8"), ("l2", "<f4"), ("pad", "<f4")])
 
 
 def _r32(n: int) -> int:
@@ -102,8 +106,7 @@ class MLP:
         # device descriptor list of every weight and bias array for the one-launch
         # Adam step (dem_mlp_tensor: w, g, m, v, w_bf16, n, l2, pad)
         nl = len(self.W)
-        rec = np.zeros(len(self.params), dtype=[("w", "<u8"), ("g", "<u8"), ("m", "<u8"), ("v", "<u8"),
-                                                  ("wh", "<u8"), ("n", "<u8"), ("l2", "<f4"), ("pad", "<f4")])
+        rec = np.zeros(len(self.params), dtype=ADAM_TENSOR_DTYPE)
         for i, (w, g, m, v) in enumerate(zip(self.params, self.grads, self.m, self.v)):
             rec[i] = (w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
                       self.Wh[i].data_ptr() if i < nl else 0, w.numel(),

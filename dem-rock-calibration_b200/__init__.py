@@ -95,7 +95,7 @@ class Result(C.Structure):
                 ("platen_bottom", C.c_double), ("platen_velocity", C.c_double), ("steps", C.c_uint64),
                 ("stepsave", C.c_uint32), ("bonds_initial", C.c_uint32), ("bonds_now", C.c_uint32),
                 ("fracture", C.c_int), ("done", C.c_int), ("stale", C.c_int), ("rebuilds", C.c_int),
-                ("E_chord", C.c_double), ("nu", C.c_double)]
+                ("E_chord", C.c_double), ("nu", C.c_double), ("numeric", C.c_int), ("reserved_r", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -134,6 +134,7 @@ def _declare(L):
     L.dem_get_particles_d.argtypes = [_vp, _i32] + [_vp] * 6
     L.dem_set_particles.argtypes = [_vp, _i32] + [_vp] * 4
     L.dem_get_pairs.argtypes = [_vp, _i32, _u32, _vp, _vp, _vp, _vp, P(_u32)]
+    L.dem_get_pairs_d.argtypes = [_vp, _i32, _u32, _vp, _vp, _vp, _vp, P(_u32)]
     L.dem_set_pairs.argtypes = [_vp, _i32, _u32, _vp, _vp, _vp, _vp]
     L.dem_set_platens.argtypes = [_vp, _i32, C.c_double, C.c_double, C.c_double]
     L.dem_rebuild_contacts.argtypes = [_vp]
@@ -406,15 +407,16 @@ class Context:
         R, V, W, Oiwt = c(R), c(V), c(W), c(Oiwt)
         _ck(_lib().dem_set_particles(self._h, sample, _p(R), _p(V), _p(W), _p(Oiwt)), "dem_set_particles")
 
-    def pairs(self, sample: int = 0) -> dict:
+    def pairs(self, sample: int = 0, double: bool = False) -> dict:
+        fn = _lib().dem_get_pairs_d if double else _lib().dem_get_pairs
         n = C.c_uint32()
-        _ck(_lib().dem_get_pairs(self._h, sample, 0, None, None, None, None, C.byref(n)), "dem_get_pairs")
+        _ck(fn(self._h, sample, 0, None, None, None, None, C.byref(n)), "dem_get_pairs")
         m = n.value
         i = np.zeros(max(m, 1), np.uint32)
         j = np.zeros(max(m, 1), np.uint32)
         kind = np.zeros(max(m, 1), np.uint32)
-        st = np.zeros(16 * max(m, 1), np.float32)
-        _ck(_lib().dem_get_pairs(self._h, sample, m, _p(i), _p(j), _p(kind), _p(st), C.byref(n)), "dem_get_pairs")
+        st = np.zeros(16 * max(m, 1), np.float64 if double else np.float32)
+        _ck(fn(self._h, sample, m, _p(i), _p(j), _p(kind), _p(st), C.byref(n)), "dem_get_pairs")
         return dict(i=i[:m], j=j[:m], kind=kind[:m], state=st[:16 * m].reshape(-1, 16))
 
     def set_pairs(self, sample: int, i, j, kind, state):

@@ -50,20 +50,37 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
+    """Compiles every source to an object in parallel (one nvcc per file; no
+    device code crosses files), then links the shared library."""
     if not force and not stale():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", str(ROOT / "include"), "-I", str(SRC),
-           *[str(SRC / s) for s in SOURCES], "-o", str(OUT) + ".tmp", "-lcuda"]
-    if verbose:
-        print(" ".join(cmd))
-    env = dict(os.environ)
     # nvcc's host compiler: the system g++ (a wrapper in CXX may lack parts of the toolchain)
-    if Path("/usr/bin/g++").exists():
-        cmd[1:1] = ["-ccbin", "/usr/bin/g++"]
-    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    ccbin = ["-ccbin", "/usr/bin/g++"] if Path("/usr/bin/g++").exists() else []
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    for src in SOURCES:
+        obj = objdir / (src + ".o")
+        cmd = [nvcc(), *ccbin, *flags, *extra, "-I", str(ROOT / "include"), "-I", str(SRC), "-c", str(SRC / src),
+               "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = False
+    for src, obj, p in procs:
+        out, _ = p.communicate()
+        if verbose or p.returncode != 0:
+            sys.stderr.write(out)
+        failed |= p.returncode != 0
+    if failed:
+        raise RuntimeError("libb200dem build failed")
+    cmd = [nvcc(), *ccbin, "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+           *[str(objdir / (s + ".o")) for s in SOURCES], "-o", str(OUT) + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("libb200dem build failed")
+        raise RuntimeError("libb200dem link failed")
     os.replace(str(OUT) + ".tmp", OUT)
     build_cli()
     return OUT

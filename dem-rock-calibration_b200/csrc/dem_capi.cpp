@@ -142,6 +142,10 @@ int dem_get_pairs(dem_ctx* ctx, int32_t s, uint32_t cap, uint32_t* i, uint32_t* 
                   uint32_t* n) {
   CTX_CALL(ctx->e->get_pairs(s, cap, i, j, kind, st, n));
 }
+int dem_get_pairs_d(dem_ctx* ctx, int32_t s, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind, double* st,
+                    uint32_t* n) {
+  CTX_CALL(ctx->e->get_pairs_d(s, cap, i, j, kind, st, n));
+}
 int dem_set_pairs(dem_ctx* ctx, int32_t s, uint32_t n, const uint32_t* i, const uint32_t* j, const uint32_t* kind,
                   const float* st) {
   CTX_CALL(ctx->e->set_pairs(s, n, i, j, kind, st));
@@ -182,7 +186,7 @@ int dem_calculation_test(const dem_options* opt, const dem_material* mat, const 
   if (!rc) rc = dem_setup(ctx);
   uint64_t steps = 0;
   if (!rc) rc = dem_run(ctx, load->max_steps ? load->max_steps : ~0ull, &steps);
-  if (!rc || rc == DEM_ERR_STALE) {
+  if (!rc || rc == DEM_ERR_STALE || rc == DEM_ERR_NUMERIC) {
     int rc2 = out ? dem_sample_result(ctx, sid, out) : DEM_OK;
     if (!rc2 && (rec || rec_bonds)) rc2 = dem_get_record(ctx, sid, rec, rec_bonds, rec_cap, rec_n);
     if (!rc) rc = rc2;

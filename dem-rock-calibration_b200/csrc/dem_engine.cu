@@ -150,6 +150,8 @@ class Engine final : public EngineBase {
                  int32_t* id) override {
     if (setup_done_) return DEM_ERR_STATE;
     if (!mat || !load || !xyz || n == 0) return DEM_ERR_ARG;
+    for (size_t k = 0; k < 3 * (size_t)n; ++k)
+      if (!std::isfinite(xyz[k])) return DEM_ERR_ARG;
     SampleHost s;
     s.mat = *mat;
     s.load = *load;
@@ -160,7 +162,7 @@ class Engine final : public EngineBase {
     else
       s.rad.assign(n, (float)mat->p_r);
     for (float r : s.rad)
-      if (!(r > 0)) return DEM_ERR_ARG;
+      if (!(r > 0) || !std::isfinite(r)) return DEM_ERR_ARG;
     samples_.push_back(std::move(s));
     if (id) *id = (int32_t)samples_.size() - 1;
     return DEM_OK;
@@ -241,6 +243,10 @@ class Engine final : public EngineBase {
     }
     CK(cudaDeviceSynchronize());
     setup_done_ = true;
+    // the step graphs are captured and instantiated here, so that no later
+    // call pays for an instantiation inside its own time (they are captured
+    // again only after a change that invalidates them)
+    RC(capture_all());
     return DEM_OK;
   }
 
@@ -1126,16 +1132,21 @@ class Engine final : public EngineBase {
     return DEM_OK;
   }
 
-  int capture_graph() {
-    invalidate_graph();
-    return capture_steps(opt_.graph_steps, &graph_exec_);
+  // A chunk shorter than graph_steps (fast particles or a thin skin shorten
+  // them) runs as graphs of 64, 16 and 4 steps and single steps, instead of
+  // two kernel launches per step.
+  static constexpr uint32_t kSizes[3] = {64, 16, 4};
+
+  // Captures every step graph that is missing (the graph_steps graph and the
+  // short-chunk graphs).
+  int capture_all() {
+    if (!graph_exec_) RC(capture_steps(opt_.graph_steps, &graph_exec_));
+    for (int k = 0; k < 3; ++k)
+      if (kSizes[k] < opt_.graph_steps && !small_graphs_[k]) RC(capture_steps(kSizes[k], &small_graphs_[k]));
+    return DEM_OK;
   }
 
-  // A chunk shorter than graph_steps (fast particles or a thin skin shorten
-  // them) runs as graphs of 64, 16 and 4 steps (captured on first use) and
-  // single steps, instead of two kernel launches per step.
   int run_short_chunk(uint64_t chunk) {
-    static constexpr uint32_t kSizes[3] = {64, 16, 4};
     for (int k = 0; k < 3; ++k) {
       while (chunk >= kSizes[k] && kSizes[k] < opt_.graph_steps) {
         if (!small_graphs_[k]) RC(capture_steps(kSizes[k], &small_graphs_[k]));
@@ -1149,7 +1160,7 @@ class Engine final : public EngineBase {
   }
 
   struct Flags {
-    uint32_t done, rebuild, stale;
+    uint32_t done, rebuild, stale, numeric;
     float v2max, d2max;
   };
 
@@ -1160,11 +1171,12 @@ class Engine final : public EngineBase {
     CK(cudaMemcpyAsync(hctl_.data(), ctl_.p, S * sizeof(SampleCtl), cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(st, stat_.p, 2 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
-    f = {1, 0, 0, st[0], st[1]};
+    f = {1, 0, 0, 0, st[0], st[1]};
     for (auto& c : hctl_) {
       f.done &= c.done ? 1u : 0u;
       f.rebuild |= c.rebuild;
       f.stale |= c.stale;
+      f.numeric |= c.numeric;
     }
     return DEM_OK;
   }
@@ -1213,11 +1225,15 @@ class Engine final : public EngineBase {
     return DEM_OK;
   }
 
+  // Runs until max_steps steps or (stop_when_done) until every sample is done.
+  // A sample whose state turned non-finite is stopped by the controller; the
+  // others run on, and the call then returns DEM_ERR_NUMERIC.
   int run(uint64_t max_steps, uint64_t* done_steps, bool stop_when_done) {
     RC(prepare());
     uint64_t steps = 0;
     Flags f{};
     RC(read_flags(f));
+    const uint32_t numeric_before = f.numeric;
     RC(update_tiles());
     while (true) {
       if (f.stale) ++stale_events_;
@@ -1231,7 +1247,7 @@ class Engine final : public EngineBase {
       const uint64_t chunk = std::min(left, chunk_steps(f));
       CK(cudaMemsetAsync(stat_.p, 0, sizeof(float), stream_));  // speed maximum of this chunk
       if (chunk == opt_.graph_steps) {
-        if (!graph_exec_) RC(capture_graph());
+        if (!graph_exec_) RC(capture_steps(opt_.graph_steps, &graph_exec_));
         CK(cudaGraphLaunch(graph_exec_, stream_));
       } else {
         RC(run_short_chunk(chunk));
@@ -1243,7 +1259,7 @@ class Engine final : public EngineBase {
     }
     total_steps_ += steps;
     if (done_steps) *done_steps = steps;
-    return DEM_OK;
+    return (f.numeric && !numeric_before) ? DEM_ERR_NUMERIC : DEM_OK;
   }
 
   int run_until_done(uint64_t max_steps, uint64_t* done) override { return run(max_steps, done, true); }
@@ -1296,6 +1312,7 @@ class Engine final : public EngineBase {
     out->bonds_now = (uint32_t)std::max(C.bonds, 0);
     out->fracture = (int)C.Fracture;
     out->done = (int)C.done;
+    out->numeric = (int)C.numeric;
     out->stale = (int)stale_events_;
     out->rebuilds = (int)std::min<uint64_t>(rebuilds_, INT32_MAX);
     // host post-processing of the record (CalculateLinearityDeviation, CalculateDestruction)
@@ -1535,6 +1552,15 @@ class Engine final : public EngineBase {
   }
 
   int get_pairs(int32_t si, uint32_t cap, uint32_t* oi, uint32_t* oj, uint32_t* kind, float* st, uint32_t* n) override {
+    return get_pairs_t<float>(si, cap, oi, oj, kind, st, n);
+  }
+  int get_pairs_d(int32_t si, uint32_t cap, uint32_t* oi, uint32_t* oj, uint32_t* kind, double* st,
+                  uint32_t* n) override {
+    return get_pairs_t<double>(si, cap, oi, oj, kind, st, n);
+  }
+
+  template <class Out>
+  int get_pairs_t(int32_t si, uint32_t cap, uint32_t* oi, uint32_t* oj, uint32_t* kind, Out* st, uint32_t* n) {
     if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
     RC(prepare());
     const SampleHost& s = samples_[si];
@@ -1554,10 +1580,10 @@ class Engine final : public EngineBase {
     }
     uint32_t m = 0;
     const uint32_t lo = s.p_begin, hi = s.p_begin + s.n;
-    auto emit = [&](uint32_t a, uint32_t b, uint32_t k, const float v[16]) {
+    auto emit = [&](uint32_t a, uint32_t b, uint32_t k, const Out v[16]) {
       if (m < cap) {
         uint32_t ia = s.perm[a - lo], ib = s.perm[b - lo];
-        float w[16];
+        Out w[16];
         std::memcpy(w, v, sizeof(w));
         if (ia > ib) {  // express in the direction i -> j with i < j: mirror the vectors
           std::swap(ia, ib);
@@ -1573,17 +1599,17 @@ class Engine final : public EngineBase {
     for (uint32_t b = 0; b < nb_; ++b) {
       if (bij[b].x < lo || bij[b].x >= hi) continue;
       const bool intact = par[b].x > 0;
-      const float v[16] = {(float)(intact ? par[b].x : -par[b].x),
-                           (float)s0[b].x, (float)s0[b].y, (float)s0[b].z,
-                           (float)s0[b].w, (float)s1[b].x, (float)s1[b].y,
-                           (float)s1[b].z, (float)s1[b].w, (float)s2[b].x,
-                           (float)s2[b].y, (float)s2[b].z, (float)s2[b].w,
-                           (float)par[b].y, (float)par[b].z, (float)par[b].w};
+      const Out v[16] = {(Out)(intact ? par[b].x : -par[b].x),
+                         (Out)s0[b].x, (Out)s0[b].y, (Out)s0[b].z,
+                         (Out)s0[b].w, (Out)s1[b].x, (Out)s1[b].y,
+                         (Out)s1[b].z, (Out)s1[b].w, (Out)s2[b].x,
+                         (Out)s2[b].y, (Out)s2[b].z, (Out)s2[b].w,
+                         (Out)par[b].y, (Out)par[b].z, (Out)par[b].w};
       emit(bij[b].x, bij[b].y, intact ? 1u : 2u, v);
     }
     for (uint32_t c = 0; c < nc_host_; ++c) {
       if (cij[c].x < lo || cij[c].x >= hi) continue;
-      const float v[16] = {0, 0, 0, 0, (float)co[c].x, (float)co[c].y, (float)co[c].z, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+      const Out v[16] = {0, 0, 0, 0, (Out)co[c].x, (Out)co[c].y, (Out)co[c].z, 0, 0, 0, 0, 0, 0, 0, 0, 0};
       emit(cij[c].x, cij[c].y & 0x7FFFFFFFu, 3u, v);
     }
     if (n) *n = m;

@@ -37,6 +37,8 @@ class EngineBase {
   virtual int set_particles(int32_t s, const float* R, const float* V, const float* W, const float* O) = 0;
   virtual int get_pairs(int32_t s, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind, float* st,
                         uint32_t* n) = 0;
+  virtual int get_pairs_d(int32_t s, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind, double* st,
+                        uint32_t* n) = 0;
   virtual int set_pairs(int32_t s, uint32_t n, const uint32_t* i, const uint32_t* j, const uint32_t* kind,
                         const float* st) = 0;
   virtual int set_platens(int32_t s, double top, double bottom, double v) = 0;

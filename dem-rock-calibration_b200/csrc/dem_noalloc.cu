@@ -12,7 +12,16 @@
 // Set-up: host code cannot use the array's name as a device address, so the
 // first call on each device looks the address up with cudaGetSymbolAddress
 // (that device current) and caches it; that first call should come before
-// any stream capture.
+// any stream capture.  The cache is keyed by the device and the unique id of
+// its current context: after a context reset (cudaDeviceReset, or a host
+// framework that recreates the primary context) the module is loaded again
+// at a new address, and the next call looks it up again instead of using the
+// stale one.
+//
+// Stream: every call issues its copies and kernels on the legacy default
+// stream and waits for them before returning, so it also waits for the other
+// blocking streams of the device, and it must not be called while another
+// host thread captures a stream in global capture mode.
 //
 // Limits: n <= DEM_STATIC_MAX_PARTICLES particles and nx*ny*nz <=
 // DEM_STATIC_MAX_CELLS cells; larger calls return DEM_ERR_CAPACITY before any
@@ -20,6 +29,8 @@
 // every call on a device: what must start at zero is cleared per call, and
 // calls that overlap on the GPU (two host threads) race on it, so callers
 // serialise them.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,17 +83,49 @@ static __device__ __align__(256) unsigned char g_scratch[DEM_STATIC_SCRATCH_BYTE
 constexpr int kMaxDevices = 64;
 std::mutex g_addr_mu;
 unsigned char* g_addr[kMaxDevices] = {};
+unsigned long long g_ctx_id[kMaxDevices] = {};   // context the cached address belongs to
+
+// Unique id of the calling thread's current context.  The driver functions
+// are reached through the runtime's entry-point query, so the library keeps
+// no link-time dependency on the driver library (it loads on hosts without a
+// GPU driver, where only its argument checks run).
+int current_context_id(unsigned long long* id) {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 4000, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f1 ||
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f2)
+      return DEM_ERR_CUDA;
+    get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS) return DEM_ERR_CUDA;
+  return DEM_OK;
+}
 
 // Device address of g_scratch on the current device: looked up with
-// cudaGetSymbolAddress on the first call on that device, then cached.
+// cudaGetSymbolAddress on the first call in the device's current context,
+// then cached for that context.
 int scratch_address(unsigned char** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DEM_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_addr_mu);
-  if (!g_addr[dev]) {
+  // makes the device's primary context current (and creates it if needed),
+  // so the driver's current context is the one the runtime calls below use
+  if (cudaSetDevice(dev) != cudaSuccess) return DEM_ERR_CUDA;
+  unsigned long long id = 0;
+  if (current_context_id(&id) != DEM_OK) return DEM_ERR_CUDA;
+  if (!g_addr[dev] || g_ctx_id[dev] != id) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return DEM_ERR_CUDA;
     g_addr[dev] = static_cast<unsigned char*>(p);
+    g_ctx_id[dev] = id;
   }
   *out = g_addr[dev];
   return DEM_OK;
@@ -177,5 +220,10 @@ int ref_cells_static(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_
 extern "C" int dem_ref_cells_static(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz,
                                     uint32_t* CI, uint32_t* CIs, uint32_t* pnC) {
   if (!xyz || n == 0 || !(a > 0) || !nx || !ny || !nz) return DEM_ERR_ARG;
-  return dem::ref_cells_static(xyz, n, a, nx, ny, nz, CI, CIs, pnC);
+  // no exception crosses the C ABI (std::mutex::lock may throw)
+  try {
+    return dem::ref_cells_static(xyz, n, a, nx, ny, nz, CI, CIs, pnC);
+  } catch (...) {
+    return DEM_ERR_STATE;
+  }
 }

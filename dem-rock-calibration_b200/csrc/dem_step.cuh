@@ -754,8 +754,9 @@ __device__ inline void controller_step(SampleCtl& C) {
   C.sFL[1] = 0.0;
   C.lat_sum = 0.0;
   ++C.step;
-  // loop condition of h_Calculation{UniaxialCompression,BrazilTest}
-  if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps) C.done = 1;
+  // loop condition of h_Calculation{UniaxialCompression,BrazilTest}; a sample
+  // whose state went non-finite also stops
+  if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps || C.numeric) C.done = 1;
 }
 
 template <class Real>
@@ -879,6 +880,13 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
         v.x = v.y = v.z = Real(0);
         parked = true;
       }
+      // a non-finite position, velocity or spin (the sum of the nine values is
+      // NaN or infinite exactly when one of them is, barring an overflow of the
+      // sum itself) stops the sample: the controller marks it done and the host
+      // reports DEM_ERR_NUMERIC
+      if (!isfinite((double)x.x + (double)x.y + (double)x.z + (double)v.x + (double)v.y + (double)v.z + (double)w.x +
+                    (double)w.y + (double)w.z))
+        C.numeric = 1u;
       A.pos[p] = x;
       A.vel[p] = v;
       A.omg[p] = w;

@@ -66,7 +66,7 @@ struct SampleCtl {
   double lat_sum;
   double* rec_lat;          // Nsave: mean radial distance of the marked particles
   uint32_t lat_count;       // marked particles (0: no lateral record)
-  uint32_t lat_pad;
+  uint32_t numeric;         // a particle's position, velocity or spin became NaN or infinite
   // deterministic mode: the platen and lateral sums of the step in 2^-40 fixed
   // point, folded into sFL / lat_sum by the controller
   long long sFLq[2];

@@ -51,7 +51,7 @@ def rock_material(r_min: float, r_mean: float, **over) -> Material:
 
 
 def _specimen(name, test, diameter, height, r_min, r_max, packing, seed, velocity_m_s, min_stress_gpa, max_strain,
-              dNsave, max_steps, space_factor=(1.3, 1.3, 1.5), pack_kw=None, **mat_over):
+              dNsave, max_steps, space_factor=(1.3, 1.3, 1.5), pack_kw=None, packer=None, **mat_over):
     radius, half_h = 0.5 * diameter, 0.5 * height
     r_mean = 0.5 * (r_min + r_max)
     n = int(round(packing * math.pi * radius * radius * height / (4.0 / 3.0 * math.pi * mean_r3(r_min, r_max))))
@@ -61,8 +61,11 @@ def _specimen(name, test, diameter, height, r_min, r_max, packing, seed, velocit
     box = reference_space(space_si, lsi, r_max, 3.2)
     pk = dict(growth_stages=30, steps_per_stage=150, max_fire_steps=6000, overlap_tol=2e-3)
     pk.update(pack_kw or {})
-    xyz, rad, rep = create_cylinder_sample(box.center.astype(np.float64), radius, half_h, n, r_min, r_max, E=50.0,
-                                           nu=0.25, rho=2.65, seed=seed, **pk)
+    # `packer`: a function with create_cylinder_sample's signature and result
+    # (the default, on the GPU); the same seeded packing can come from another
+    # implementation of the same algorithm
+    xyz, rad, rep = (packer or create_cylinder_sample)(box.center.astype(np.float64), radius, half_h, n, r_min, r_max,
+                                                       E=50.0, nu=0.25, rho=2.65, seed=seed, **pk)
     size_real, center_real = bounding_box(xyz, n, r_max, radii=rad)
     ld = loading(test, box, size_real, center_real, velocity=-velocity_m_s / VELOCITY, min_stress=min_stress_gpa,
                  max_strain=max_strain, cond_fracture=0.1, dNsave=dNsave, max_steps=max_steps, p_r_platen=r_mean)

@@ -139,6 +139,12 @@ typedef struct {
    * between 10% and 50% of the peak stress, and the Poisson ratio over the
    * same interval from the lateral record; NaN when undefined */
   double E_chord, nu;
+  /* 1 when a particle's position, velocity or spin became NaN or infinite:
+   * the specimen was stopped at that step (done = 1) and the dem_run /
+   * dem_step call in which it happened returned DEM_ERR_NUMERIC.  The
+   * reference has no such check (its loop runs on with NaN state). */
+  int numeric;
+  int reserved_r;
 } dem_result;
 
 /* --- context and specimens --- */
@@ -214,6 +220,9 @@ int dem_set_particles(dem_ctx* ctx, int32_t sample, const float* R, const float*
  * normal strength, shear strength, bond radius). */
 int dem_get_pairs(dem_ctx* ctx, int32_t sample, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind,
                   float* state, uint32_t* n);
+/* The same in double (the FP64 builds' pair state without rounding). */
+int dem_get_pairs_d(dem_ctx* ctx, int32_t sample, uint32_t cap, uint32_t* i, uint32_t* j, uint32_t* kind,
+                    double* state, uint32_t* n);
 /* Overwrites the state of listed pairs (the first 13 values of the record
  * layout; kind 1/2 sets a bond intact/broken, contacts take only the
  * tangential history). */
@@ -276,7 +285,11 @@ int dem_ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, ui
  * array of DEM_STATIC_SCRATCH_BYTES (4.5 MiB), which every GPU that loads the
  * library holds until the process exits.  The first call on a device looks
  * up that array's device address (cudaGetSymbolAddress, with that device
- * current) and keeps it; make that first call before any stream capture.
+ * current) and keeps it for the device's current context (a context reset
+ * makes the next call look it up again); make that first call before any
+ * stream capture.  Every call issues its work on the legacy default stream
+ * and waits for it, so it also waits for the device's other blocking streams
+ * and must not run while another thread captures in global mode.
  * Returns DEM_ERR_CAPACITY, before any device work, when n >
  * DEM_STATIC_MAX_PARTICLES or nx*ny*nz > DEM_STATIC_MAX_CELLS.  All calls on
  * a device share the array: calls that overlap on the GPU (several host

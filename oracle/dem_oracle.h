@@ -154,6 +154,30 @@ double orc_linearity_deviation(orc_compress* C);
 /* md_results.cu:182-187 */
 double orc_destruction(const orc_compress* C);
 
+/* Seeded sample creation restated from the engine's packer (dem_pack_oracle.c):
+ * same fill, growth, FIRE and contact-list schedule, fixed-point pair sums, so
+ * the packing equals the GPU's bit for bit.  Fields as the engine's
+ * dem_pack_params (max_removed must be 0).  fire_trace (optional) receives
+ * (dt, alpha, half-step-back flag) after every FIRE step. */
+typedef struct {
+  double center[3];
+  double radius, half_height;
+  double r_min, r_max;
+  double E, nu, rho;
+  double overlap_tol;
+  uint32_t n, growth_stages, steps_per_stage, max_fire_steps;
+  uint64_t seed;
+  int device, fire_variant;
+  uint32_t max_removed, reserved;
+} orc_pack_params;
+typedef struct {
+  uint64_t steps;
+  double max_overlap, packing_fraction;
+  uint32_t rebuilds, removed;
+} orc_pack_report;
+int orc_pack_cylinder(const orc_pack_params* p, float* xyz, float* radii, uint32_t cap, uint32_t* n,
+                      orc_pack_report* rep, double* fire_trace, uint32_t trace_cap, uint32_t* ntrace);
+
 #ifdef __cplusplus
 }
 #endif

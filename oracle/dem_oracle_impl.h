@@ -201,8 +201,9 @@ void FN(orc_construct_bonds)(const REAL* R, uint32_t N, const uint32_t* IL, uint
       REAL rm2 = (rx * rx + ry * ry) + rz * rz;
       REAL thr = aa_create;
       if (rad) {
+        /* a gap below -(r_i + r_j) bonds nothing (squaring would bond again) */
         double s = (double)rad[idx] + (double)rad[jdx] + gap;
-        thr = (REAL)(s * s);
+        thr = s > 0.0 ? (REAL)(s * s) : (REAL)0;
       }
       if (rm2 < thr && rm2 > 1e-18) {
         inv_L0[kdx] = RSQRT_RN(rm2);

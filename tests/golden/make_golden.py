@@ -2,7 +2,9 @@
 CUDA kernels (oracle/_ref/libdemref.so, compiled by oracle/Makefile from the
 reference sources).  Needs a GPU:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <directory>
+
+(then copy the .npz files into tests/golden/).
 
 Each fixture holds a seeded input state in the reference layout and the state
 the reference kernels produce from it, so that the CPU oracle (and through it

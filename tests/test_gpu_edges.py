@@ -150,3 +150,37 @@ def test_ragged_batch_equals_single_runs():
         for i in [i for i, kk in enumerate(order) if kk == k][:3]:
             assert all(batched[i][key] == r[key] or (np.isnan(batched[i][key]) and np.isnan(r[key]))
                        for key in KEYS), (sizes[k], i)
+
+
+def test_non_finite_state_stops_its_sample_and_is_reported():
+    """A NaN velocity put into one of two specimens (host-side injection):
+    that specimen stops at the step where its state became non-finite
+    (done, numeric flag), the call returns DEM_ERR_NUMERIC, the other
+    specimen runs on unaffected; later calls succeed, and positions given
+    with a NaN are refused up front."""
+    J = _spec(800)
+    ld = _loading(J, max_steps=10 ** 6)
+    ctx = dem.Context()
+    s0 = ctx.add_sample(_mat(J), ld, J.xyz, J.rad)
+    s1 = ctx.add_sample(_mat(J), ld, J.xyz, J.rad)
+    ctx.setup()
+    p = ctx.particles(s0)
+    V = p["V"].copy()
+    V[7] = np.nan
+    ctx.set_particles(s0, V=V)
+    with pytest.raises(dem.DemError) as e:
+        ctx.step(30)
+    assert e.value.code == -8
+    r0, r1 = ctx.result(s0), ctx.result(s1)
+    assert r0["numeric"] == 1 and r0["done"] == 1 and r0["steps"] == 1, r0
+    assert r1["numeric"] == 0 and r1["done"] == 0 and r1["steps"] == 30, r1
+    ctx.step(10)                                   # no new non-finite state: no error
+    assert ctx.result(s1)["steps"] == 40 and ctx.result(s0)["steps"] == 1
+    ctx.close()
+    bad = J.xyz.copy()
+    bad[3] = np.inf
+    ctx = dem.Context()
+    with pytest.raises(dem.DemError) as e:
+        ctx.add_sample(_mat(J), ld, bad, J.rad)
+    assert e.value.code == -1
+    ctx.close()

@@ -5,8 +5,11 @@ against dem_ref_cells on the same inputs.
 
 Two calls in a row on different specimens (the larger first, so counters left
 over from it would show in the second), each compared with dem_ref_cells;
-outputs are integers, so the comparison is exact.  The size limits are checked
-before any device work and are tested without a GPU.
+outputs are integers, so the comparison is exact.  A second test runs a
+case near the limits (60,000 random points in a 40 x 40 x 40 grid: 64,000
+cells, so the cell scan takes its two-level path) and a small specimen after
+it.  The size limits are checked before any device work and are tested
+without a GPU.
 """
 from __future__ import annotations
 
@@ -53,3 +56,21 @@ def test_static_binning_matches_ref_cells_on_two_calls_in_a_row():
     g = load("cells_il_s1")
     CI, CIs, pnC = got
     assert np.array_equal(CI, g["CI"]) and np.array_equal(CIs, g["CIs"]) and np.array_equal(pnC, g["pnC"])
+
+
+@pytest.mark.gpu
+def test_static_binning_near_its_limits_then_small():
+    rng = np.random.default_rng(7)
+    n, g, a = 60000, 40, 1.0
+    xyz = np.ascontiguousarray(rng.uniform(0.0, g * a, 3 * n).astype(np.float32))
+    assert n <= MAX_PARTICLES and g ** 3 <= MAX_CELLS and g ** 3 > 1024   # two scan levels
+    small = T.ref_case(seed=1, **SMALL)
+    cases = [(xyz, (a, g, g, g)), (small.R, (small.cells.a, small.cells.nx, small.cells.ny, small.cells.nz))]
+    for _ in range(2):                     # twice: each call starts from the other's leftovers
+        for pts, cells in cases:
+            want = dem.ref_cells(pts, *cells)
+            got = dem.ref_cells_static(pts, *cells)
+            for w, h in zip(want, got):
+                assert np.array_equal(w, h)
+    CI, CIs, pnC = got
+    assert int(pnC[small.cells.nx * small.cells.ny * small.cells.nz:].sum()) == small.N

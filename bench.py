@@ -16,7 +16,9 @@ collective (weak scaling); the timing barrier and max-over-ranks use
 torch.distributed.
 
 --impl reference times the CPU restatement of the reference step (oracle,
-all host threads) on a bounded number of steps of the same specimen.
+all host threads) for the same --warmup and --steps on the same specimens,
+which it packs on the host with the CPU restatement of the packer (the same
+packings bit for bit); it does not load the product library.
 
 Other workloads (each prints its own line): calibration_sweep (many
 cylinders and parameter sets in one context against one context at a time),
@@ -152,9 +154,74 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_specimen(dem, workload: str, seed: int, device: int):
+def build_specimen(dem, workload: str, seed: int, device: int, packer=None):
+    """A named specimen; `packer` replaces the GPU packer by another
+    implementation of the same seeded algorithm (the reference leg builds its
+    specimens on the host with the CPU restatement, bit for bit the same)."""
     W = importlib.import_module("dem-rock-calibration_b200.workloads")
-    return getattr(W, workload)(seed=seed, pack_kw=dict(device=device))
+    pk = dict(device=device) if packer is None else {}
+    return getattr(W, workload)(seed=seed, pack_kw=pk, packer=packer)
+
+
+def specimen_seeds(args, rank: int) -> list[int]:
+    return [1 + rank * args.specimens + k for k in range(args.specimens)]
+
+
+def workload_config(args, specs, ws: int) -> dict:
+    """The benchmark configuration (identical for both legs): what is run, not
+    what was measured."""
+    n = sum(sp.n for sp in specs)
+    spec = specs[0]
+    if args.workload == "brazilian_disc":
+        what = (f"{args.specimens} x brazilian_disc ({spec.n} spheres each, radii U[0.18,0.30] mm, "
+                f"Brazilian platens at 0.02 m/s) advanced together")
+    else:
+        what = f"{args.specimens} x {args.workload} ({spec.n} spheres each)"
+    return {"workload": what, "particles_per_gpu": n, "specimens": args.specimens,
+            "seeds": specimen_seeds(args, 0), "precision": "f64" if args.precision == 1 else "f32",
+            "parallelism": f"{ws} GPU(s), independent specimens",
+            "l2": "inputs larger than L2 (state above 126 MB), no flush" if n > 300000 else "state inside the L2"}
+
+
+class CpuStep:
+    """The oracle's full loop body (cells, interaction-list rebuild, BPM, HM,
+    platens, integration, escape parking, far-link deletion) of one specimen
+    in the configuration's physics (oracle/physics.py: per-sphere radii and
+    masses, per-slot bond radius and strengths), on host cores."""
+
+    def __init__(self, spec, IonP: int = 48):
+        from oracle import physics as PH
+        from oracle import sim
+
+        self.sim = sim
+        mat, ld = spec.material, spec.loading
+        self.pc = PH.physics_case(mat, ld, spec.radii, IonP=IonP)
+        st = sim.RefState.empty(spec.n, IonP=IonP)
+        st.R[:] = spec.xyz
+        sim.oracle_setup_bonds(st, self.pc.sc, rad=self.pc.rad, gap=mat.gap)
+        n = spec.n
+        IL = st.IL.reshape(n, IonP)
+        jj = np.where(IL == 0xFFFFFFFF, 0, IL)
+        lo, hi = np.minimum(np.arange(n)[:, None], jj), np.maximum(np.arange(n)[:, None], jj)
+        slot_br = (np.float32(mat.bond_radius_factor) * np.minimum(self.pc.rad[:, None], self.pc.rad[jj]))
+        sn, stn = PH.bond_strengths(mat, lo.reshape(-1), hi.reshape(-1))
+        self.kw = self.pc.kw(slot_br.astype(np.float32).reshape(-1), sn, stn)
+        self.st = st
+        self.n = n
+
+    def step(self):
+        self.sim.oracle_step(self.st, self.pc.sc, **self.kw)
+
+    def bonds(self):
+        """Intact undirected bonds (i < j) and their radii."""
+        n, P = self.n, self.pc.IonP
+        IL = self.st.IL.reshape(n, P)
+        ty = self.st.ILtype.reshape(n, P)
+        r, c = np.nonzero((IL != 0xFFFFFFFF) & (ty == 1))
+        j = IL[r, c]
+        keep = r < j
+        br = self.kw["slot_br"].reshape(n, P)[r, c]
+        return r[keep].astype(np.uint32), j[keep].astype(np.uint32), br[keep].astype(np.float32)
 
 
 def algorithmic_bytes(n, bonds, touching, fp64=False):
@@ -167,96 +234,44 @@ def algorithmic_bytes(n, bonds, touching, fp64=False):
     return 60.0 * n + 104.0 * bonds + 28.0 * touching
 
 
-def cpu_baseline(spec, nsteps: int, threads: int):
-    """The oracle's full loop body (cells, interaction-list rebuild, BPM, HM,
-    platens, integration, escape parking, far-link deletion) on host cores."""
-    sys.path.insert(0, str(ROOT / "tests"))
+def cpu_baseline(specs, nsteps: int, warmup: int, threads: int):
+    """Times nsteps loop bodies of every specimen (after `warmup` untimed
+    ones) on `threads` host threads: particle-steps/s, seconds, threads."""
     from oracle import lib as L
-    from oracle import params as prm
-    from oracle import sim
 
-    dem = importlib.import_module("dem-rock-calibration_b200")
     L.lib().orc_set_threads(threads)
-    n = spec.n
-    mat, ld = spec.material, spec.loading
-    r_mean = float(np.mean(spec.radii))
-    a_far = mat.farcut * mat.p_r
-    C_a = float(np.float32(2.0 * a_far))
-    B = [ld.space_center[d] + ld.space_half[d] + 1.01 * C_a for d in range(3)]
-    cells = prm.cells_for(2.0 * a_far, B)
-    st = sim.RefState.empty(n)
-    st.R[:] = spec.xyz
-    # per-particle constants as the engine derives them
-    rad = spec.radii.astype(np.float32)
-    r = rad.astype(np.float64)
-    mass = mat.rho * (4.0 * (1.0 / 3.0) * np.pi * r ** 3)
-    # the engine's rule: factor * min(Rayleigh time, bond time) of the smallest sphere
-    rmin = r.min()
-    t_r = np.pi * rmin * np.sqrt(2.0 * mat.rho * (1.0 + mat.nu)) / (np.sqrt(mat.E) * (0.163 * mat.nu + 0.8766))
-    e_b = mat.E_bond if mat.E_bond > 0 else mat.E
-    g_b = e_b / mat.kn_ks if mat.kn_ks > 0 else 0.5 * e_b / (1.0 + mat.nu)
-    k_b = max(e_b, g_b) * np.pi * (mat.bond_radius_factor * rmin) ** 2 / (2.0 * rmin)
-    t_b = 2.0 * np.sqrt(mat.rho * 4.0 / 3.0 * np.pi * rmin ** 3 / k_b)
-    dt = mat.dt_rayleigh_factor * min(t_r, t_b)
-    dtm = ((1.0 / mass) * dt).astype(np.float32)
-    dtI = (dt / (0.4 * mass * r * r)).astype(np.float32)
-    hmE = 0.5 * mat.E / (1 - mat.nu ** 2)
-    Gp = 0.5 * mat.E / (1 + mat.nu)
-    hmG = 0.5 * Gp / (2 - mat.nu)
-    le = np.log(mat.p_e)
-    pA = le / np.sqrt(np.pi ** 2 + le ** 2)
-    Eb = mat.E_bond
-    Gb = Eb / mat.kn_ks
-    sc = sim.Scalars(a=cells.a, inv_a=cells.inv_a, nx=cells.nx, ny=cells.ny, nz=cells.nz, IonP=32,
-                     il_aacut=prm.il_aacut(a_far), aa_farcut=prm.F(a_far * a_far), dt=prm.F(dt), m_E=prm.F(Eb),
-                     m_G=prm.F(Gb), b_r=0.0, m_Ec=prm.F(mat.Ec), m_Gc=prm.F(mat.Gc), hm_E=prm.F(hmE),
-                     hm_G=prm.F(hmG), p_A=prm.F(pA), p_mu=prm.F(mat.mu), p_mur=prm.F(mat.mur), p_m=0.0, p_r=r_mean,
-                     wall_E=prm.F(hmE), wall_G=prm.F(hmG), center=np.array(ld.center_real[:], np.float32),
-                     wall_RR=float(np.float32(0.5 * ld.size_real[0]) ** 2), wall_top=prm.F(ld.center_real[1] +
-                                                                                        0.5 * ld.size_real[1]),
-                     wall_bot=prm.F(ld.center_real[1] - 0.5 * ld.size_real[1]), wall_V=prm.F(ld.velocity),
-                     Zcut=prm.F(ld.zcut), dt_d_m=0.0, dt_d_I=0.0,
-                     s_center=np.array(ld.space_center[:], np.float32),
-                     s_spacesized2=np.array(ld.space_half[:], np.float32),
-                     hidenpoint=np.array(ld.hidden_point[:], np.float32), brazil=1)
-    sim.oracle_setup_bonds(st, sc, rad=rad, gap=mat.gap)
-    # per-slot bond radius and strengths (0.8 min r, mean strengths)
-    IL = st.IL.reshape(n, 32)
-    jj = np.where(IL == L.EMPTY, 0, IL)
-    slot_br = (0.8 * np.minimum(rad[:, None], rad[jj])).astype(np.float32).reshape(-1)
-    slot_sn = np.full(n * 32, prm.F(mat.Ec), np.float32)
-    slot_st = np.full(n * 32, prm.F(mat.Gc), np.float32)
-    kw = dict(rad=rad, mass=mass.astype(np.float32), slot_br=slot_br, slot_sn=slot_sn, slot_st=slot_st,
-              dtm_i=dtm, dtI_i=dtI)
-    sim.oracle_step(st, sc, **kw)  # warm caches / first-touch
+    steps = [CpuStep(sp) for sp in specs]
+    for _ in range(warmup):
+        for c in steps:
+            c.step()
     t0 = time.perf_counter()
     for _ in range(nsteps):
-        sim.oracle_step(st, sc, **kw)
+        for c in steps:
+            c.step()
     el = time.perf_counter() - t0
-    return n * nsteps / el, el, L.lib().orc_get_threads()
+    n = sum(c.n for c in steps)
+    return n * nsteps / el, el, L.lib().orc_get_threads(), steps
 
 
-def reference_bpm_cpu(spec, pairs, seconds: float = 3.0, max_bonds: int = 20000):
+def reference_bpm_cpu(spec, bonds, seconds: float = 3.0, max_bonds: int = 20000):
     """The reference's own CPU BPM routine, h_CalculateForceElastic
     (md_calculateforcesbpm_cpu.cu:20-262), compiled from the reference sources
     into oracle/_ref/libdemref.so: one call per directed bond slot of the
-    specimen's first max_bonds intact bonds (fresh bond state), on one host
-    thread (the routine prints on every call and is not re-entrant; its output
-    goes to /dev/null), for `seconds`.  Reported as directed-bond evaluations
-    per second and as the particle-steps/s of a BPM-only step (2 B evaluations
-    per step over the whole specimen).  None when the library is absent."""
-    if pairs is None:
-        return None
-    sys.path.insert(0, str(ROOT / "tests"))
+    specimen's first max_bonds intact bonds (fresh bond state; bonds and radii
+    from the oracle's set-up), on one host thread (the routine prints on every
+    call and is not re-entrant; its output goes to /dev/null), for `seconds`.
+    Reported as directed-bond evaluations per second and as the
+    particle-steps/s of a BPM-only step (2 B evaluations per step over the
+    whole specimen)."""
     try:
         from oracle import lib as L
         R = L.ref()
     except Exception as e:                      # library not built / not shipped
         return {"value": None, "unavailable": f"oracle/_ref/libdemref.so: {type(e).__name__}: {e}"[:200]}
-    bond = pairs["kind"] == 1
-    bi = np.ascontiguousarray(pairs["i"][bond][:max_bonds], np.uint32)
-    bj = np.ascontiguousarray(pairs["j"][bond][:max_bonds], np.uint32)
-    br = np.ascontiguousarray(pairs["state"][bond][:max_bonds, 15], np.float32)
+    bi_all, bj_all, br_all = bonds
+    bi = np.ascontiguousarray(bi_all[:max_bonds])
+    bj = np.ascontiguousarray(bj_all[:max_bonds])
+    br = np.ascontiguousarray(br_all[:max_bonds])
     n = spec.n
     Rs = np.ascontiguousarray(spec.xyz, np.float32)
     V = np.zeros(3 * n, np.float32)
@@ -268,7 +283,7 @@ def reference_bpm_cpu(spec, pairs, seconds: float = 3.0, max_bonds: int = 20000)
                              m.E_bond / m.kn_ks, m.Ec, m.Gc, seconds, C.byref(ev), C.byref(sec))
     if rc != 0:
         return {"value": None, "unavailable": f"refh_time_bpm_cpu returned {rc}"}
-    B = int(bond.sum())
+    B = int(bi_all.size)
     return {"value": n * ev.value / (2.0 * B), "unit": UNIT, "cores": 1, "kind": "reference",
             "bond_evaluations_per_s": ev.value, "seconds": sec.value,
             "sample": f"h_CalculateForceElastic over {bi.size} of the {B} bonds of the {n}-sphere specimen, "
@@ -277,26 +292,38 @@ def reference_bpm_cpu(spec, pairs, seconds: float = 3.0, max_bonds: int = 20000)
 
 
 def run_reference(args, ws, rank, local):
-    """--impl reference: the CPU restatement on host cores (rank 0 only)."""
+    """--impl reference: the reference's loop body restated by the oracle (the
+    reference has no CPU implementation of the step; its kernels are CUDA) on
+    all host threads, over the same specimens as the engine's leg - built on
+    the host by the CPU restatement of the packer, bit for bit the GPU's
+    packing - for exactly --warmup untimed and --steps timed steps.  Rank 0
+    alone runs; the product library is not loaded."""
     if rank != 0:
         return 0
-    dem = importlib.import_module("dem-rock-calibration_b200")
-    spec = build_specimen(dem, args.workload, 1, local)
+    from oracle import pack
+
+    dem = importlib.import_module("dem-rock-calibration_b200")   # Python helpers only (no library load)
+    t0 = time.perf_counter()
+    specs = [build_specimen(dem, args.workload, sd, local, packer=pack.create_cylinder_sample)
+             for sd in specimen_seeds(args, 0)]
+    t_pack = time.perf_counter() - t0
     threads = os.cpu_count() or 1
-    steps = max(1, min(args.steps, args.ref_steps))
-    v, el, th = cpu_baseline(spec, steps, threads)
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": steps,
-            "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded packing)",
-            "config": {"workload": f"{args.workload}: {spec.n} spheres", "particles": spec.n},
+    v, el, th, steps = cpu_baseline(specs, args.steps, args.warmup, threads)
+    n = sum(sp.n for sp in specs)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
+            "config": workload_config(args, specs, ws),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
-                             "sample": f"{steps} full loading steps of the {spec.n}-sphere specimen"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    ctx = dem.Context(device=local)
-    ctx.add_sample(spec.material, spec.loading, spec.xyz, spec.radii)
-    ctx.setup()
-    line["cpu_baseline_reference_bpm"] = reference_bpm_cpu(spec, ctx.pairs(0))
-    ctx.close()
+                             "sample": f"{args.steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
+                                       f"integration) of each of the {len(specs)} specimens ({n} spheres)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "details": {"packing_seconds_untimed": t_pack,
+                        "packing": [sp.pack for sp in specs],
+                        "note": "specimens packed on the host by oracle/dem_pack_oracle.c (the engine's packer "
+                                "restated; identical packings); the reference's own step is CUDA only, so the "
+                                "oracle's restatement of it stands in on the CPU"}}
+    line["cpu_baseline_reference_bpm"] = reference_bpm_cpu(specs[0], steps[0].bonds())
     print(json.dumps(line), flush=True)
     return 0
 
@@ -595,8 +622,8 @@ def run_solves(args, ws, rank, local):
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3000)
-    ap.add_argument("--warmup", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brazilian_disc",
                     choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep", "calibration_solves",
@@ -604,7 +631,6 @@ def main() -> int:
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
-    ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sim-data", type=int, default=0,
                     help="surrogate: train on this many simulated parameter sets instead of synthetic targets")
@@ -629,7 +655,7 @@ def main() -> int:
         return run_solves(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
-    specs = [build_specimen(dem, args.workload, 1 + rank * args.specimens + k, local) for k in range(args.specimens)]
+    specs = [build_specimen(dem, args.workload, sd, local) for sd in specimen_seeds(args, rank)]
     spec = specs[0]
     ctx = dem.Context(precision=args.precision, device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
                       deterministic=args.deterministic, skin_factor=args.skin)
@@ -658,7 +684,6 @@ def main() -> int:
     w = 2 if args.precision == 1 else 1
     state_mb = (n_gpu * (7 * 16 * w + 8) + cnt["bonds"] * (8 + 4 * 16 * w) + cnt["contacts"] * 24 * w) / 1e6
     stale = sum(r["stale"] for r in res)
-    pairs0 = ctx.pairs(sids[0]) if rank == 0 and ws == 1 and not args.no_cpu else None
     ctx.close()
     # the same pipeline on one specimen alone (state inside the L2), for reference
     one = dem.Context(precision=args.precision, device=local, graph_steps=200, skin_factor=args.skin,
@@ -693,30 +718,25 @@ def main() -> int:
     d2h = sum(r.nbytes + b.nbytes for r, b in recs) + len(specs) * 160
     cpu = cpu_bpm = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, el, th = cpu_baseline(spec, args.cpu_steps, os.cpu_count() or 1)
+        v, el, th, steps = cpu_baseline([spec], args.cpu_steps, 1, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                "sample": f"{args.cpu_steps} full loading steps (cells, list rebuild, BPM, HM, platens, "
                          f"integration) of the {spec.n}-sphere specimen"}
-        cpu_bpm = reference_bpm_cpu(spec, pairs0)
+        cpu_bpm = reference_bpm_cpu(spec, steps[0].bonds())
     default_disc = (args.workload == "brazilian_disc" and args.specimens == 2 and args.precision == 0
                     and not args.deterministic and args.skin in (0.0, 0.1))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == 1 else "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
-        "config": {"workload": f"{args.specimens} x {args.workload} ({spec.n} spheres each, radii "
-                               f"U[0.18,0.30] mm, Brazilian platens at 0.02 m/s) advanced together"
-                               if args.workload == "brazilian_disc" else
-                               f"{args.specimens} x {args.workload} ({spec.n} spheres each)",
-                   "particles_per_gpu": n_gpu, "bonds": bonds, "contacts_listed": cnt["contacts"],
-                   "touching_contacts": prof["touching"], "parallelism": f"{ws} GPU(s), independent specimens",
-                   "l2": f"inputs larger than L2: state {state_mb:.0f} MB per GPU vs 126 MB L2, no flush",
-                   "packing": spec.pack, "stale_lists": stale,
-                   "force_sums": "fixed point (deterministic)" if args.deterministic else "float atomics",
-                   "contact_list_builds_timed": rb1 - rb0,
-                   "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
-                                       "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
-                                       "note": "state inside the L2"}},
+        "config": workload_config(args, specs, ws),
+        "details": {"bonds": bonds, "contacts_listed": cnt["contacts"], "touching_contacts": prof["touching"],
+                    "packing": spec.pack, "stale_lists": stale,
+                    "force_sums": "fixed point (deterministic)" if args.deterministic else "float atomics",
+                    "contact_list_builds_timed": rb1 - rb0, "state_mb": state_mb,
+                    "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
+                                        "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
+                                        "note": "state inside the L2"}},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -392,16 +392,36 @@ __device__ __forceinline__ void scatter_j_warp(const StepArgs<Real>& A, uint32_t
 // reference is its exact mirror (all vectors negated, the unsymmetric moment
 // equal), so j receives -F, -(Mn + Mt) terms and the same unsymmetric moment.
 template <class Real, bool kDetJ>
+__device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
+                                             typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
+                                             typename RT<Real>::V4 s1, typename RT<Real>::V4 s2, uint32_t ts,
+                                             const typename RT<Real>::V4& pi, const typename RT<Real>::V4& pj,
+                                             const typename RT<Real>::V4& vi, const typename RT<Real>::V4& vj,
+                                             const typename RT<Real>::V4& wi, const typename RT<Real>::V4& wj);
+
+template <class Real, bool kDetJ>
 __device__ __forceinline__ void do_bond(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
                                         typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
                                         typename RT<Real>::V4 s1, typename RT<Real>::V4 s2, uint32_t ts) {
-  using T = RT<Real>;
-  using V4 = typename T::V4;
+  using V4 = typename RT<Real>::V4;
   // the gathers depend only on (i, j): all issued before the first branch
   const uint32_t i = ij.x, j = ij.y;
   const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
   const V4 wi = ld4(A.omg + i), wj = ld4(A.omg + j);
   const V4 vi = ld4(A.vel + i), vj = ld4(A.vel + j);
+  do_bond_core<Real, kDetJ>(A, b, ij, par, s0, s1, s2, ts, pi, pj, vi, vj, wi, wj);
+}
+
+// The bond itself, given the particle states of its two ends.
+template <class Real, bool kDetJ>
+__device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b, const uint2 ij,
+                                             typename RT<Real>::V4 par, typename RT<Real>::V4 s0,
+                                             typename RT<Real>::V4 s1, typename RT<Real>::V4 s2, uint32_t ts,
+                                             const typename RT<Real>::V4& pi, const typename RT<Real>::V4& pj,
+                                             const typename RT<Real>::V4& vi, const typename RT<Real>::V4& vj,
+                                             const typename RT<Real>::V4& wi, const typename RT<Real>::V4& wj) {
+  using T = RT<Real>;
+  const uint32_t i = ij.x, j = ij.y;
   const uint32_t s = ts != ~0u ? ts : A.sid[i];
   if (A.ctl[s].done) return;
   const SampleParams<Real>& sp = A.sp[s];
@@ -620,6 +640,113 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) 
   }
   const uint32_t nc = *A.nc;
   for (uint32_t c = blockIdx.x * tile + threadIdx.x; c < nc; c += stride) do_contact<Real>(A, c);
+}
+
+// 16-byte asynchronous copy global -> shared (cp.async, L1-allocating), and
+// its group fences.  Each thread waits only for its own copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// FP32 pair kernel with the particle gathers of the next bond tile in flight
+// while the current one is computed.  Every thread copies the six particle
+// vectors of its next bond (position, velocity, spin of both ends: 96 bytes)
+// into its own slots of a two-stage shared-memory buffer with cp.async, then
+// waits only for the stage of the current bond: no block or warp barrier (a
+// thread reads only what it copied itself), so each warp runs its own
+// pipeline.  The pair indices run one more tile ahead, so that the copies of
+// the next tile can be issued at the top of an iteration without an index
+// round trip; the bond state itself streams through L2 (bulk prefetch of the
+// next tile, evict-first loads).  Float atomics only (deterministic contexts
+// use k_pairs).
+template <int kMinBlocks, int kBlock = 128>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_async(StepArgs<float> A) {
+  __shared__ float4 g[2][6][kBlock];   // stage, (pos i, pos j, vel i, vel j, spin i, spin j), thread
+  const uint32_t nb = A.nb, tid = threadIdx.x;
+  const uint32_t tile = kBlock;
+  const uint32_t ntl = A.tiles ? *A.ntiles : (nb + tile - 1) / tile;
+  auto tile_base = [&](uint32_t k) { return (A.tiles ? A.tiles[k] : k) * tile; };
+  auto issue = [&](uint32_t stage, uint2 ij) {
+    cp_async16(&g[stage][0][tid], A.pos + ij.x);
+    cp_async16(&g[stage][1][tid], A.pos + ij.y);
+    cp_async16(&g[stage][2][tid], A.vel + ij.x);
+    cp_async16(&g[stage][3][tid], A.vel + ij.y);
+    cp_async16(&g[stage][4][tid], A.omg + ij.x);
+    cp_async16(&g[stage][5][tid], A.omg + ij.y);
+  };
+  uint32_t k = blockIdx.x;
+  uint32_t base = 0, ts = ~0u;
+  uint2 ij = make_uint2(0, 0);
+  bool have = false;
+  if (k < ntl) {
+    base = tile_base(k);
+    if (A.tile_s) ts = __ldg(A.tile_s + base / tile);
+    have = base + tid < nb;
+    if (have) {
+      ij = __ldcs(A.b_ij + base + tid);
+      issue(0, ij);
+    }
+  }
+  cp_async_commit();
+  // pair indices of the next tile
+  uint32_t kn = k + gridDim.x, nbase = 0, nts = ~0u;
+  uint2 nij = make_uint2(0, 0);
+  bool nhave = false;
+  if (kn < ntl) {
+    nbase = tile_base(kn);
+    if (A.tile_s) nts = __ldg(A.tile_s + nbase / tile);
+    nhave = nbase + tid < nb;
+    if (nhave) nij = __ldcs(A.b_ij + nbase + tid);
+  }
+  uint32_t stage = 0;
+  for (; k < ntl; k += gridDim.x) {
+    // copies of the next tile into the other stage (an empty group past the end)
+    if (nhave) issue(stage ^ 1u, nij);
+    cp_async_commit();
+    // pair indices of the tile after it, and the next tile's bond state into L2
+    const uint32_t knn = kn + gridDim.x;
+    uint32_t nnbase = 0, nnts = ~0u;
+    uint2 nnij = make_uint2(0, 0);
+    bool nnhave = false;
+    if (knn < ntl) {
+      nnbase = tile_base(knn);
+      if (A.tile_s) nnts = __ldg(A.tile_s + nnbase / tile);
+      nnhave = nnbase + tid < nb;
+      if (nnhave) nnij = __ldcs(A.b_ij + nnbase + tid);
+    }
+    if (kn < ntl && tid == 0) {
+      l2_prefetch(A.b_par + nbase, tile * sizeof(float4));
+      l2_prefetch(A.b_s0 + nbase, tile * sizeof(float4));
+      l2_prefetch(A.b_s1 + nbase, tile * sizeof(float4));
+      l2_prefetch(A.b_s2 + nbase, tile * sizeof(float4));
+    }
+    if (have) {
+      const uint32_t b = base + tid;
+      const float4 par = ld4_cs(A.b_par + b), s0 = ld4_cs(A.b_s0 + b), s1 = ld4_cs(A.b_s1 + b),
+                   s2 = ld4_cs(A.b_s2 + b);
+      cp_async_wait_all_but_one();   // this tile's copies (the next tile's may still fly)
+      const float4 pi = g[stage][0][tid], pj = g[stage][1][tid], vi = g[stage][2][tid], vj = g[stage][3][tid],
+                   wi = g[stage][4][tid], wj = g[stage][5][tid];
+      do_bond_core<float, false>(A, b, ij, par, s0, s1, s2, ts, pi, pj, vi, vj, wi, wj);
+    }
+    stage ^= 1u;
+    base = nbase;
+    ts = nts;
+    ij = nij;
+    have = nhave;
+    kn = knn;
+    nbase = nnbase;
+    nts = nnts;
+    nij = nnij;
+    nhave = nnhave;
+  }
+  cp_async_wait_all();
+  const uint32_t nc = *A.nc;
+  for (uint32_t c = blockIdx.x * tile + tid; c < nc; c += gridDim.x * tile) do_contact<float>(A, c);
 }
 
 // Particle-platen contact (dd_Calculate_fijn_pwHM_2 + dd_Calculate_fijtmijt_pwHM_2,

@@ -92,7 +92,8 @@ def normal_deviates(seed: int, a, b, stream: int) -> np.ndarray:
         a = np.asarray(a, np.uint64)
         b = np.asarray(b, np.uint64)
         s = np.uint64(seed)
-        k = s ^ _splitmix64(a * np.uint64(0x100000001B3) + b) ^ (np.uint64(stream) * np.uint64(0xD6E8FEB86659FD93))
+        k = _splitmix64(s ^ _splitmix64(a * np.uint64(0x100000001B3) + b) ^
+                        (np.uint64(stream) * np.uint64(0xD6E8FEB86659FD93)))
         u1 = _u01(_splitmix64(k))
         u2 = _u01(_splitmix64(k ^ np.uint64(0x5851F42D4C957F2D)))
     return np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586476925286766559 * u2)

@@ -1,0 +1,174 @@
+"""Macro properties of whole loading tests, over five seeds: Young's modulus
+and Poisson's ratio against the oracle, uniaxial strength and Brazilian
+tensile strength against the reference's own drivers.
+
+* Elastic moduli (the configurations' physics: polydisperse 4 mm x 8 mm
+  cylinders, bond modulus 30 GPa, kn/ks 2.5, bond radius 0.8 min r;
+  unbreakable bonds, loading to 0.15% strain): the engine's whole test
+  against the oracle running the same test on the CPU (oracle/drive.py: the
+  reference's loop body and host controller restated, in the
+  configurations' physics).  The chord Young modulus (10-50% of the peak) and
+  the Poisson ratio over the same interval from the lateral record must
+  agree within 1% for every seed.  The reference computes neither property
+  (it records platen stresses only, md_results.cu:56-145), so the oracle
+  carries the comparison; the elastic record itself is compared with the
+  reference's driver in test_gpu_dynamics.py.
+* Strengths (reference-mode specimens the reference's drivers run: equal
+  radii 0.25 mm, 40 MPa bonds): uniaxial compressive strength and strain at
+  peak (h_CalculationUniaxialCompression, md_calculationuniaxialcompression.cu:126-340)
+  and Brazilian tensile strength (h_CalculationBrazilTest,
+  md_calculationbraziltest.cu:116-265; sigma_t = F / (pi R t),
+  md_data_types.h:395).  Once bonds break the run is chaotic: the engine's
+  own repeated runs of one specimen differ (float atomics change the
+  summation order), so one reference run is one draw of a distribution.
+  Compared are the means over five specimens (reference once, engine four
+  times each); the bound is three standard errors of the difference of the
+  means, estimated from the engine's spread between its repeated runs.  The
+  statistics are printed (pytest -s).
+"""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+
+from dem_api import dem
+from oracle import drive
+from oracle import lib as L
+from oracle import physics as PH
+from oracle import sim
+from test_gpu_dynamics import _both_drivers, _sigma
+
+pytestmark = pytest.mark.gpu
+
+W = importlib.import_module("dem-rock-calibration_b200.workloads")
+SEEDS = (1, 2, 3, 4, 5)
+
+
+def _elastic_specimen(seed):
+    pk = dict(growth_stages=20, steps_per_stage=150, max_fire_steps=4000)
+    sp = W.uniaxial_cylinder(seed=seed, diameter=4.0, height=8.0, pack_kw=pk)
+    mat = dem.Material.from_buffer_copy(sp.material)
+    mat.nobreak = 1
+    ld = dem.Loading.from_buffer_copy(sp.loading)
+    ld.max_strain = 0.0015
+    ld.dNsave = 20
+    return sp, mat, ld
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+def test_elastic_moduli_match_oracle(seed):
+    sp, mat, ld = _elastic_specimen(seed)
+    ctx = dem.Context(deterministic=True)
+    sid = ctx.add_sample(mat, ld, sp.xyz, sp.radii)
+    ctx.setup()
+    ctx.run(10 ** 6)
+    res = ctx.result(sid)
+    rec, _ = ctx.record(sid)
+    lat = ctx.lateral_record(sid)
+    ctx.close()
+    assert res["done"] and res["bonds_now"] == res["bonds_initial"]
+    # the oracle runs the same test
+    pc = PH.physics_case(mat, ld, sp.radii, dt=res["dt"])
+    st = sim.RefState.empty(sp.n, IonP=pc.IonP)
+    st.R[:] = sp.xyz
+    sim.oracle_setup_bonds(st, pc.sc, rad=pc.rad, gap=mat.gap)
+    n, P = sp.n, pc.IonP
+    jj = np.where(st.IL.reshape(n, P) == L.EMPTY, 0, st.IL.reshape(n, P))
+    slot_br = (np.float32(mat.bond_radius_factor) * np.minimum(pc.rad[:, None], pc.rad[jj])).astype(np.float32)
+    lateral = drive.lateral_spheres(sp.xyz, sp.radii.astype(np.float64), ld.center_real, ld.size_real,
+                                    float(np.mean(sp.radii.astype(np.float64))))
+    o = drive.loading_run(st, pc.sc, brazil=False, size_real=list(ld.size_real), center_real=list(ld.center_real),
+                          p_r=ld.p_r_platen, min_stress=ld.min_stress, max_strain=ld.max_strain,
+                          cond_fracture=ld.cond_fracture, velocity=ld.velocity, dt=res["dt"], dNsave=ld.dNsave,
+                          max_steps=10 ** 6, nobreak=1, lateral=lateral,
+                          axis_center=np.float32(np.array(ld.center_real[:2])).astype(np.float64),
+                          **pc.kw(slot_br.reshape(-1), None, None))
+    E_o, nu_o = drive.chord_moduli(o["rec"], o["lat"])
+    E_e, nu_e = drive.chord_moduli(rec, lat)
+    assert E_e == pytest.approx(res["E_chord"], rel=1e-9) and nu_e == pytest.approx(res["nu"], rel=1e-9)
+    # whole records: same length, stresses within 1% of the peak at every entry
+    m = min(len(rec), len(o["rec"]))
+    assert abs(len(rec) - len(o["rec"])) <= 1
+    dev = np.abs(_sigma(rec[:m]) - _sigma(o["rec"][:m])).max() / _sigma(o["rec"]).max()
+    print(f"\nseed {seed}: {sp.n} spheres, {o['steps']} steps; E {E_e:.5g} vs {E_o:.5g} GPa "
+          f"({(E_e / E_o - 1) * 100:+.3f}%), nu {nu_e:.5g} vs {nu_o:.5g} ({(nu_e / nu_o - 1) * 100:+.3f}%), "
+          f"record {dev * 100:.3f}% of peak")
+    assert dev <= 0.01
+    assert abs(E_e - E_o) <= 0.01 * E_o
+    assert 0.0 < nu_o < 0.5 and abs(nu_e - nu_o) <= 0.01 * nu_o
+
+
+def _compare_means(name, ref_vals, eng_vals):
+    """ref_vals[s]: one reference value per seed; eng_vals[s]: the engine's
+    runs of seed s.  Returns (mean_ref, mean_eng, standard error of the
+    difference, relative difference)."""
+    r = np.asarray(ref_vals, np.float64)
+    e = np.asarray(eng_vals, np.float64)
+    S, k = e.shape
+    s = float(np.sqrt(np.mean(np.var(e, axis=1, ddof=1))))     # run-to-run spread (pooled over seeds)
+    se = s * np.sqrt(1.0 / (S * k) + 1.0 / S)
+    mr, me = float(r.mean()), float(e.mean())
+    print(f"{name}: reference mean {mr:.5g}, engine mean {me:.5g} ({(me / mr - 1) * 100:+.2f}%), run-to-run "
+          f"sd {s / mr * 100:.2f}%, standard error of the difference {se / mr * 100:.2f}%")
+    return mr, me, se, me / mr - 1
+
+
+@pytest.mark.skipif(not L.ref_available(), reason="reference harness not built")
+def test_uniaxial_strength_statistics_match_reference_driver(tmp_path):
+    ucs_r, eps_r, ucs_m, eps_m = [], [], [], []
+    for seed in SEEDS:
+        out, ref_rec, mine = _both_drivers(tmp_path / f"s{seed}", seed, 40e6, 40e6, 0.01, 0.7, runs=4)
+        ucs_r.append(out.FractureStress)
+        eps_r.append(out.FractureStrain)
+        ucs_m.append([res["FractureStress"] for res, _ in mine])
+        eps_m.append([res["FractureStrain"] for res, _ in mine])
+        for res, _ in mine:
+            assert 0.0 < res["nu"] < 0.5
+    print()
+    for name, r, e in (("UCS", ucs_r, ucs_m), ("strain at peak", eps_r, eps_m)):
+        mr, me, se, rel = _compare_means(name, r, e)
+        assert abs(me - mr) <= 3.0 * se + 0.005 * mr, (name, mr, me, se)
+
+
+@pytest.mark.skipif(not L.ref_available(), reason="reference harness not built")
+def test_brazilian_tensile_strength_statistics_match_reference_driver(tmp_path):
+    lsi, space = (0.006, 0.006, 0.003), (0.012, 0.012, 0.006)
+    st_r, st_m = [], []
+    for seed in SEEDS:
+        out, ref_rec, mine = _both_drivers(tmp_path / f"s{seed}", seed, 40e6, 40e6, 0.03, 0.1, runs=4, brazil=True,
+                                           lsi=lsi, space=space, minstress_si=1e6, dNsave=50)
+        st_r.append(out.FractureStress)
+        st_m.append([res["FractureStress"] for res, _ in mine])
+        for res, rec in mine:
+            assert res["fracture"] == 1 and res["FractureStress"] > 1e6 / dem.STRESS
+    print()
+    mr, me, se, rel = _compare_means("Brazilian tensile strength", st_r, st_m)
+    assert abs(me - mr) <= 3.0 * se + 0.005 * mr, (mr, me, se)
+
+
+@pytest.mark.skipif(not L.ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_brazilian_elastic_record_matches_reference_driver(tmp_path, seed):
+    """Unbreakable bonds, diametral loading to 0.1% strain: the engine's
+    stress-strain record against h_CalculationBrazilTest's (the Brazilian
+    controller CompressB_S3 with its symmetric platens and wait on
+    asymmetry, md_data_types.h:462-494; SumForcesBLoading with its peak reset,
+    md_results.cu:101-145).  Within 2% of the peak at every strain, the final
+    stress within 1%."""
+    lsi, space = (0.006, 0.006, 0.003), (0.012, 0.012, 0.006)
+    out, ref_rec, mine = _both_drivers(tmp_path, seed, 1e12, 1e12, 0.001, 0.1, runs=1, brazil=True, lsi=lsi,
+                                       space=space, minstress_si=1e6, dNsave=50)
+    res, rec = mine[0]
+    assert res["bonds_now"] == res["bonds_initial"]
+    eps_r, sig_r = -ref_rec[:, 0], _sigma(ref_rec)
+    eps_m, sig_m = -rec[:, 0], _sigma(rec)
+    assert abs(len(rec) - len(ref_rec)) <= 1
+    lo, hi = max(eps_r[0], eps_m[0]), min(eps_r[-1], eps_m[-1])
+    sel = (eps_r >= lo) & (eps_r <= hi)
+    dev = np.abs(np.interp(eps_r[sel], eps_m, sig_m) - sig_r[sel]).max()
+    print(f"\nBrazilian elastic, seed {seed}: {out.N} spheres, record deviation {dev / sig_r.max() * 100:.3f}% of "
+          f"peak, final stress {sig_m[-1]:.5g} vs {sig_r[-1]:.5g} GPa")
+    assert dev <= 0.02 * sig_r.max(), (dev, sig_r.max())
+    assert abs(sig_m[-1] - sig_r[-1]) <= 0.01 * sig_r[-1], (sig_m[-1], sig_r[-1])

@@ -1,8 +1,8 @@
 """Benchmark of the bonded-particle DEM step (BPM + Hertz-Mindlin) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload brazilian_disc|uniaxial_cylinder|calibration_sweep|
-                                calibration_solves|surrogate]
+                    [--workload brazilian_disc|brazilian_disc_postpeak|uniaxial_cylinder|
+                                calibration_sweep|calibration_solves|surrogate]
 
 A step is one DEM time step of a loading test (pair forces, platens,
 integration, loading controller; contact-list rebuilds when needed) over the
@@ -619,6 +619,81 @@ def run_solves(args, ws, rank, local):
     return 0
 
 
+def run_postpeak(args, ws, rank, local):
+    """The default workload's discs loaded past the peak first: platens at
+    ten times the configuration's speed, no stop condition, until every disc
+    has lost `--damage` of its bonds; then the timed steps, where broken
+    bonds and new touching pairs make the Hertz-Mindlin contacts and the
+    contact-list rebuilds part of every step.  Every rank loads its own discs
+    (weak scaling)."""
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    D = Dist(ws)
+    specs = [build_specimen(dem, "brazilian_disc", sd, local) for sd in specimen_seeds(args, rank)]
+    ctx = dem.Context(precision=args.precision, device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
+                      deterministic=args.deterministic, skin_factor=args.skin)
+    sids = []
+    for sp in specs:
+        ld = dem.Loading.from_buffer_copy(sp.loading)
+        ld.velocity *= 10.0
+        ld.min_stress = 1.0                      # 1 GPa: the fracture test never arms
+        ld.max_strain = 0.5
+        sids.append(ctx.add_sample(sp.material, ld, sp.xyz, sp.radii))
+    ctx.setup()
+    t0 = time.perf_counter()
+    prep = 0
+    while prep < 400000:
+        ctx.step(5000)
+        prep += 5000
+        res = [ctx.result(s) for s in sids]
+        if all(r["bonds_now"] <= (1.0 - args.damage) * r["bonds_initial"] for r in res):
+            break
+    t_prep = time.perf_counter() - t0
+    cnt = ctx.counts()
+    n_gpu = cnt["particles"]
+    ctx.run_timed(args.warmup)
+    rb0 = ctx.result(sids[0])["rebuilds"]
+    D.barrier()
+    clk = Clocks(local)
+    ms = ctx.run_timed(args.steps)
+    clocks = clk.stop()
+    D.barrier()
+    rb1 = ctx.result(sids[0])["rebuilds"]
+    ms_max = D.max(ms)
+    value = D.sum(float(n_gpu)) * args.steps / (ms_max * 1e-3)
+    prof = ctx.profile(min(args.steps, 300))
+    res = [ctx.result(s) for s in sids]
+    cnt = ctx.counts()
+    ctx.close()
+    bonds = sum(r["bonds_now"] for r in res)
+    A = algorithmic_bytes(n_gpu, bonds, prof["touching"], fp64=args.precision == 1)
+    achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == 1 else "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
+        "config": {"workload": f"{args.specimens} x brazilian_disc loaded past the peak ({args.damage:.0%} of the "
+                               f"bonds broken)", "particles_per_gpu": n_gpu, "specimens": args.specimens,
+                   "seeds": specimen_seeds(args, 0), "parallelism": f"{ws} GPU(s), independent specimens",
+                   "l2": "inputs larger than L2, no flush"},
+        "details": {"bonds_intact": bonds, "bonds_initial": sum(r["bonds_initial"] for r in res),
+                    "contacts_listed": cnt["contacts"], "touching_contacts": prof["touching"],
+                    "contact_list_builds_timed": rb1 - rb0, "preparation_steps": prep,
+                    "preparation_seconds_untimed": t_prep, "stale_lists": sum(r["stale"] for r in res),
+                    "done": [r["done"] for r in res]},
+        "gpu_launches": None, "clocks": clocks,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
+                     "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
+                     "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
+        "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -626,8 +701,10 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brazilian_disc",
-                    choices=["brazilian_disc", "uniaxial_cylinder", "calibration_sweep", "calibration_solves",
-                             "surrogate"])
+                    choices=["brazilian_disc", "brazilian_disc_postpeak", "uniaxial_cylinder", "calibration_sweep",
+                             "calibration_solves", "surrogate"])
+    ap.add_argument("--damage", type=float, default=0.03,
+                    help="brazilian_disc_postpeak: fraction of the bonds broken before the timed steps")
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
@@ -646,6 +723,11 @@ def main() -> int:
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
     if args.impl == "reference":
+        if args.workload not in ("brazilian_disc", "uniaxial_cylinder"):
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"the reference leg times the loop body on the "
+                                  f"specimen workloads only, not {args.workload}"}), flush=True)
+            return 0
         return run_reference(args, ws, rank, local)
     if args.workload == "calibration_sweep":
         return run_sweep(args, ws, rank, local)
@@ -653,6 +735,8 @@ def main() -> int:
         return run_surrogate(args, ws, rank, local)
     if args.workload == "calibration_solves":
         return run_solves(args, ws, rank, local)
+    if args.workload == "brazilian_disc_postpeak":
+        return run_postpeak(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")
     D = Dist(ws)
     specs = [build_specimen(dem, args.workload, sd, local) for sd in specimen_seeds(args, rank)]

@@ -26,6 +26,9 @@ struct RT<float> {
   static __device__ __forceinline__ float sqrt_rn(float x) { return __fsqrt_rn(x); }
   static __device__ __forceinline__ float rsqrt_rn(float x) { return __frsqrt_rn(x); }
   static __device__ __forceinline__ float fabs_(float x) { return fabsf(x); }
+  // a*b+c with one rounding (the contractions the bond kernel chooses; its
+  // CPU restatement uses fmaf at the same places)
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
   static constexpr float kPi = 3.14159265358979f;    // value of the reference's float pi
   static constexpr float kTwoThirds = 0.6666666667f;  // value of the reference's float 2/3
   static constexpr float kDamp = -1.8257f;
@@ -38,6 +41,7 @@ struct RT<double> {
   static __device__ __forceinline__ double sqrt_rn(double x) { return sqrt(x); }
   static __device__ __forceinline__ double rsqrt_rn(double x) { return 1.0 / sqrt(x); }
   static __device__ __forceinline__ double fabs_(double x) { return fabs(x); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
   static constexpr double kPi = 3.1415926535897932384626433832795;
   static constexpr double kTwoThirds = 2.0 / 3.0;
   static constexpr double kDamp = -1.8257;
@@ -58,6 +62,17 @@ __device__ __forceinline__ float norm3(float x, float y, float z) {
   return __double2float_rn(sqrt((dx * dx + dy * dy) + dz * dz));
 }
 __device__ __forceinline__ double norm3(double x, double y, double z) { return sqrt((x * x + y * y) + z * z); }
+
+// Norm of a history vector for the bond-break test, in the working precision:
+// sqrt(z*z + (y*y + x*x)) with the sums fused into the products.  The
+// reference's norm3df is not correctly rounded either; a threshold test
+// cannot tell the two apart except at exact ties.
+__device__ __forceinline__ float norm3_hist(float x, float y, float z) {
+  return __fsqrt_rn(__fmaf_rn(z, z, __fmaf_rn(y, y, x * x)));
+}
+__device__ __forceinline__ double norm3_hist(double x, double y, double z) {
+  return sqrt(__fma_rn(z, z, __fma_rn(y, y, x * x)));
+}
 
 // 128-bit (float) / 256-bit (double) vector loads and stores through the
 // read-only / default paths.

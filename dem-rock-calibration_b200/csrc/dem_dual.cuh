@@ -154,6 +154,7 @@ struct RT<Dual<K>> {
   static __host__ __device__ Dual<K> sqrt_rn(const Dual<K>& x) { return sqrt(x); }
   static __host__ __device__ Dual<K> rsqrt_rn(const Dual<K>& x) { return 1.0 / sqrt(x); }
   static __host__ __device__ Dual<K> fabs_(const Dual<K>& x) { return fabs(x); }
+  static __host__ __device__ Dual<K> fma(const Dual<K>& a, const Dual<K>& b, const Dual<K>& c) { return a * b + c; }
   static constexpr double kPi = 3.1415926535897932384626433832795;
   static constexpr double kTwoThirds = 2.0 / 3.0;
   static constexpr double kDamp = -1.8257;
@@ -210,6 +211,10 @@ __device__ __forceinline__ Dual4<K> unfix4(const Dual4<K>& a) {
 }
 template <int K>
 __host__ __device__ __forceinline__ Dual<K> norm3(const Dual<K>& x, const Dual<K>& y, const Dual<K>& z) {
+  return sqrt((x * x + y * y) + z * z);
+}
+template <int K>
+__host__ __device__ __forceinline__ Dual<K> norm3_hist(const Dual<K>& x, const Dual<K>& y, const Dual<K>& z) {
   return sqrt((x * x + y * y) + z * z);
 }
 

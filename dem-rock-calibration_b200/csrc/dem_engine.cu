@@ -913,10 +913,7 @@ class Engine final : public EngineBase {
   // the captured graph and the bond-tile list (tiles are blocks).
   int set_pair_config(uint32_t min_blocks) {
     constexpr bool kSmallBlocks = sizeof(Real) == 4 && !DualK<Real>::K;
-    // FP32: 9..12 select the pipelined-gather kernel with 5..8 blocks of 128
-    // threads (float atomics; deterministic contexts take the plain variant)
-    if (kSmallBlocks && min_blocks >= 9 && min_blocks <= 12 && det_) min_blocks -= 4;
-    if (min_blocks == 0 || min_blocks > (kSmallBlocks ? 12u : 4u))
+    if (min_blocks == 0 || min_blocks > (kSmallBlocks ? 8u : 4u))
       min_blocks = DualK<Real>::K ? 1 : (sizeof(Real) == 4 ? 7 : 2);
     opt_.pair_min_blocks = min_blocks;
     opt_.pair_block = min_blocks > 4 ? 128 : 256;
@@ -944,7 +941,7 @@ class Engine final : public EngineBase {
     if (DualK<Real>::K)
       pairs = {1, 2};
     else if (sizeof(Real) == 4)
-      pairs = det_ ? std::vector<uint32_t>{7, 3, 6, 5, 4} : std::vector<uint32_t>{7, 11, 10, 12, 6, 3};
+      pairs = {7, 3, 6, 5, 4};
     else
       pairs = {2, 1, 3};
     const uint32_t parts[2] = {256, 128};
@@ -1057,10 +1054,6 @@ class Engine final : public EngineBase {
         case 6: return (const void*)k_pairs<Real, 6, 128>;
         case 7: return (const void*)k_pairs<Real, 7, 128>;
         case 8: return (const void*)k_pairs<Real, 8, 128>;
-        case 9: return (const void*)k_pairs_async<5>;
-        case 10: return (const void*)k_pairs_async<6>;
-        case 11: return (const void*)k_pairs_async<7>;
-        case 12: return (const void*)k_pairs_async<8>;
         default: break;
       }
     }

@@ -443,6 +443,9 @@ __device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b
   const Real rijm = norm3(rx, ry, rz);
   Real ox = s0.w, oy = s1.x, oz = s1.y;
   if (intact) {
+    // The reference's operation order (dd_*_bpm_2, md_calculateforcesdem3.cu:41-200)
+    // with chosen products fused into their sums (T::fma, one rounding); the CPU
+    // oracle fuses the same ones, so both stay identical bit for bit.
     const Real one = Real(1), half = Real(0.5), dt = sp.dt, E = sp.E, G = sp.G, pi_ = T::kPi;
     const Real il = par.x, br = par.w;
     const Real rinv = T::rcp(rijm);
@@ -453,55 +456,56 @@ __device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b
     cef *= br * br * pi_;
     const Real fn0 = n0 * cef, fn1 = n1 * cef, fn2 = n2 * cef;
     // incremental rotation (dd_Calculate_M123_bpm_2)
-    const Real tp0 = s0.y * n2 - s0.z * n1, tp1 = s0.z * n0 - s0.x * n2, tp2 = s0.x * n1 - s0.y * n0;
-    cef = ((wj.x + wi.x) * n0 + (wj.y + wi.y) * n1 + (wj.z + wi.z) * n2) * dt * half;
+    const Real tp0 = T::fma(s0.y, n2, -(s0.z * n1)), tp1 = T::fma(s0.z, n0, -(s0.x * n2)),
+               tp2 = T::fma(s0.x, n1, -(s0.y * n0));
+    cef = T::fma(wj.z + wi.z, n2, T::fma(wj.y + wi.y, n1, (wj.x + wi.x) * n0)) * dt * half;
     const Real ph0 = n0 * cef, ph1 = n1 * cef, ph2 = n2 * cef;
     s0.x = n0;
     s0.y = n1;
     s0.z = n2;
-    const Real M10 = one + tp2 * ph2 + tp1 * ph1;
-    const Real M11 = ph2 - tp2 - tp1 * ph0;
-    const Real M12 = -ph1 - tp2 * ph0 + tp1;
-    const Real M20 = tp2 - ph2 - tp0 * ph1;
-    const Real M21 = tp2 * ph2 + one + tp0 * ph0;
-    const Real M22 = -tp2 * ph1 + ph0 - tp0;
-    const Real M30 = -tp1 - tp0 * ph2 + ph1;
-    const Real M31 = -tp1 * ph2 + tp0 - ph0;
-    const Real M32 = tp1 * ph1 + tp0 * ph0 + one;
+    const Real M10 = T::fma(tp1, ph1, T::fma(tp2, ph2, one));
+    const Real M11 = T::fma(-tp1, ph0, ph2 - tp2);
+    const Real M12 = T::fma(-tp2, ph0, -ph1) + tp1;
+    const Real M20 = T::fma(-tp0, ph1, tp2 - ph2);
+    const Real M21 = T::fma(tp0, ph0, T::fma(tp2, ph2, one));
+    const Real M22 = T::fma(-tp2, ph1, ph0) - tp0;
+    const Real M30 = T::fma(-tp0, ph2, -tp1) + ph1;
+    const Real M31 = T::fma(-tp1, ph2, tp0) - ph0;
+    const Real M32 = T::fma(tp0, ph0, tp1 * ph1) + one;
     // twisting moment (dd_Calculate_mijn_bpm_2)
     const Real dwx = wj.x - wi.x, dwy = wj.y - wi.y, dwz = wj.z - wi.z;
-    const Real wn = n0 * dwx + n1 * dwy + n2 * dwz;
+    const Real wn = T::fma(n2, dwz, T::fma(n1, dwy, n0 * dwx));
     Real cef1 = wn * (dt * half * G * il);
     const Real Nx = s1.z, Ny = s1.w, Nz = s2.x;
-    const Real mn0 = M10 * Nx + M11 * Ny + M12 * Nz + n0 * cef1;
-    const Real mn1 = M20 * Nx + M21 * Ny + M22 * Nz + n1 * cef1;
-    const Real mn2 = M30 * Nx + M31 * Ny + M32 * Nz + n2 * cef1;
+    const Real mn0 = T::fma(n0, cef1, T::fma(M12, Nz, T::fma(M11, Ny, M10 * Nx)));
+    const Real mn1 = T::fma(n1, cef1, T::fma(M22, Nz, T::fma(M21, Ny, M20 * Nx)));
+    const Real mn2 = T::fma(n2, cef1, T::fma(M32, Nz, T::fma(M31, Ny, M30 * Nx)));
     cef1 = pi_ * br * br * br * br;
     const Real tn0 = mn0 * cef1, tn1 = mn1 * cef1, tn2 = mn2 * cef1;
     // bending moment (dd_Calculate_mijt_bpm_2)
     Real cef2 = dt * Real(0.25) * E * il;
     const Real Tx = s2.y, Ty = s2.z, Tz = s2.w;
-    const Real mt0 = M10 * Tx + M11 * Ty + M12 * Tz + (dwx - n0 * wn) * cef2;
-    const Real mt1 = M20 * Tx + M21 * Ty + M22 * Tz + (dwy - n1 * wn) * cef2;
-    const Real mt2 = M30 * Tx + M31 * Ty + M32 * Tz + (dwz - n2 * wn) * cef2;
+    const Real mt0 = T::fma(T::fma(-n0, wn, dwx), cef2, T::fma(M12, Tz, T::fma(M11, Ty, M10 * Tx)));
+    const Real mt1 = T::fma(T::fma(-n1, wn, dwy), cef2, T::fma(M22, Tz, T::fma(M21, Ty, M20 * Tx)));
+    const Real mt2 = T::fma(T::fma(-n2, wn, dwz), cef2, T::fma(M32, Tz, T::fma(M31, Ty, M30 * Tx)));
     cef2 *= pi_ * br * br * br * br;
     const Real tt0 = mt0 * cef2, tt1 = mt1 * cef2, tt2 = mt2 * cef2;
     // shear force and unsymmetric moment (dd_Calculate_fijt_mijunsym_bpm_2)
     const Real ws0 = half * (wj.x + wi.x), ws1 = half * (wj.y + wi.y), ws2 = half * (wj.z + wi.z);
-    const Real v0 = vj.x - vi.x - ws1 * rz + ws2 * ry;
-    const Real v1 = vj.y - vi.y - ws2 * rx + ws0 * rz;
-    const Real v2 = vj.z - vi.z - ws0 * ry + ws1 * rx;
-    cef = n0 * v0 + n1 * v1 + n2 * v2;
-    const Real ot0 = (M10 * ox + M11 * oy + M12 * oz) + (v0 - n0 * cef) * dt;
-    const Real ot1 = (M20 * ox + M21 * oy + M22 * oz) + (v1 - n1 * cef) * dt;
-    const Real ot2 = (M30 * ox + M31 * oy + M32 * oz) + (v2 - n2 * cef) * dt;
+    const Real v0 = T::fma(ws2, ry, T::fma(-ws1, rz, vj.x - vi.x));
+    const Real v1 = T::fma(ws0, rz, T::fma(-ws2, rx, vj.y - vi.y));
+    const Real v2 = T::fma(ws1, rx, T::fma(-ws0, ry, vj.z - vi.z));
+    cef = T::fma(n2, v2, T::fma(n1, v1, n0 * v0));
+    const Real ot0 = T::fma(T::fma(-n0, cef, v0), dt, T::fma(M12, oz, T::fma(M11, oy, M10 * ox)));
+    const Real ot1 = T::fma(T::fma(-n1, cef, v1), dt, T::fma(M22, oz, T::fma(M21, oy, M20 * ox)));
+    const Real ot2 = T::fma(T::fma(-n2, cef, v2), dt, T::fma(M32, oz, T::fma(M31, oy, M30 * ox)));
     cef = G * il;
     Real Mc = cef;
     cef *= br * br * pi_;
     const Real ft0 = ot0 * cef, ft1 = ot1 * cef, ft2 = ot2 * cef;
-    const Real mu0 = half * (ry * ot2 - rz * ot1) * cef;
-    const Real mu1 = half * (rz * ot0 - rx * ot2) * cef;
-    const Real mu2 = half * (rx * ot1 - ry * ot0) * cef;
+    const Real mu0 = half * T::fma(ry, ot2, -(rz * ot1)) * cef;
+    const Real mu1 = half * T::fma(rz, ot0, -(rx * ot2)) * cef;
+    const Real mu2 = half * T::fma(rx, ot1, -(ry * ot0)) * cef;
     // contributions: i gets (F, Mn+Mt+Mu), j gets (-F, -(Mn+Mt)+Mu)
     scatter_j_warp<Real, kDetJ>(A, j, -(fn0 + ft0), -(fn1 + ft1), -(fn2 + ft2), mu0 - (tn0 + tt0), mu1 - (tn1 + tt1),
                          mu2 - (tn2 + tt2));
@@ -510,9 +514,9 @@ __device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b
     // break test (dd_CheckBreakConditionDEM_2)
     bool broke = false;
     if (!sp.nobreak) {
-      Mc *= norm3(ot0, ot1, ot2);
-      Sc += norm3(mt0, mt1, mt2) * Real(4) * br;
-      Mc += norm3(mn0, mn1, mn2) * Real(2) * br;
+      Mc *= norm3_hist(ot0, ot1, ot2);
+      Sc += norm3_hist(mt0, mt1, mt2) * Real(4) * br;
+      Mc += norm3_hist(mn0, mn1, mn2) * Real(2) * br;
       broke = (Sc > par.y) || (Mc > par.z);
     }
     if (!broke) {
@@ -640,113 +644,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs(StepArgs<Real> A) 
   }
   const uint32_t nc = *A.nc;
   for (uint32_t c = blockIdx.x * tile + threadIdx.x; c < nc; c += stride) do_contact<Real>(A, c);
-}
-
-// 16-byte asynchronous copy global -> shared (cp.async, L1-allocating), and
-// its group fences.  Each thread waits only for its own copies.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// FP32 pair kernel with the particle gathers of the next bond tile in flight
-// while the current one is computed.  Every thread copies the six particle
-// vectors of its next bond (position, velocity, spin of both ends: 96 bytes)
-// into its own slots of a two-stage shared-memory buffer with cp.async, then
-// waits only for the stage of the current bond: no block or warp barrier (a
-// thread reads only what it copied itself), so each warp runs its own
-// pipeline.  The pair indices run one more tile ahead, so that the copies of
-// the next tile can be issued at the top of an iteration without an index
-// round trip; the bond state itself streams through L2 (bulk prefetch of the
-// next tile, evict-first loads).  Float atomics only (deterministic contexts
-// use k_pairs).
-template <int kMinBlocks, int kBlock = 128>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_async(StepArgs<float> A) {
-  __shared__ float4 g[2][6][kBlock];   // stage, (pos i, pos j, vel i, vel j, spin i, spin j), thread
-  const uint32_t nb = A.nb, tid = threadIdx.x;
-  const uint32_t tile = kBlock;
-  const uint32_t ntl = A.tiles ? *A.ntiles : (nb + tile - 1) / tile;
-  auto tile_base = [&](uint32_t k) { return (A.tiles ? A.tiles[k] : k) * tile; };
-  auto issue = [&](uint32_t stage, uint2 ij) {
-    cp_async16(&g[stage][0][tid], A.pos + ij.x);
-    cp_async16(&g[stage][1][tid], A.pos + ij.y);
-    cp_async16(&g[stage][2][tid], A.vel + ij.x);
-    cp_async16(&g[stage][3][tid], A.vel + ij.y);
-    cp_async16(&g[stage][4][tid], A.omg + ij.x);
-    cp_async16(&g[stage][5][tid], A.omg + ij.y);
-  };
-  uint32_t k = blockIdx.x;
-  uint32_t base = 0, ts = ~0u;
-  uint2 ij = make_uint2(0, 0);
-  bool have = false;
-  if (k < ntl) {
-    base = tile_base(k);
-    if (A.tile_s) ts = __ldg(A.tile_s + base / tile);
-    have = base + tid < nb;
-    if (have) {
-      ij = __ldcs(A.b_ij + base + tid);
-      issue(0, ij);
-    }
-  }
-  cp_async_commit();
-  // pair indices of the next tile
-  uint32_t kn = k + gridDim.x, nbase = 0, nts = ~0u;
-  uint2 nij = make_uint2(0, 0);
-  bool nhave = false;
-  if (kn < ntl) {
-    nbase = tile_base(kn);
-    if (A.tile_s) nts = __ldg(A.tile_s + nbase / tile);
-    nhave = nbase + tid < nb;
-    if (nhave) nij = __ldcs(A.b_ij + nbase + tid);
-  }
-  uint32_t stage = 0;
-  for (; k < ntl; k += gridDim.x) {
-    // copies of the next tile into the other stage (an empty group past the end)
-    if (nhave) issue(stage ^ 1u, nij);
-    cp_async_commit();
-    // pair indices of the tile after it, and the next tile's bond state into L2
-    const uint32_t knn = kn + gridDim.x;
-    uint32_t nnbase = 0, nnts = ~0u;
-    uint2 nnij = make_uint2(0, 0);
-    bool nnhave = false;
-    if (knn < ntl) {
-      nnbase = tile_base(knn);
-      if (A.tile_s) nnts = __ldg(A.tile_s + nnbase / tile);
-      nnhave = nnbase + tid < nb;
-      if (nnhave) nnij = __ldcs(A.b_ij + nnbase + tid);
-    }
-    if (kn < ntl && tid == 0) {
-      l2_prefetch(A.b_par + nbase, tile * sizeof(float4));
-      l2_prefetch(A.b_s0 + nbase, tile * sizeof(float4));
-      l2_prefetch(A.b_s1 + nbase, tile * sizeof(float4));
-      l2_prefetch(A.b_s2 + nbase, tile * sizeof(float4));
-    }
-    if (have) {
-      const uint32_t b = base + tid;
-      const float4 par = ld4_cs(A.b_par + b), s0 = ld4_cs(A.b_s0 + b), s1 = ld4_cs(A.b_s1 + b),
-                   s2 = ld4_cs(A.b_s2 + b);
-      cp_async_wait_all_but_one();   // this tile's copies (the next tile's may still fly)
-      const float4 pi = g[stage][0][tid], pj = g[stage][1][tid], vi = g[stage][2][tid], vj = g[stage][3][tid],
-                   wi = g[stage][4][tid], wj = g[stage][5][tid];
-      do_bond_core<float, false>(A, b, ij, par, s0, s1, s2, ts, pi, pj, vi, vj, wi, wj);
-    }
-    stage ^= 1u;
-    base = nbase;
-    ts = nts;
-    ij = nij;
-    have = nhave;
-    kn = knn;
-    nbase = nnbase;
-    nts = nnts;
-    nij = nnij;
-    nhave = nnhave;
-  }
-  cp_async_wait_all();
-  const uint32_t nc = *A.nc;
-  for (uint32_t c = blockIdx.x * tile + tid; c < nc; c += gridDim.x * tile) do_contact<float>(A, c);
 }
 
 // Particle-platen contact (dd_Calculate_fijn_pwHM_2 + dd_Calculate_fijtmijt_pwHM_2,

@@ -60,16 +60,13 @@ typedef struct dem_ctx dem_ctx;
 typedef struct {
   int precision;          /* 0: FP32, 1: FP64, 2: FP64 with tangents (dem_sensitivities) */
   int device;             /* CUDA device ordinal */
-  uint32_t pair_block;    /* ignored: set from pair_min_blocks (256 threads, 128 for 5..12) */
+  uint32_t pair_block;    /* ignored: set from pair_min_blocks (256 threads, 128 for 5..8) */
   uint32_t pair_grid;     /* blocks of the pair kernel (0: all co-resident blocks) */
   uint32_t particle_block;/* threads per block of the particle kernel (0: 256) */
   uint32_t graph_steps;   /* steps per captured CUDA graph (0: 100) */
   double skin_factor;     /* contact-list skin as a multiple of the smallest radius (0: 0.1) */
   uint32_t pair_min_blocks; /* register budget of the pair kernel: blocks per SM it must fit
-                               (1..4 of 256 threads, FP32 also 5..8 of 128 threads; FP32
-                               9..12: 5..8 blocks of 128 threads of the variant that copies
-                               the next bonds' particle states into shared memory while it
-                               computes the current ones, float sums only;
+                               (1..4 of 256 threads, FP32 also 5..8 of 128 threads;
                                0: 7 for FP32, 2 for FP64, 1 for the sensitivity build) */
   uint32_t deterministic; /* 1: FP32 force and platen sums in exact 64-bit fixed point
                              (2^-40 resolution), so a run is bit-reproducible and a

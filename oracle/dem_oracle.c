@@ -99,6 +99,7 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #define TWO_THIRDS 0.6666666667f /* MCf_2d3, md_math_constants.h:146 */
 #define DAMP (-1.8257f)
 #define SQRT sqrtf
+#define FMA fmaf
 #define FABS fabsf
 #define FLOOR floorf
 #define COPYSIGN copysignf
@@ -118,6 +119,7 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #undef TWO_THIRDS
 #undef DAMP
 #undef SQRT
+#undef FMA
 #undef FABS
 #undef FLOOR
 #undef COPYSIGN
@@ -138,6 +140,7 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #define TWO_THIRDS (2.0 / 3.0)
 #define DAMP (-1.8257)
 #define SQRT sqrt
+#define FMA fma
 #define FABS fabs
 #define FLOOR floor
 #define COPYSIGN copysign

@@ -253,36 +253,40 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       REAL rijm = NORM3(rx, ry, rz);
       REAL rinv = ONE / rijm;
       REAL n[3] = {rx * rinv, ry * rinv, rz * rinv};
-      /* dd_Calculate_fijn_bpm_2, dem3.cu:94-106 */
+      /* dd_Calculate_fijn_bpm_2, dem3.cu:94-106.  The reference's operation
+       * order; the products fused into their sums here (FMA, one rounding) are
+       * the ones the CUDA product fuses, so the two agree bit for bit. */
       REAL cef = E * (rijm - ONE / il) * il;
       REAL Sc = cef;
       cef *= b_r * b_r * PI;
       REAL fn[3] = {n[0] * cef, n[1] * cef, n[2] * cef};
       for (int d = 0; d < 3; ++d) fs[d] += fn[d];
       /* dd_Calculate_M123_bpm_2, dem3.cu:57-92 */
-      REAL tmp[3] = {Rk[1] * n[2] - Rk[2] * n[1], Rk[2] * n[0] - Rk[0] * n[2], Rk[0] * n[1] - Rk[1] * n[0]};
-      cef = ((Wj[0] + Wi[0]) * n[0] + (Wj[1] + Wi[1]) * n[1] + (Wj[2] + Wi[2]) * n[2]) * dt * HALF;
+      REAL tmp[3] = {FMA(Rk[1], n[2], -(Rk[2] * n[1])), FMA(Rk[2], n[0], -(Rk[0] * n[2])),
+                     FMA(Rk[0], n[1], -(Rk[1] * n[0]))};
+      cef = FMA(Wj[2] + Wi[2], n[2], FMA(Wj[1] + Wi[1], n[1], (Wj[0] + Wi[0]) * n[0])) * dt * HALF;
       REAL phi[3] = {n[0] * cef, n[1] * cef, n[2] * cef};
       Rk[0] = n[0];
       Rk[1] = n[1];
       Rk[2] = n[2];
       REAL M1[3], M2[3], M3[3];
-      M1[0] = ONE + tmp[2] * phi[2] + tmp[1] * phi[1];
-      M1[1] = phi[2] - tmp[2] - tmp[1] * phi[0];
-      M1[2] = -phi[1] - tmp[2] * phi[0] + tmp[1];
-      M2[0] = tmp[2] - phi[2] - tmp[0] * phi[1];
-      M2[1] = tmp[2] * phi[2] + ONE + tmp[0] * phi[0];
-      M2[2] = -tmp[2] * phi[1] + phi[0] - tmp[0];
-      M3[0] = -tmp[1] - tmp[0] * phi[2] + phi[1];
-      M3[1] = -tmp[1] * phi[2] + tmp[0] - phi[0];
-      M3[2] = tmp[1] * phi[1] + tmp[0] * phi[0] + ONE;
+      M1[0] = FMA(tmp[1], phi[1], FMA(tmp[2], phi[2], ONE));
+      M1[1] = FMA(-tmp[1], phi[0], phi[2] - tmp[2]);
+      M1[2] = FMA(-tmp[2], phi[0], -phi[1]) + tmp[1];
+      M2[0] = FMA(-tmp[0], phi[1], tmp[2] - phi[2]);
+      M2[1] = FMA(tmp[0], phi[0], FMA(tmp[2], phi[2], ONE));
+      M2[2] = FMA(-tmp[2], phi[1], phi[0]) - tmp[0];
+      M3[0] = FMA(-tmp[0], phi[2], -tmp[1]) + phi[1];
+      M3[1] = FMA(-tmp[1], phi[2], tmp[0]) - phi[0];
+      M3[2] = FMA(tmp[0], phi[0], tmp[1] * phi[1]) + ONE;
       /* dd_Calculate_mijn_bpm_2, dem3.cu:108-132 */
-      REAL cef1 = n[0] * (Wj[0] - Wi[0]) + n[1] * (Wj[1] - Wi[1]) + n[2] * (Wj[2] - Wi[2]);
-      cef1 *= dt * HALF * G * il;
+      const REAL dw[3] = {Wj[0] - Wi[0], Wj[1] - Wi[1], Wj[2] - Wi[2]};
+      const REAL wn = FMA(n[2], dw[2], FMA(n[1], dw[1], n[0] * dw[0]));
+      REAL cef1 = wn * (dt * HALF * G * il);
       REAL mn[3];
-      mn[0] = M1[0] * Nk[0] + M1[1] * Nk[1] + M1[2] * Nk[2] + n[0] * cef1;
-      mn[1] = M2[0] * Nk[0] + M2[1] * Nk[1] + M2[2] * Nk[2] + n[1] * cef1;
-      mn[2] = M3[0] * Nk[0] + M3[1] * Nk[1] + M3[2] * Nk[2] + n[2] * cef1;
+      mn[0] = FMA(n[0], cef1, FMA(M1[2], Nk[2], FMA(M1[1], Nk[1], M1[0] * Nk[0])));
+      mn[1] = FMA(n[1], cef1, FMA(M2[2], Nk[2], FMA(M2[1], Nk[1], M2[0] * Nk[0])));
+      mn[2] = FMA(n[2], cef1, FMA(M3[2], Nk[2], FMA(M3[1], Nk[1], M3[0] * Nk[0])));
       Nk[0] = mn[0];
       Nk[1] = mn[1];
       Nk[2] = mn[2];
@@ -290,12 +294,11 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       REAL tn[3] = {mn[0] * cef1, mn[1] * cef1, mn[2] * cef1};
       for (int d = 0; d < 3; ++d) ms[d] += tn[d];
       /* dd_Calculate_mijt_bpm_2, dem3.cu:134-155 */
-      cef1 = n[0] * (Wj[0] - Wi[0]) + n[1] * (Wj[1] - Wi[1]) + n[2] * (Wj[2] - Wi[2]);
       REAL cef2 = dt * QUARTER * E * il;
       REAL mt[3];
-      mt[0] = M1[0] * Tk[0] + M1[1] * Tk[1] + M1[2] * Tk[2] + (Wj[0] - Wi[0] - n[0] * cef1) * cef2;
-      mt[1] = M2[0] * Tk[0] + M2[1] * Tk[1] + M2[2] * Tk[2] + (Wj[1] - Wi[1] - n[1] * cef1) * cef2;
-      mt[2] = M3[0] * Tk[0] + M3[1] * Tk[1] + M3[2] * Tk[2] + (Wj[2] - Wi[2] - n[2] * cef1) * cef2;
+      mt[0] = FMA(FMA(-n[0], wn, dw[0]), cef2, FMA(M1[2], Tk[2], FMA(M1[1], Tk[1], M1[0] * Tk[0])));
+      mt[1] = FMA(FMA(-n[1], wn, dw[1]), cef2, FMA(M2[2], Tk[2], FMA(M2[1], Tk[1], M2[0] * Tk[0])));
+      mt[2] = FMA(FMA(-n[2], wn, dw[2]), cef2, FMA(M3[2], Tk[2], FMA(M3[1], Tk[1], M3[0] * Tk[0])));
       Tk[0] = mt[0];
       Tk[1] = mt[1];
       Tk[2] = mt[2];
@@ -305,14 +308,14 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       /* dd_Calculate_fijt_mijunsym_bpm_2, dem3.cu:157-200 */
       REAL wsd[3] = {HALF * (Wj[0] + Wi[0]), HALF * (Wj[1] + Wi[1]), HALF * (Wj[2] + Wi[2])};
       REAL vij[3];
-      vij[0] = Vj[0] - Vi[0] - wsd[1] * rz + wsd[2] * ry;
-      vij[1] = Vj[1] - Vi[1] - wsd[2] * rx + wsd[0] * rz;
-      vij[2] = Vj[2] - Vi[2] - wsd[0] * ry + wsd[1] * rx;
-      cef = n[0] * vij[0] + n[1] * vij[1] + n[2] * vij[2];
+      vij[0] = FMA(wsd[2], ry, FMA(-wsd[1], rz, Vj[0] - Vi[0]));
+      vij[1] = FMA(wsd[0], rz, FMA(-wsd[2], rx, Vj[1] - Vi[1]));
+      vij[2] = FMA(wsd[1], rx, FMA(-wsd[0], ry, Vj[2] - Vi[2]));
+      cef = FMA(n[2], vij[2], FMA(n[1], vij[1], n[0] * vij[0]));
       REAL ot[3];
-      ot[0] = (M1[0] * Ok[0] + M1[1] * Ok[1] + M1[2] * Ok[2]) + (vij[0] - n[0] * cef) * dt;
-      ot[1] = (M2[0] * Ok[0] + M2[1] * Ok[1] + M2[2] * Ok[2]) + (vij[1] - n[1] * cef) * dt;
-      ot[2] = (M3[0] * Ok[0] + M3[1] * Ok[1] + M3[2] * Ok[2]) + (vij[2] - n[2] * cef) * dt;
+      ot[0] = FMA(FMA(-n[0], cef, vij[0]), dt, FMA(M1[2], Ok[2], FMA(M1[1], Ok[1], M1[0] * Ok[0])));
+      ot[1] = FMA(FMA(-n[1], cef, vij[1]), dt, FMA(M2[2], Ok[2], FMA(M2[1], Ok[1], M2[0] * Ok[0])));
+      ot[2] = FMA(FMA(-n[2], cef, vij[2]), dt, FMA(M3[2], Ok[2], FMA(M3[1], Ok[1], M3[0] * Ok[0])));
       cef = G * il;
       REAL Mc = cef;
       cef *= b_r * b_r * PI;
@@ -322,9 +325,9 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       Ok[1] = ot[1];
       Ok[2] = ot[2];
       REAL mu[3];
-      mu[0] = HALF * (ry * ot[2] - rz * ot[1]) * cef;
-      mu[1] = HALF * (rz * ot[0] - rx * ot[2]) * cef;
-      mu[2] = HALF * (rx * ot[1] - ry * ot[0]) * cef;
+      mu[0] = HALF * FMA(ry, ot[2], -(rz * ot[1])) * cef;
+      mu[1] = HALF * FMA(rz, ot[0], -(rx * ot[2])) * cef;
+      mu[2] = HALF * FMA(rx, ot[1], -(ry * ot[0])) * cef;
       for (int d = 0; d < 3; ++d) ms[d] += mu[d];
       if (Fabs)
         for (int d = 0; d < 3; ++d) fa[d] += FABS(fn[d]) + FABS(ft[d]);
@@ -334,9 +337,11 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       if (Fsens) fsens += (double)(E * (b_r * b_r * PI) * il) * (double)ULP(rijm);
       /* dd_CheckBreakConditionDEM_2, dem3.cu:20-39 */
       if (!nobreak) {
-        Mc *= NORM3(Ok[0], Ok[1], Ok[2]);
-        Sc += NORM3(Tk[0], Tk[1], Tk[2]) * FOUR * b_r;
-        Mc += NORM3(Nk[0], Nk[1], Nk[2]) * TWO * b_r;
+        /* history norms: sqrt(z*z + (y*y + x*x)) with fused sums (the
+         * reference's norm3df is not correctly rounded either) */
+        Mc *= SQRT(FMA(Ok[2], Ok[2], FMA(Ok[1], Ok[1], Ok[0] * Ok[0])));
+        Sc += SQRT(FMA(Tk[2], Tk[2], FMA(Tk[1], Tk[1], Tk[0] * Tk[0]))) * FOUR * b_r;
+        Mc += SQRT(FMA(Nk[2], Nk[2], FMA(Nk[1], Nk[1], Nk[0] * Nk[0]))) * TWO * b_r;
         if ((Sc > Ec) || (Mc > Gc)) {
           ILtype[kdx] = 0;
           for (int d = 0; d < 3; ++d) {

@@ -69,9 +69,8 @@ CASES = {
     "brazilian_bonds": ("brazilian", {}, (6e-4, 2e-4, 2e-3)),
     "uniaxial_contacts": ("uniaxial", {"gap": -1.0}, (3e-3, 5e-4, 5e-3)),
 }
-# precision, deterministic sums, pair-kernel variant (0: default; 11: FP32 with
-# the particle gathers pipelined through shared memory)
-MODES = {"fp32": (0, False, 0), "fp32_async": (0, False, 11), "fp32_det": (0, True, 0), "fp64": (1, False, 0)}
+# precision, deterministic sums, pair-kernel register budget (0: the default)
+MODES = {"fp32": (0, False, 0), "fp32_det": (0, True, 0), "fp64": (1, False, 0)}
 
 
 def _engine(sp, mat, precision, det, pair_min_blocks=0):

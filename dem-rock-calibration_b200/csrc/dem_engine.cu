@@ -386,22 +386,38 @@ class Engine final : public EngineBase {
     double lo[3] = {1e300, 1e300, 1e300};
     for (uint32_t i = 0; i < s.n; ++i)
       for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], (double)s.xyz[d * s.n + i]);
-    std::vector<std::pair<uint64_t, uint32_t>> key(s.n);
+    std::vector<uint64_t> key(s.n);
     for (uint32_t i = 0; i < s.n; ++i) {
       uint32_t c[3];
       for (int d = 0; d < 3; ++d) {
         double v = ((double)s.xyz[d * s.n + i] - lo[d]) / q;
         c[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
       }
-      key[i] = {morton3(c[0], c[1], c[2]), i};
+      key[i] = morton3(c[0], c[1], c[2]);
     }
-    std::stable_sort(key.begin(), key.end());
+    // stable LSD radix sort of the particle indices by key (16-bit digits over
+    // the 63 key bits): equal keys keep ascending index order
     s.perm.resize(s.n);
-    s.inv.resize(s.n);
-    for (uint32_t k = 0; k < s.n; ++k) {
-      s.perm[k] = key[k].second;
-      s.inv[key[k].second] = k;
+    std::vector<uint32_t> tmp(s.n);
+    for (uint32_t i = 0; i < s.n; ++i) s.perm[i] = i;
+    std::vector<uint32_t> count(65537);
+    for (int shift = 0; shift < 64; shift += 16) {
+      std::fill(count.begin(), count.end(), 0u);
+      for (uint32_t i = 0; i < s.n; ++i) ++count[((key[i] >> shift) & 0xFFFF) + 1];
+      bool one_bucket = false;
+      for (uint32_t b = 0; b < 65536; ++b) {
+        if (count[b + 1] == s.n) one_bucket = true;
+        count[b + 1] += count[b];
+      }
+      if (one_bucket) continue;   // this digit is the same for every key
+      for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t i = s.perm[k];
+        tmp[count[(key[i] >> shift) & 0xFFFF]++] = i;
+      }
+      s.perm.swap(tmp);
     }
+    s.inv.resize(s.n);
+    for (uint32_t k = 0; k < s.n; ++k) s.inv[s.perm[k]] = k;
   }
 
   static V4 make4(Real a, Real b, Real c, Real d) {

@@ -562,6 +562,66 @@ def run_surrogate(args, ws, rank, local):
     return 0
 
 
+def run_solves_cfg2(args, ws, rank, local):
+    """Calibration solves per hour at the batched configuration's sizes:
+    `cases` Latin-hypercube parameter sets over 16 packed cylinders of 5k-60k
+    spheres (case k on cylinder k mod 16), uniaxial tests to 70% post-peak
+    (or 1% strain), deterministic mode.  Batched: all cases in one context,
+    until the last one finishes.  Plain: one context per solve, one after
+    another, for one case per cylinder (16 solves covering the size range).
+    Wall-clock per whole solve (context, set-up, loading, results)."""
+    sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    D = Dist(ws)
+    max_steps = 2_000_000
+    sw = sweep.build_sweep(args.cases, sweep_sizes(16, 11 + rank), seed=1 + rank, max_steps=max_steps, device=local)
+
+    def solve(cases):
+        ctx = dem.Context(device=local, graph_steps=200, deterministic=True)
+        ids = [ctx.add_sample(c.material, c.loading, c.xyz, c.radii) for c in cases]
+        ctx.setup()
+        ctx.run(max_steps)
+        res = [ctx.result(i) for i in ids]
+        ctx.close()
+        return res
+
+    solve(sw.cases[:2])                                   # kernel loading, allocator warm-up
+    D.barrier()
+    clk = Clocks(local)
+    t0 = time.perf_counter()
+    res_b = solve(sw.cases)
+    t_b = time.perf_counter() - t0
+    clocks = clk.stop()
+    t_b = D.max(t_b)
+    plain_cases = sw.cases[:16]
+    t0 = time.perf_counter()
+    res_p = [solve([c])[0] for c in plain_cases]
+    t_p = time.perf_counter() - t0
+    agree = max(abs(a["FractureStress"] - b["FractureStress"]) / max(abs(b["FractureStress"]), 1e-30)
+                for a, b in zip(res_b[:16], res_p))
+    value = D.sum(float(len(sw.cases))) / t_b * 3600.0
+    plain = D.sum(len(plain_cases) / t_p * 3600.0)
+    steps = [r["steps"] for r in res_b]
+    line = {
+        "metric": "calibration solves/hour", "value": value, "unit": "solves/hour", "n_gpus": ws, "steps": 1,
+        "warmup": 1, "ms_per_step": t_b * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded packings, Latin-hypercube micro-parameters)",
+        "config": {"workload": f"{len(sw.cases)} uniaxial solves over 16 cylinders of 5k-60k spheres "
+                               f"({sw.particles} spheres in all) to 70% post-peak or 1% strain, one context",
+                   "step": "the whole batch of solves, wall-clock (context, set-up, loading, results)",
+                   "plain": {"solves": len(plain_cases), "seconds": t_p, "value": plain,
+                             "note": "one context per solve, one after another, one case per cylinder size"},
+                   "batched_over_plain": value / plain, "max_rel_difference_batched_vs_plain_ucs": agree,
+                   "solve_steps_range": [min(steps), max(steps)], "all_done": all(r["done"] for r in res_b),
+                   "l2": "state above the L2 (batch); no flush"},
+        "gpu_launches": None, "clocks": clocks, "roofline": None, "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+    return 0
+
+
 def run_solves(args, ws, rank, local):
     """Calibration solves per hour: `cases` uniaxial tests of one packed
     cylinder of about 2,000 spheres (Latin-hypercube micro-parameters over the
@@ -703,6 +763,8 @@ def main() -> int:
     ap.add_argument("--workload", default="brazilian_disc",
                     choices=["brazilian_disc", "brazilian_disc_postpeak", "uniaxial_cylinder", "calibration_sweep",
                              "calibration_solves", "surrogate"])
+    ap.add_argument("--solve-sizes", default="2000", choices=["2000", "cfg2"],
+                    help="calibration_solves: one 2,000-sphere cylinder, or 16 cylinders of 5k-60k spheres")
     ap.add_argument("--damage", type=float, default=0.03,
                     help="brazilian_disc_postpeak: fraction of the bonds broken before the timed steps")
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
@@ -734,7 +796,8 @@ def main() -> int:
     if args.workload == "surrogate":
         return run_surrogate(args, ws, rank, local)
     if args.workload == "calibration_solves":
-        return run_solves(args, ws, rank, local)
+        return run_solves_cfg2(args, ws, rank, local) if args.solve_sizes == "cfg2" else run_solves(args, ws, rank,
+                                                                                                    local)
     if args.workload == "brazilian_disc_postpeak":
         return run_postpeak(args, ws, rank, local)
     dem = importlib.import_module("dem-rock-calibration_b200")

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "dem_build.cuh"
@@ -77,6 +78,24 @@ struct DBuf {
 };
 
 static uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// fn(begin, end) over [0, n) split into contiguous ranges on up to 16 host
+// threads (set-up loops over hundreds of thousands of particles); fn must not
+// throw and its ranges must write disjoint data.
+template <class Fn>
+static void parallel_ranges(uint32_t n, Fn fn) {
+  const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const uint32_t T = std::max(1u, std::min(hw, n / 32768u));
+  if (T == 1) {
+    fn(0u, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(T);
+  for (uint32_t t = 0; t < T; ++t)
+    th.emplace_back(fn, (uint32_t)((uint64_t)n * t / T), (uint32_t)((uint64_t)n * (t + 1) / T));
+  for (auto& x : th) x.join();
+}
 
 // 30-bit Morton interleave of three 10-bit coordinates
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
@@ -187,19 +206,21 @@ class Engine final : public EngineBase {
     std::vector<uint32_t> hsid(np_), horig(np_);
     for (uint32_t si = 0; si < S; ++si) {
       const SampleHost& s = samples_[si];
-      for (uint32_t k = 0; k < s.n; ++k) {
-        const uint32_t q = s.perm[k];
-        const uint32_t p = s.p_begin + k;
-        const double r = s.rad[q];
-        double m, dtm, dtI;
-        particle_constants(r, s.pot.m_ro, s.dt, m, dtm, dtI);
-        hpos[p] = make4((Real)s.xyz[q], (Real)s.xyz[s.n + q], (Real)s.xyz[2 * s.n + q], (Real)s.rad[q]);
-        hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
-        homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
-        hmass[p] = (Real)m;
-        hsid[p] = si;
-        horig[p] = q;
-      }
+      parallel_ranges(s.n, [&](uint32_t k0, uint32_t k1) {
+        for (uint32_t k = k0; k < k1; ++k) {
+          const uint32_t q = s.perm[k];
+          const uint32_t p = s.p_begin + k;
+          const double r = s.rad[q];
+          double m, dtm, dtI;
+          particle_constants(r, s.pot.m_ro, s.dt, m, dtm, dtI);
+          hpos[p] = make4((Real)s.xyz[q], (Real)s.xyz[s.n + q], (Real)s.xyz[2 * s.n + q], (Real)s.rad[q]);
+          hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
+          homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
+          hmass[p] = (Real)m;
+          hsid[p] = si;
+          horig[p] = q;
+        }
+      });
     }
     CK(pos_.alloc(np_));
     CK(vel_.alloc(np_));
@@ -387,14 +408,16 @@ class Engine final : public EngineBase {
     for (uint32_t i = 0; i < s.n; ++i)
       for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], (double)s.xyz[d * s.n + i]);
     std::vector<uint64_t> key(s.n);
-    for (uint32_t i = 0; i < s.n; ++i) {
-      uint32_t c[3];
-      for (int d = 0; d < 3; ++d) {
-        double v = ((double)s.xyz[d * s.n + i] - lo[d]) / q;
-        c[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
+    parallel_ranges(s.n, [&](uint32_t i0, uint32_t i1) {
+      for (uint32_t i = i0; i < i1; ++i) {
+        uint32_t c[3];
+        for (int d = 0; d < 3; ++d) {
+          double v = ((double)s.xyz[d * s.n + i] - lo[d]) / q;
+          c[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
+        }
+        key[i] = morton3(c[0], c[1], c[2]);
       }
-      key[i] = morton3(c[0], c[1], c[2]);
-    }
+    });
     // stable LSD radix sort of the particle indices by key (16-bit digits over
     // the 63 key bits): equal keys keep ascending index order
     s.perm.resize(s.n);
@@ -1212,13 +1235,13 @@ class Engine final : public EngineBase {
 
   // Largest number of steps the next chunk may take: a particle may not move
   // more than half the skin between list builds; with the speed of the last
-  // chunk and a safety factor of 2 on the remaining distance.
+  // chunk and a safety factor on it (2, doubled after every stale event).
   uint64_t chunk_steps(const Flags& f) const {
     const double budget = 0.5 * min_skin_ - std::sqrt((double)f.d2max);
     const double v = std::sqrt((double)f.v2max);
     // no speed seen yet (the first chunk after set-up): a short chunk measures it
     if (!(v > 0)) return std::min<uint64_t>(opt_.graph_steps, 16);
-    const double k = 0.5 * budget / (v * max_dt_);
+    const double k = budget / (speed_margin_ * v * max_dt_);
     if (!(k >= 1.0)) return 1;
     return (uint64_t)std::min<double>(k, opt_.graph_steps);
   }
@@ -1252,7 +1275,12 @@ class Engine final : public EngineBase {
     const uint32_t numeric_before = f.numeric;
     RC(update_tiles());
     while (true) {
-      if (f.stale) ++stale_events_;
+      if (f.stale) {
+        // a particle outran the speed margin (violent fracture): chunks are
+        // sized with twice the margin from now on (at most 16 x the speed)
+        ++stale_events_;
+        speed_margin_ = std::min(2.0 * speed_margin_, 16.0);
+      }
       if (f.rebuild || f.stale || (double)f.d2max > 0.0625 * min_skin_ * min_skin_) {
         RC(build_contacts(false));
         RC(clear_rebuild_flags());
@@ -1754,35 +1782,53 @@ class Engine final : public EngineBase {
     return rc;
   }
 
+  // Per-kernel device time of nsteps steps run the way the timed steps run:
+  // one captured graph of the steps, with an event record node before the
+  // pair kernel, between the two kernels and after the particle kernel of
+  // every step; the graph is replayed once and the event pairs give each
+  // launch's duration.  Also counts the touching contacts (algorithmic-byte
+  // accounting).
   int profile(uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching) override {
     RC(prepare());
     if (nsteps == 0) return DEM_ERR_ARG;
-    std::vector<cudaEvent_t> ev(4 * (size_t)nsteps);
+    std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     DBuf<unsigned long long> cnt;
     CK(cnt.alloc(1));
     StepArgs<Real> A = args();
     A.touching = cnt.p;
     const uint32_t g = particle_grid();
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     for (uint32_t k = 0; k < nsteps; ++k) {
-      CK(cudaEventRecord(ev[4 * k], stream_));
+      cudaEventRecord(ev[3 * k], stream_);
       launch_pairs(A);
-      CK(cudaEventRecord(ev[4 * k + 1], stream_));
-      CK(cudaEventRecord(ev[4 * k + 2], stream_));
+      cudaEventRecord(ev[3 * k + 1], stream_);
       k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
-      CK(cudaEventRecord(ev[4 * k + 3], stream_));
+      cudaEventRecord(ev[3 * k + 2], stream_);
     }
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(stream_));
+    cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) {
+      for (auto& x : ev) cudaEventDestroy(x);
+      last_cuda_ = e;
+      note_cuda_error(e, __FILE__, __LINE__);
+      return DEM_ERR_CUDA;
+    }
     double sp = 0, sq = 0;
     for (uint32_t k = 0; k < nsteps; ++k) {
       float t1 = 0, t2 = 0;
-      CK(cudaEventElapsedTime(&t1, ev[4 * k], ev[4 * k + 1]));
-      CK(cudaEventElapsedTime(&t2, ev[4 * k + 2], ev[4 * k + 3]));
+      CK(cudaEventElapsedTime(&t1, ev[3 * k], ev[3 * k + 1]));
+      CK(cudaEventElapsedTime(&t2, ev[3 * k + 1], ev[3 * k + 2]));
       sp += t1;
       sq += t2;
     }
-    for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& x : ev) cudaEventDestroy(x);
     unsigned long long tc = 0;
     CK(cnt.download(&tc, 1));
     if (pair_ms) *pair_ms = sp / nsteps;
@@ -1810,6 +1856,7 @@ class Engine final : public EngineBase {
   cudaError_t last_cuda_ = cudaSuccess;
   uint64_t total_steps_ = 0, rebuilds_ = 0, stale_events_ = 0;
   double min_skin_ = 0, max_dt_ = 0;
+  double speed_margin_ = 2.0;   // chunk sizing: the fastest particle may speed up this much within a chunk
 
   std::vector<SampleHost> samples_;
   std::vector<SampleParams<Real>> hparams_;

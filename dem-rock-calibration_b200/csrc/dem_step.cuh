@@ -788,6 +788,28 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
   using T = RT<Real>;
   using V4 = typename T::V4;
   __shared__ int s_last;
+  // The constants and this step's controller state of every sample (up to
+  // kCacheSamples; FP32 and FP64), copied into shared memory once per block:
+  // a particle's sample id then costs one shared lookup instead of two
+  // dependent global loads (controller flags, then the sample's constants).
+  // The controller updates the global state only after every block is done.
+  constexpr uint32_t kCacheSamples = 16;
+  constexpr bool kCacheable = sizeof(Real) <= 8;
+  __shared__ SampleParams<Real> c_sp[kCacheable ? kCacheSamples : 1];
+  __shared__ float c_wall[kCacheable ? kCacheSamples : 1][3];   // platen top, bottom, velocity (as float)
+  __shared__ uint32_t c_flag[kCacheable ? kCacheSamples : 1];   // bit 0: done; bit 1: a lateral-record step
+  const bool cached = kCacheable && A.nsamples <= kCacheSamples;
+  if (cached) {
+    for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
+      c_sp[s] = A.sp[s];
+      const SampleCtl& C = A.ctl[s];
+      c_wall[s][0] = (float)C.Top;
+      c_wall[s][1] = (float)C.Bottom;
+      c_wall[s][2] = (float)C.V;
+      c_flag[s] = (C.done ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u);
+    }
+    __syncthreads();
+  }
   // platen force partial sums of this block are kept per sample in registers and
   // flushed with one double atomic per (sample, warp) run
   float my_v2 = 0.f, my_d2 = 0.f;
@@ -809,8 +831,9 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
     double sb = 0.0, st = 0.0, sl = 0.0;
-    if (!C.done) {
-      const SampleParams<Real>& sp = A.sp[s];
+    const uint32_t flag = cached ? c_flag[s] : ((C.done ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u));
+    if (!(flag & 1u)) {
+      const SampleParams<Real>& sp = cached ? c_sp[s] : A.sp[s];
       if constexpr (sizeof(Real) == 4) {
         if (A.det) {
           const longlong2 q0 = *reinterpret_cast<const longlong2*>(A.frcq + 4 * (size_t)p);
@@ -854,11 +877,11 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
         // platen zone that touches neither platen and had no history keeps a zero
         // one: nothing to read or write.
         if (lat < Real(sp.wall_RR) && r[2] < Real(sp.zcut)) {
-          const Real wtop = Real((float)C.Top), wbot = Real((float)C.Bottom);
+          const Real wtop = Real(cached ? c_wall[s][0] : (float)C.Top), wbot = Real(cached ? c_wall[s][1] : (float)C.Bottom);
           const bool top = wtop - r[ax] < x.w, bot = r[ax] - wbot < x.w;
           const uint8_t had = A.wflag[p];
           if (top || bot || had) {
-            const Real wvel = Real((float)C.V);
+            const Real wvel = Real(cached ? c_wall[s][2] : (float)C.V);
             V4 o4 = had ? A.wallO[p] : mk4(Real(0), Real(0), Real(0), Real(0));
             Real o[3] = {o4.x, o4.y, o4.z};
             const Real ri = x.w, mi = A.mass[p];
@@ -932,7 +955,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
       // particle interacts with nothing (all parked particles coincide, and
       // pairs closer than 1e-10 are ignored), so it restarts its reference.
       // lateral surface particles on record steps: radial distance from the axis
-      if (A.lat && A.lat[p] && !parked && C.dNsave && C.step % C.dNsave == 0) {
+      if (A.lat && A.lat[p] && !parked && (flag & 2u)) {
         const double ex = (double)x.x - sp.wall_c[0], ey = (double)x.y - sp.wall_c[1];
         sl = sqrt(ex * ex + ey * ey);
       }

@@ -235,8 +235,9 @@ int dem_rebuild_contacts(dem_ctx* ctx);
 /* Advances nsteps steps from the captured step graph; *ms = device time of
  * the whole run (CUDA events on the context's stream, rebuilds included). */
 int dem_run_timed(dem_ctx* ctx, uint64_t nsteps, double* ms);
-/* Advances nsteps steps launching the two step kernels one by one with CUDA
- * events around each: average per-launch times of the pair kernel and the
+/* Advances nsteps steps as one captured graph with a CUDA event record node
+ * before, between and after the two step kernels of every step (the way the
+ * timed steps run): average per-launch times of the pair kernel and the
  * particle kernel, and the mean number of touching contacts per step. */
 int dem_profile(dem_ctx* ctx, uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching);
 /* Launch-schedule autotuner (no counterpart in the reference): after

@@ -316,8 +316,8 @@ static void fire_power(packer_t* S, int viscous) {
   ++F->step;
 }
 
-/* k_fire_move: the viscous, FIRE 2.0 or reference FIRE move, then the wall
- * put-back; speed and displacement maxima. */
+/* k_fire_move: the viscous or FIRE 2.0 move, then the wall put-back; speed
+ * and displacement maxima (the reference's FIRE move: fire_move_reference). */
 static void fire_move(packer_t* S, int viscous) {
   const uint32_t n = S->n;
   const float* c = S->cyl;
@@ -337,33 +337,6 @@ static void fire_move(packer_t* S, int viscous) {
       x.x += v.x * dt;
       x.y += v.y * dt;
       x.z += v.z * dt;
-    } else if (F.variant == 1) {
-      /* md_firerelaxation.cu:58-70 (half step back) and :18-56 (velocity
-       * rebuilt from the current force, mixed, position increment) */
-      const float dt = (float)F.dt, alpha = (float)F.alpha;
-      if (F.back) {
-        const float h = 0.5f * dt;
-        x.x -= v.x * h;
-        x.y -= v.y * h;
-        x.z -= v.z * h;
-      }
-      float vx = f[0] * dtm, vy = f[1] * dtm, vz = f[2] * dtm;
-      const float vv = (vx * vx + vy * vy) + vz * vz;
-      const float ff = (f[0] * f[0] + f[1] * f[1]) + f[2] * f[2];
-      float vdf;
-      if (ff > 1e-12f)
-        vdf = alpha * sqrtf(vv * (1.0f / ff));
-      else
-        vdf = alpha * sqrtf(vv) * 1e6f;
-      vx = (1.0f - alpha) * vx + vdf * f[0];
-      vy = (1.0f - alpha) * vy + vdf * f[1];
-      vz = (1.0f - alpha) * vz + vdf * f[2];
-      v.x = vx;
-      v.y = vy;
-      v.z = vz;
-      x.x += vx * dt;
-      x.y += vy * dt;
-      x.z += vz * dt;
     } else {
       /* FIRE 2.0 (Guenole et al. 2020): half step back and v = 0 on P <= 0,
        * semi-implicit Euler, velocity mixing */
@@ -425,11 +398,83 @@ static void fire_move(packer_t* S, int viscous) {
   if (d2max > S->F.dmax2) S->F.dmax2 = d2max;
 }
 
+/* The reference's FIRE move (fire_variant 1) through the oracle's own
+ * restatements of its kernels: d_CalculateDecrementsHalfStepFIRE
+ * (orc_fire_half_step_back, md_firerelaxation.cu:58-70) when the power was
+ * not positive, then d_CalculateIncrementsFIRE (orc_fire_increments,
+ * md_firerelaxation.cu:18-56) with the per-sphere dt0/m; then the engine's
+ * wall put-back as in fire_move.  The GPU packer's variant 1 must match this
+ * bit for bit. */
+static void fire_move_reference(packer_t* S) {
+  const uint32_t n = S->n;
+  float* R = malloc(3 * (size_t)n * sizeof(float));
+  float* V = malloc(3 * (size_t)n * sizeof(float));
+  float* Fs = malloc(3 * (size_t)n * sizeof(float));
+  float* am = malloc((size_t)n * sizeof(float));
+  for (uint32_t p = 0; p < n; ++p) {
+    R[p] = S->pos[p].x;
+    R[n + p] = S->pos[p].y;
+    R[2 * (size_t)n + p] = S->pos[p].z;
+    V[p] = S->vel[p].x;
+    V[n + p] = S->vel[p].y;
+    V[2 * (size_t)n + p] = S->vel[p].z;
+    for (int d = 0; d < 3; ++d) Fs[(size_t)d * n + p] = S->frc[3 * (size_t)p + d];
+    am[p] = S->vel[p].w;
+  }
+  const float dt = (float)S->F.dt, alpha = (float)S->F.alpha;
+  if (S->F.back) orc_fire_half_step_back_f(V, R, n, 0.5f * dt);
+  orc_fire_increments_f(Fs, V, R, n, 0.f, dt, alpha, am);
+  const float* c = S->cyl;
+  float v2max = 0.f, d2max = 0.f;
+  for (uint32_t p = 0; p < n; ++p) {
+    f4 x = {R[p], R[n + p], R[2 * (size_t)n + p], S->pos[p].w};
+    f4 v = {V[p], V[n + p], V[2 * (size_t)n + p], S->vel[p].w};
+    const float R1 = c[3], H1 = c[4];
+    const float dx = x.x - c[0], dy = x.y - c[1], dz = x.z - c[2];
+    const float rr = dx * dx + dy * dy;
+    if (rr > R1 * R1) {
+      const float rinv = orc_rsqrt_rn_f(rr);
+      const float qq = R1 * rinv - 1.0f;
+      x.x += dx * qq;
+      x.y += dy * qq;
+      const float vn = (v.x * dx + v.y * dy) * rinv;
+      if (vn > 0.f) {
+        v.x -= vn * dx * rinv;
+        v.y -= vn * dy * rinv;
+      }
+    }
+    if (dz > H1) {
+      x.z += H1 - dz;
+      if (v.z > 0.f) v.z = 0.f;
+    }
+    if (dz < -H1) {
+      x.z += -H1 - dz;
+      if (v.z < 0.f) v.z = 0.f;
+    }
+    S->pos[p] = x;
+    S->vel[p] = v;
+    const f4 r0 = S->ref[p];
+    const float ex = x.x - r0.x, ey = x.y - r0.y, ez = x.z - r0.z;
+    const float a = (v.x * v.x + v.y * v.y) + v.z * v.z, b = (ex * ex + ey * ey) + ez * ez;
+    if (a > v2max) v2max = a;
+    if (b > d2max) d2max = b;
+  }
+  if (v2max > S->F.vmax2) S->F.vmax2 = v2max;
+  if (d2max > S->F.dmax2) S->F.dmax2 = d2max;
+  free(R);
+  free(V);
+  free(Fs);
+  free(am);
+}
+
 static void step(packer_t* S, int viscous) {
   const float w = soft_pairs(S);
   if (w > S->F.max_overlap) S->F.max_overlap = w;
   fire_power(S, viscous);
-  fire_move(S, viscous);
+  if (!viscous && S->F.variant == 1)
+    fire_move_reference(S);
+  else
+    fire_move(S, viscous);
 }
 
 /* Relaxation loop with the GPU's list and chunk schedule (Packer::relax). */

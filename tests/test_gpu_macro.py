@@ -135,18 +135,26 @@ def test_uniaxial_strength_statistics_match_reference_driver(tmp_path):
 @pytest.mark.skipif(not L.ref_available(), reason="reference harness not built")
 def test_brazilian_tensile_strength_statistics_match_reference_driver(tmp_path):
     lsi, space = (0.006, 0.006, 0.003), (0.012, 0.012, 0.006)
-    st_r, st_m = [], []
+    st_r, st_m, pk_r, pk_m = [], [], [], []
     for seed in SEEDS:
         out, ref_rec, mine = _both_drivers(tmp_path / f"s{seed}", seed, 40e6, 40e6, 0.015, 0.1, runs=4, brazil=True,
                                            lsi=lsi, space=space, minstress_si=1e6, dNsave=50)
         assert out.FractureStress > 1e6 / dem.STRESS
         st_r.append(out.FractureStress)
+        pk_r.append(_sigma(ref_rec).max())
         st_m.append([res["FractureStress"] for res, _ in mine])
+        pk_m.append([_sigma(rec).max() for _, rec in mine])
         for res, rec in mine:
             assert res["done"] == 1 and res["FractureStress"] > 1e6 / dem.STRESS
     print()
-    mr, me, se, rel = _compare_means("Brazilian tensile strength", st_r, st_m)
-    assert abs(me - mr) <= 3.0 * se + 0.005 * mr, (mr, me, se)
+    # the reference's sigma_t: FractureStress, whose peak restarts whenever the
+    # stress drops below ConditionFracture x peak (md_results.cu:130-134), so
+    # it may report a later peak of the broken disc; and the first peak of the
+    # record, the usual definition
+    for name, r, e in (("Brazilian tensile strength (reference definition)", st_r, st_m),
+                       ("Brazilian peak stress of the record", pk_r, pk_m)):
+        mr, me, se, rel = _compare_means(name, r, e)
+        assert abs(me - mr) <= 3.0 * se + 0.005 * mr, (name, mr, me, se)
 
 
 @pytest.mark.skipif(not L.ref_available(), reason="reference harness not built")

@@ -5,6 +5,12 @@ restatement (oracle/dem_pack_oracle.c), on a column and a disc, with FIRE 2.0
 and with the reference's FIRE update (md_firerelaxation.cu:18-70 and the
 dt / alpha adaptation of md_createcylindersample.cu:368-397).
 
+For the reference's FIRE update the CPU side moves the spheres with the
+oracle's restatements of the reference kernels themselves
+(orc_fire_half_step_back, orc_fire_increments: d_CalculateDecrementsHalfStepFIRE
+and d_CalculateIncrementsFIRE), so this also pins the GPU packer's FIRE
+update to the reference's.
+
 Pair forces are summed in fixed point on both sides and every other
 operation is rounded the same way, so the packings must agree bit for bit:
 positions, radii, step count, list rebuilds and the final largest overlap.

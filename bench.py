@@ -335,12 +335,16 @@ def sweep_sizes(k: int, seed: int = 11) -> list[int]:
 
 
 def run_sweep(args, ws, rank, local):
-    """Batched calibration sweep: `cases` Latin-hypercube parameter sets over 16
-    packed cylinders (5k-60k spheres) in one context, against the same cases
-    one context at a time.  Every rank runs its own sweep (weak scaling)."""
+    """Batched calibration sweep: `cases` Latin-hypercube parameter sets per
+    rank over 16 packed cylinders (5k-60k spheres) in one context, against the
+    same cases one context at a time.  Under torchrun one sweep of
+    cases x ranks parameter sets is split into contiguous blocks (weak
+    scaling); after the timed steps the ranks exchange the per-case macro
+    properties, so every rank holds the whole sweep's results."""
     sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
     D = Dist(ws)
-    sw = sweep.build_sweep(args.cases, sweep_sizes(16, 11 + rank), seed=1 + rank, device=local)
+    n_total = args.cases * ws
+    sw = sweep.build_sweep(n_total, sweep_sizes(16, 11), seed=1, device=local, only=sweep.shard(n_total, rank, ws))
     n = sw.particles
     dem = importlib.import_module("dem-rock-calibration_b200")
     # launch schedule and contact-list skin chosen by the engine's autotuner on
@@ -372,6 +376,10 @@ def run_sweep(args, ws, rank, local):
     prof = ctx.profile(min(args.steps, 200))
     res = [ctx.result(i) for i in range(len(sw.cases))]
     ctx.close()
+    whole = sweep.gather_results({c.index: r for c, r in zip(sw.cases, res)}, n_total)
+    gathered = {"cases": len(whole), "done": sum(r["done"] for r in whole),
+                "bonds_broken": sum(r["bonds_initial"] - r["bonds_now"] for r in whole),
+                "max_stress_mean_GPa": float(np.mean([r["FractureStress"] for r in whole]))}
     # the same cases one context at a time, a bounded sample of them
     k_seq = min(len(sw.cases), 32)
     sub = sweep.Sweep(cases=sw.cases[:k_seq])
@@ -389,6 +397,7 @@ def run_sweep(args, ws, rank, local):
         "config": {"workload": f"calibration sweep: {len(sw.cases)} uniaxial cylinders (16 packings, "
                                f"{min(c.n for c in sw.cases)}-{max(c.n for c in sw.cases)} spheres) in one context",
                    "particles_per_gpu": n, "cases": len(sw.cases), "bonds": bonds,
+                   "sweep_results_gathered": gathered,
                    "sequential": {"cases": k_seq, "particles": n_sub, "value": seq_rate,
                                   "device_ms": seq["device_ms"],
                                   "note": "the same cases one context at a time (device time summed)"},

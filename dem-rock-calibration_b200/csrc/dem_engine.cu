@@ -29,6 +29,10 @@ void note_cuda_error(cudaError_t e, const char* file, int line) {
   const char* base = std::strrchr(file, '/');
   std::snprintf(g_detail, sizeof g_detail, "%s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e),
                 base ? base + 1 : file, line);
+  // the error is reported through the return code: clear the thread's last
+  // runtime error, so that a later cudaGetLastError check of another call
+  // does not report it again
+  (void)cudaGetLastError();
 }
 
 const char* last_error_detail() { return g_detail; }
@@ -1800,15 +1804,20 @@ class Engine final : public EngineBase {
     const uint32_t g = particle_grid();
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // an event recorded during capture becomes an event record node only
+    // with cudaEventRecordExternal (a plain record is a capture-internal
+    // dependency and is never recorded when the graph runs)
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    for (uint32_t k = 0; k < nsteps; ++k) {
-      cudaEventRecord(ev[3 * k], stream_);
+    cudaError_t ce = cudaSuccess;
+    for (uint32_t k = 0; k < nsteps && ce == cudaSuccess; ++k) {
+      ce = cudaEventRecordWithFlags(ev[3 * k], stream_, cudaEventRecordExternal);
       launch_pairs(A);
-      cudaEventRecord(ev[3 * k + 1], stream_);
+      if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 1], stream_, cudaEventRecordExternal);
       k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
-      cudaEventRecord(ev[3 * k + 2], stream_);
+      if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 2], stream_, cudaEventRecordExternal);
     }
     cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+    if (e == cudaSuccess && ce != cudaSuccess) e = ce;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream_);

@@ -82,6 +82,7 @@ class SweepCase:
     loading: object
     xyz: np.ndarray
     radii: np.ndarray
+    index: int = 0          # position in the whole sweep
 
     @property
     def n(self) -> int:
@@ -98,22 +99,104 @@ class Sweep:
 
 
 def build_sweep(n_cases: int, sizes: list[int], seed: int = 1, velocity_m_s: float = 0.1, max_steps: int = 0,
-                device: int = 0) -> Sweep:
+                device: int = 0, only=None) -> Sweep:
     """n_cases parameter sets (Latin hypercube) over len(sizes) packed
     cylinders (case k uses specimen k mod len(sizes)): uniaxial loading at
-    velocity_m_s until the peak has passed (70% of it) or 1% strain."""
-    specs = []
-    for k, n in enumerate(sizes):
-        xyz, rad, rep, box, size_real, center_real = cylinder(n, seed * 1000 + k, device=device)
-        specs.append((xyz, rad, box, size_real, center_real))
+    velocity_m_s until the peak has passed (70% of it) or 1% strain.
+    `only`: the case indices to build (a rank's shard); the parameter sets
+    and per-case seeds are those of the whole sweep, and only the specimens
+    these cases use are packed."""
+    keep = range(n_cases) if only is None else sorted(set(int(k) for k in only))
+    specs = {}
+    for k in keep:
+        i = k % len(sizes)
+        if i not in specs:
+            xyz, rad, rep, box, size_real, center_real = cylinder(sizes[i], seed * 1000 + i, device=device)
+            specs[i] = (xyz, rad, box, size_real, center_real)
+    params = latin_hypercube(n_cases, seed)
     sw = Sweep()
-    for k, p in enumerate(latin_hypercube(n_cases, seed)):
-        xyz, rad, box, size_real, center_real = specs[k % len(specs)]
+    for k in keep:
+        p = params[k]
+        xyz, rad, box, size_real, center_real = specs[k % len(sizes)]
         r_min, r_mean = float(rad.min()), float(rad.mean())
         ld = loading(TEST_UNIAXIAL, box, size_real, center_real, velocity=-velocity_m_s / VELOCITY, min_stress=0.010,
                      max_strain=0.01, cond_fracture=0.7, dNsave=100, max_steps=max_steps, p_r_platen=r_mean)
-        sw.cases.append(SweepCase(k % len(specs), p, material_for(p, r_min, r_mean, seed * 7919 + k), ld, xyz, rad))
+        sw.cases.append(SweepCase(k % len(sizes), p, material_for(p, r_min, r_mean, seed * 7919 + k), ld, xyz, rad,
+                                  index=k))
     return sw
+
+
+def shard(n_cases: int, rank: int, world: int) -> range:
+    """The cases rank `rank` of `world` solves: a contiguous block, sizes
+    differing by at most one.  Consecutive cases cycle through the specimens,
+    so every block of at least len(sizes) cases holds every specimen size and
+    the ranks' particle counts stay balanced."""
+    if not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside world size {world}")
+    return range(rank * n_cases // world, (rank + 1) * n_cases // world)
+
+
+# per-case macro properties exchanged between ranks (dem_result fields)
+MACRO_FIELDS = ("FractureStress", "FractureStrain", "E_chord", "nu", "Strain", "Stress", "Destruction", "dt", "steps",
+                "bonds_initial", "bonds_now", "fracture", "done", "numeric")
+
+
+def gather_results(local: dict, n_cases: int, group=None, device=None) -> list:
+    """All-gather of the per-case macro properties of a sharded sweep: every
+    rank passes {case index: result dict} for its own cases and receives the
+    whole sweep's results in case order (MACRO_FIELDS of each).  One
+    all_gather of a float64 table of ceil(n_cases / world) rows per rank;
+    `device` is where the table lives (a CUDA device under the NCCL backend,
+    the CPU under gloo).  With no process group (or world size 1) the local
+    results are the whole sweep."""
+    import torch
+    import torch.distributed as td
+
+    F = len(MACRO_FIELDS)
+    world = td.get_world_size(group) if td.is_available() and td.is_initialized() else 1
+    per = -(-n_cases // max(world, 1))
+    if len(local) > per:
+        raise ValueError(f"{len(local)} local cases, more than a rank's share {per} of {n_cases}")
+    table = np.full((per, 1 + F), np.nan)
+    for row, (k, res) in enumerate(sorted(local.items())):
+        if not 0 <= k < n_cases:
+            raise ValueError(f"case index {k} outside the sweep's {n_cases} cases")
+        table[row, 0] = k
+        table[row, 1:] = [float(res[f]) for f in MACRO_FIELDS]
+    if world > 1:
+        t = torch.from_numpy(table).to(device if device is not None else "cpu")
+        parts = [torch.empty_like(t) for _ in range(world)]
+        td.all_gather(parts, t, group=group)
+        table = np.concatenate([p.cpu().numpy() for p in parts])
+    out = [None] * n_cases
+    for row in table:
+        if np.isnan(row[0]):
+            continue
+        k = int(row[0])
+        if out[k] is not None:
+            raise RuntimeError(f"case {k} solved by two ranks")
+        out[k] = {f: (int(v) if f in _INT_FIELDS else float(v)) for f, v in zip(MACRO_FIELDS, row[1:])}
+    missing = [k for k, r in enumerate(out) if r is None]
+    if missing:
+        raise RuntimeError(f"cases {missing[:8]} solved by no rank")
+    return out
+
+
+_INT_FIELDS = {"steps", "bonds_initial", "bonds_now", "fracture", "done", "numeric"}
+
+
+def run_sharded(n_cases: int, sizes: list[int], steps: int, rank: int, world: int, seed: int = 1,
+                device: int = 0, group=None, gather_device=None, **kw) -> dict:
+    """One sweep of n_cases cases split over `world` ranks (shard()): each
+    rank packs and solves its block in one batched context, then the ranks
+    exchange the per-case macro properties (gather_results()).  No data-path
+    collective: the specimens are independent.  Returns this rank's device
+    time and the whole sweep's results in case order."""
+    sw = build_sweep(n_cases, sizes, seed=seed, device=device, only=shard(n_cases, rank, world), **kw)
+    out = run_batched(sw, steps, device=device)
+    local = {c.index: r for c, r in zip(sw.cases, out["results"])}
+    return dict(device_ms=out["device_ms"], cases=[c.index for c in sw.cases],
+                results=gather_results(local, n_cases, group=group, device=gather_device))
 
 
 def run_batched(sw: Sweep, steps: int, device: int = 0, graph_steps: int = 200) -> dict:

@@ -115,9 +115,36 @@ def tensor_peak():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: an NVML
+    thread polling every half millisecond (so that a region of a few
+    milliseconds still gets samples; it takes its first sample before the
+    constructor returns and a last one in stop()), else nvidia-smi at 100 ms."""
+
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    _BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
+        self.p = None
+        self.nv = None
+        self.rows = []
+        try:
+            import threading
+
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(device)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.nv = pynvml
+            self.stop_ev = threading.Event()
+            self._sample()
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -128,7 +155,33 @@ class Clocks:
         except FileNotFoundError:
             self.p = None
 
+    def _sample(self):
+        nv = self.nv
+        try:
+            fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.rows.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                              float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)), int(fn(self.h))))
+        except Exception:
+            pass
+
+    def _loop(self):
+        while not self.stop_ev.wait(0.0005):
+            self._sample()
+
     def stop(self) -> dict:
+        if self.nv is not None:
+            self._sample()
+            self.stop_ev.set()
+            self.t.join(5)
+            sm = [r[0] for r in self.rows]
+            mx = [r[1] for r in self.rows]
+            reasons = sorted({k for r in self.rows for k, bit in self._BITS.items() if r[2] & bit})
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -151,7 +204,7 @@ class Clocks:
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def build_specimen(dem, workload: str, seed: int, device: int, packer=None):

@@ -46,6 +46,13 @@ __device__ __forceinline__ void bar_init(uint64_t* b) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(b)) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+__device__ __forceinline__ void bar_init_count(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
 __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
   const uint32_t a = saddr(b);
   for (uint32_t n = 0; n < kPollLimit; ++n) {
@@ -134,6 +141,71 @@ struct GemmCfg {
   static constexpr int kSmem = kStages * kStageBytes + 1024 /* alignment */ + 8 * (2 * kStages + 1) + 16;
   static constexpr uint32_t kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256));
 };
+
+// Epilogue of one 32-column chunk of an accumulator row: tcgen05.ld of the
+// thread's 32 consecutive FP32 columns (TMEM address taddr: lane quarter of
+// the warp, column), then + bias and the activation to BF16 and/or the FP32
+// values, written with 16-byte stores (scalar stores at a ragged right edge
+// or when a row is not a multiple of 16 bytes).  Every lane of the warp takes
+// part in the load; rows >= M and columns >= N are not written.
+__device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int M, int N,
+                                            const float* __restrict__ bias, int mode, bool act,
+                                            float* __restrict__ outf, __nv_bfloat16* __restrict__ outh) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  if (row >= M || nc >= N) return;
+  const int cols = min(32, N - nc);
+  float v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+  if (mode != DEM_MLP_PLAIN) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] += (j < cols) ? __ldg(bias + nc + j) : 0.f;
+  }
+  const size_t o = (size_t)row * N + nc;
+  if (outf) {
+    if (cols == 32 && (N & 3) == 0) {
+      float4* dst = reinterpret_cast<float4*>(outf + o);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < cols) outf[o + j] = v[j];
+    }
+  }
+  if (act) {
+    const bool g = mode == DEM_MLP_BIAS_GELU;
+    uint32_t h[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const float a0 = g ? gelu(v[2 * j]) : fmaxf(v[2 * j], 0.f);
+      const float a1 = g ? gelu(v[2 * j + 1]) : fmaxf(v[2 * j + 1], 0.f);
+      const __nv_bfloat162 p = __floats2bfloat162_rn(a0, a1);
+      h[j] = *reinterpret_cast<const uint32_t*>(&p);
+    }
+    if (cols == 32 && (N & 7) == 0) {
+      uint4* dst = reinterpret_cast<uint4*>(outh + o);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dst[j] = make_uint4(h[4 * j], h[4 * j + 1], h[4 * j + 2], h[4 * j + 3]);
+    } else {
+      unsigned short* dst = reinterpret_cast<unsigned short*>(outh + o);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < cols) dst[j] = (unsigned short)((j & 1) ? (h[j >> 1] >> 16) : (h[j >> 1] & 0xFFFFu));
+    }
+  }
+}
 
 // Warp-specialised: warp 0 lane 0 streams the stages with the TMA (A box
 // 64 x 128 rows, B box 64 x TN rows, 128-byte swizzle, zero fill past the
@@ -244,63 +316,174 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ CU
     const int q4 = warp & 3, half = warp >> 2;
     const int row = m0 + q4 * 32 + lane;
     const bool act = mode == DEM_MLP_BIAS_GELU || mode == DEM_MLP_BIAS_RELU;
-    for (int col0 = 32 * half; col0 < TN; col0 += 64) {
-      uint32_t r[32];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)col0)
-          : "memory");
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int nc = n0 + col0;
-      if (row >= M || nc >= N) continue;
-      const int cols = min(32, N - nc);
-      float v[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-      if (mode != DEM_MLP_PLAIN) {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] += (j < cols) ? __ldg(bias + nc + j) : 0.f;
-      }
-      const size_t o = (size_t)row * N + nc;
-      if (outf) {
-        if (cols == 32 && (N & 3) == 0) {
-          float4* dst = reinterpret_cast<float4*>(outf + o);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (j < cols) outf[o + j] = v[j];
-        }
-      }
-      if (act) {
-        const bool g = mode == DEM_MLP_BIAS_GELU;
-        uint32_t h[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const float a0 = g ? gelu(v[2 * j]) : fmaxf(v[2 * j], 0.f);
-          const float a1 = g ? gelu(v[2 * j + 1]) : fmaxf(v[2 * j + 1], 0.f);
-          const __nv_bfloat162 p = __floats2bfloat162_rn(a0, a1);
-          h[j] = *reinterpret_cast<const uint32_t*>(&p);
-        }
-        if (cols == 32 && (N & 7) == 0) {
-          uint4* dst = reinterpret_cast<uint4*>(outh + o);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) dst[j] = make_uint4(h[4 * j], h[4 * j + 1], h[4 * j + 2], h[4 * j + 3]);
-        } else {
-          unsigned short* dst = reinterpret_cast<unsigned short*>(outh + o);
-#pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (j < cols) dst[j] = (unsigned short)((j & 1) ? (h[j >> 1] >> 16) : (h[j >> 1] & 0xFFFFu));
-        }
-      }
+    for (int col0 = 32 * half; col0 < TN; col0 += 64)
+      drain_chunk(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)col0, row, n0 + col0, M, N, bias, mode, act, outf,
+                  outh);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols) : "memory");
+}
+
+// Persistent form for the tall layers (many 128-row tiles, N <= 256, K <= 256,
+// the surrogate's forward and inference passes): one block per SM (two when
+// the accumulators are narrow) walks the 128-row tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ...  The whole B operand (N x K, at most 128 KB)
+// is loaded once and stays in shared memory; A streams through a four-stage
+// ring.  Tensor memory holds two accumulators, so the epilogue of tile t
+// (eight warps draining accumulator t % 2) overlaps the loads and MMAs of
+// tile t + 1 (warp 0: TMA producer, warp 1: MMA issuer).
+//   full[s] / empty[s]   A stage s loaded / consumed by its MMAs
+//   bfull                the resident B has landed
+//   tfull[a] / tempty[a] accumulator a complete / drained (eight arrivals)
+template <int TN>
+struct PersistCfg {
+  static constexpr int kStages = 4;
+  static constexpr int kABytes = kTM * 128;                     // one 64-wide K slice of a 128-row tile
+  static constexpr int kBBlock = TN * 128;                      // one 64-wide K slice of B
+  static constexpr int kMaxK = 256;
+  static constexpr int kBBytes = (kMaxK / kSK) * kBBlock;
+  static constexpr int kSmem = kStages * kABytes + kBBytes + 1024 + 8 * (2 * kStages + 5) + 16;
+  static constexpr uint32_t kCols = 2 * (TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256)));
+  static constexpr int kThreads = 320;                          // producer, MMA, eight epilogue warps
+};
+
+template <int TN>
+__global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
+    k_gemm_tn_persist(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
+                      int K, const float* __restrict__ bias, int mode, float* __restrict__ outf,
+                      __nv_bfloat16* __restrict__ outh, unsigned int* err) {
+  using Cfg = PersistCfg<TN>;
+  constexpr int S = Cfg::kStages;
+  constexpr uint32_t kAcc = Cfg::kCols / 2;   // column offset of the second accumulator
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* bres = base + S * Cfg::kABytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(bres + Cfg::kBBytes);
+  uint64_t* empty = full + S;
+  uint64_t* bfull = empty + S;
+  uint64_t* tfull = bfull + 1;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+  const uint32_t sbase = saddr(base), bbase = saddr(bres);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles = (M + kTM - 1) / kTM;
+  const int rounds = (K + kSK - 1) / kSK;
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                 "r"(Cfg::kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      bar_init(&full[s]);
+      bar_init(&empty[s]);
     }
+    bar_init(bfull);
+    for (int a = 0; a < 2; ++a) {
+      bar_init(&tfull[a]);
+      bar_init_count(&tempty[a], 8);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {
+      // producer: B once, then the A slices of every tile of this block
+      bar_expect_tx(bfull, (uint32_t)(rounds * Cfg::kBBlock));
+      for (int c = 0; c < rounds; ++c) tma_load_2d(bbase + c * Cfg::kBBlock, &tmB, c * kSK, 0, bfull);
+      int g = 0;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        for (int c = 0; c < rounds; ++c, ++g) {
+          const int s = g % S;
+          if (g >= S && !bar_wait(&empty[s], (uint32_t)((g / S - 1) & 1))) {
+            ok = false;
+            break;
+          }
+          bar_expect_tx(&full[s], (uint32_t)Cfg::kABytes);
+          tma_load_2d(sbase + s * Cfg::kABytes, &tmA, c * kSK, t * kTM, &full[s]);
+        }
+      }
+      // no load may still be writing shared memory when the block ends
+      for (int q = (g > S ? g - S : 0); q < g; ++q)
+        if (!bar_wait(&full[q % S], (uint32_t)((q / S) & 1))) ok = false;
+      if (!bar_wait(bfull, 0u)) ok = false;
+      if (!ok) atomicOr(err, 1u);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer
+      int g = 0, it = 0, last_commit = -1;
+      if (!bar_wait(bfull, 0u)) ok = false;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++it) {
+        const int a = it & 1;
+        if (it >= 2 && !bar_wait(&tempty[a], (uint32_t)(((it >> 1) - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)a * kAcc;
+        for (int c = 0; c < rounds; ++c, ++g) {
+          const int s = g % S;
+          if (!bar_wait(&full[s], (uint32_t)((g / S) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + s * Cfg::kABytes;
+          for (int kk = 0; kk < kSK / 16; ++kk) {
+            const uint64_t da = smem_desc_sw128(st + (uint32_t)(kk * 32));
+            const uint64_t db = smem_desc_sw128(bbase + (uint32_t)(c * Cfg::kBBlock + kk * 32));
+            const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                ::"r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                : "memory");
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           saddr(&empty[s]))
+                       : "memory");
+          last_commit = s;
+        }
+        if (!ok) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         saddr(&tfull[a]))
+                     : "memory");
+      }
+      // on a timeout, let the MMAs already issued finish before the block ends
+      if (!ok && last_commit >= 0) bar_wait(&empty[last_commit], (uint32_t)(((g - 1) / S) & 1));
+      if (!ok) atomicOr(err, 1u);
+    }
+  } else {
+    // epilogue warps 2..9: lane quarter warp % 4 (the accumulator lanes this
+    // warp may read), column half (warp - 2) / 4
+    const int q4 = warp & 3, half = (warp - 2) >> 2;
+    const bool act = mode == DEM_MLP_BIAS_GELU || mode == DEM_MLP_BIAS_RELU;
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int a = it & 1;
+      if (!bar_wait(&tfull[a], (uint32_t)((it >> 1) & 1))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int row = t * kTM + q4 * 32 + lane;
+      const uint32_t acc = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)a * kAcc;
+      for (int col0 = 32 * half; col0 < TN; col0 += 64)
+        drain_chunk(acc + (uint32_t)col0, row, col0, M, N, bias, mode, act, outf, outh);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) bar_arrive(&tempty[a]);
+    }
+    if (!ok && lane == 0) atomicOr(err, 1u);
   }
   tc_fence_before();
   __syncthreads();
@@ -514,6 +697,34 @@ int launch_gemm(unsigned gx, unsigned gy, cudaStream_t st, const __nv_bfloat16* 
   return DEM_OK;
 }
 
+template <int TN>
+int launch_gemm_persist(unsigned grid, cudaStream_t st, const __nv_bfloat16* a, const __nv_bfloat16* b, int M, int N,
+                        int K, const float* bias, int mode, float* outf, __nv_bfloat16* oh, unsigned int* err) {
+  static bool raised[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return DEM_ERR_CUDA;
+  if (!raised[dev]) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (cudaFuncSetAttribute(k_gemm_tn_persist<TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             PersistCfg<TN>::kSmem) != cudaSuccess)
+      return DEM_ERR_CUDA;
+    raised[dev] = true;
+  }
+  CUtensorMap ma, mb;
+  if (make_map(&ma, a, M, K, kTM) || make_map(&mb, b, N, K, TN)) return DEM_ERR_CUDA;
+  k_gemm_tn_persist<TN><<<grid, PersistCfg<TN>::kThreads, PersistCfg<TN>::kSmem, st>>>(ma, mb, M, N, K, bias, mode,
+                                                                                       outf, oh, err);
+  return DEM_OK;
+}
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                               cudaSuccess)
+    return 0;
+  return n;
+}
+
 }  // namespace
 }  // namespace dem
 
@@ -536,6 +747,23 @@ int dem_mlp_gemm_tn(const void* A, const void* B, int M, int N, int K, const flo
   const auto* b = static_cast<const __nv_bfloat16*>(B);
   auto* oh = static_cast<__nv_bfloat16*>(out_bf16);
   const unsigned gx = (unsigned)((M + kTM - 1) / kTM);
+  // tall layers (at least two 128-row tiles per SM, one column tile, B small
+  // enough to stay in shared memory): the persistent kernel, one block per SM
+  const int sms = sm_count();
+  if (sms > 0 && N <= 256 && K <= PersistCfg<256>::kMaxK && gx >= 2u * (unsigned)sms) {
+    const unsigned grid = (unsigned)sms;
+    int rc;
+    if (N <= 32)
+      rc = launch_gemm_persist<32>(grid, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+    else if (N <= 64)
+      rc = launch_gemm_persist<64>(grid, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+    else if (N <= 128)
+      rc = launch_gemm_persist<128>(grid, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+    else
+      rc = launch_gemm_persist<256>(grid, st, a, b, M, N, K, bias, mode, out_f32, oh, err);
+    if (rc) return rc;
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+  }
   // tile width: the widest that covers N, narrowed while the grid would leave
   // most SMs idle (small batches), down to 32 columns
   int tn = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));

@@ -44,8 +44,11 @@ def _status_ok():
     assert f.value == 0
 
 
+# the last four shapes take the persistent kernel (at least two 128-row tiles
+# per SM, N <= 256, K <= 256): ragged rows, narrow and ragged columns, K = 32
 @pytest.mark.parametrize("M,N,K", [(128, 32, 32), (300, 256, 64), (1000, 4, 256), (256, 320, 96), (77, 64, 512),
-                                   (4096, 128, 256)])
+                                   (4096, 128, 256), (65536, 256, 256), (40000, 100, 128), (38000, 4, 256),
+                                   (50000, 64, 32)])
 @pytest.mark.parametrize("mode", [S.PLAIN, S.BIAS, S.BIAS_GELU, S.BIAS_RELU])
 def test_gemm_tn_against_torch_fp32(M, N, K, mode):
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K + mode)

@@ -125,6 +125,36 @@ class CGTask:
         return new
 
 
+def descent_step(R0: np.ndarray, dR: np.ndarray, goal: np.ndarray, weight: np.ndarray):
+    """The first step of CalculateNewParameters2 (mp_task.h:253-300) for a
+    functional F = sum_j w_j (goal_j - R_j)^2 over any number of results and
+    parameters, given the result Jacobian dR[i, j] = dR_j / dp_i: from the
+    reference's one-sided finite differences (its six solves per step) or from
+    the sensitivity build.  Returns the direction dfun_i = -2 sum_j w_j D_j
+    dR[i, j] (the gradient of F; on a first step the conjugate direction is
+    dfun itself, bcoeff = 0) and the Gauss-Newton step length t = -a1 / a0
+    along it; the reference's update is then p - t dfun."""
+    R0, dR = np.asarray(R0, np.float64), np.asarray(dR, np.float64)
+    w, goal = np.asarray(weight, np.float64), np.asarray(goal, np.float64)
+    D = goal - R0
+    dfun = np.array([sum(-2 * w[j] * D[j] * dR[i, j] for j in range(D.size)) for i in range(dR.shape[0])])
+    a0 = a1 = 0.0
+    for j in range(D.size):
+        for i in range(dR.shape[0]):
+            a1 += w[j] * D[j] * dR[i, j] * dfun[i]
+            for k in range(dR.shape[0]):
+                a0 += w[j] * dR[i, j] * dfun[i] * dR[k, j] * dfun[k]
+    return dfun, -a1 / a0
+
+
+def finite_difference_jacobian(R0: np.ndarray, R_varied: np.ndarray, variation: np.ndarray) -> np.ndarray:
+    """dR[i, j] = (R_varied[i, j] - R0[j]) / variation[i]: the reference's
+    one-sided differences (mp_task.h:233-246, ParameterVariation = MaterialDeltaFactor
+    x parameter)."""
+    R0, Rv, v = (np.asarray(a, np.float64) for a in (R0, R_varied, variation))
+    return (Rv - R0[None, :]) / v[:, None]
+
+
 @dataclass
 class Specimen:
     """A loaded sample file: positions (SoA) and the loading set-up."""

@@ -147,7 +147,11 @@ struct GemmCfg {
 // the warp, column), then + bias and the activation to BF16 and/or the FP32
 // values, written with 16-byte stores (scalar stores at a ragged right edge
 // or when a row is not a multiple of 16 bytes).  Every lane of the warp takes
-// part in the load; rows >= M and columns >= N are not written.
+// part in the load; rows >= M and columns >= N are not written.  kBias4: the
+// bias is a zero-padded shared-memory copy read as 16-byte vectors (the same
+// address in every lane: one broadcast per vector); otherwise it is read from
+// global memory value by value.
+template <bool kBias4 = false>
 __device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int M, int N,
                                             const float* __restrict__ bias, int mode, bool act,
                                             float* __restrict__ outf, __nv_bfloat16* __restrict__ outh) {
@@ -169,8 +173,20 @@ __device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int
 #pragma unroll
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
   if (mode != DEM_MLP_PLAIN) {
+    if constexpr (kBias4) {
+      const float4* b4 = reinterpret_cast<const float4*>(bias + nc);
 #pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] += (j < cols) ? __ldg(bias + nc + j) : 0.f;
+      for (int j = 0; j < 8; ++j) {
+        const float4 b = b4[j];
+        v[4 * j] += b.x;
+        v[4 * j + 1] += b.y;
+        v[4 * j + 2] += b.z;
+        v[4 * j + 3] += b.w;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] += (j < cols) ? __ldg(bias + nc + j) : 0.f;
+    }
   }
   const size_t o = (size_t)row * N + nc;
   if (outf) {
@@ -344,9 +360,15 @@ struct PersistCfg {
   static constexpr int kBBlock = TN * 128;                      // one 64-wide K slice of B
   static constexpr int kMaxK = 256;
   static constexpr int kBBytes = (kMaxK / kSK) * kBBlock;
-  static constexpr int kSmem = kStages * kABytes + kBBytes + 1024 + 8 * (2 * kStages + 5) + 16;
+  // mbarriers and the TMEM address slot, rounded to 16 bytes (the bias copy
+  // after them is read as 16-byte vectors)
+  static constexpr int kBarBytes = (8 * (2 * kStages + 5) + 16 + 15) / 16 * 16;
+  static constexpr int kSmem = kStages * kABytes + kBBytes + 1024 + kBarBytes + TN * 4;
   static constexpr uint32_t kCols = 2 * (TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256)));
-  static constexpr int kThreads = 320;                          // producer, MMA, eight epilogue warps
+  static constexpr int kEpiWarps = 16;
+  static_assert((kStages * kABytes + kBBytes) % 1024 == 0, "B and the barriers follow 1024-byte aligned stages");
+  static_assert(kSmem <= 227 * 1024, "dynamic shared memory of one block");
+  static constexpr int kThreads = 64 + 32 * kEpiWarps;          // producer, MMA, sixteen epilogue warps
 };
 
 template <int TN>
@@ -366,6 +388,7 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
   uint64_t* tfull = bfull + 1;
   uint64_t* tempty = tfull + 2;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+  float* sbias = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(full) + Cfg::kBarBytes);
   const uint32_t sbase = saddr(base), bbase = saddr(bres);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tiles = (M + kTM - 1) / kTM;
@@ -384,7 +407,7 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
     bar_init(bfull);
     for (int a = 0; a < 2; ++a) {
       bar_init(&tfull[a]);
-      bar_init_count(&tempty[a], 8);
+      bar_init_count(&tempty[a], Cfg::kEpiWarps);
     }
   }
   tc_fence_before();
@@ -463,10 +486,14 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
       if (!ok) atomicOr(err, 1u);
     }
   } else {
-    // epilogue warps 2..9: lane quarter warp % 4 (the accumulator lanes this
-    // warp may read), column half (warp - 2) / 4
-    const int q4 = warp & 3, half = (warp - 2) >> 2;
+    // epilogue warps 2..17: lane quarter warp % 4 (the accumulator lanes this
+    // warp may read), column group (warp - 2) / 4 (32-column chunks cg,
+    // cg + 4, ...).  The bias goes to shared memory first (zero past N).
+    const int q4 = warp & 3, cg = (warp - 2) >> 2;
     const bool act = mode == DEM_MLP_BIAS_GELU || mode == DEM_MLP_BIAS_RELU;
+    for (int c = tid - 64; c < TN; c += 32 * Cfg::kEpiWarps)
+      sbias[c] = (mode != DEM_MLP_PLAIN && c < N) ? bias[c] : 0.f;
+    asm volatile("bar.sync 1, %0;" ::"n"(32 * Cfg::kEpiWarps) : "memory");
     int it = 0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
       const int a = it & 1;
@@ -477,8 +504,8 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
       tc_fence_after();
       const int row = t * kTM + q4 * 32 + lane;
       const uint32_t acc = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)a * kAcc;
-      for (int col0 = 32 * half; col0 < TN; col0 += 64)
-        drain_chunk(acc + (uint32_t)col0, row, col0, M, N, bias, mode, act, outf, outh);
+      for (int col0 = 32 * cg; col0 < TN; col0 += 128)
+        drain_chunk<true>(acc + (uint32_t)col0, row, col0, M, N, sbias, mode, act, outf, outh);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) bar_arrive(&tempty[a]);
@@ -717,12 +744,17 @@ int launch_gemm_persist(unsigned grid, cudaStream_t st, const __nv_bfloat16* a, 
   return DEM_OK;
 }
 
+// SM count of the current device (looked up once per device)
 int sm_count() {
-  int dev = 0, n = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
-                                               cudaSuccess)
-    return 0;
-  return n;
+  static int cached[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 0;
+  if (cached[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    cached[dev] = n;
+  }
+  return cached[dev];
 }
 
 }  // namespace

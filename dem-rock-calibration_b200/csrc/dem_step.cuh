@@ -106,12 +106,15 @@ template <class Real>
 __device__ __forceinline__ void tangent_step_end(const StepArgs<Real>&, const SampleCtl&, uint32_t) {}
 
 // A value whose derivative the sensitivity build drops (the identity for float
-// and double).  Used for the contact terms that are not Lipschitz in the state:
-// the overlap factor sqrt(R* overlap) inside the damping coefficients
-// sqrt(K m) (derivative ~ overlap^-3/4 at first touch; the moduli and masses
-// keep theirs), and the unit directions of the Coulomb cap and of rolling
-// friction (derivative ~ 1/|v| near rest).  Their derivatives would swamp the
-// tangents of a loading run with spikes at every contact onset.
+// and double).  Used for the unit directions of the Coulomb cap and of rolling
+// friction (derivative ~ 1/|v| or 1/|w| near rest): rolling friction turns a
+// spin that is nearly zero into a moment of fixed size whose direction
+// flips from step to step, and the linearised step of that term is
+// unstable, so its tangents would grow without bound.  The contact damping
+// keeps its full derivative (the overlap factor sqrt(R* overlap) inside
+// sqrt(K m) included): on a 20,000-sphere uniaxial run the secant-modulus
+// derivatives were 7e-4 to 1.7e-3 (relative) from central differences with
+// that factor's derivative dropped, and 8e-5 to 6e-4 with it kept.
 template <class Real>
 __device__ __forceinline__ Real frozen(const Real& x) {
   return x;
@@ -139,9 +142,6 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   Real cef1 = T::sqrt_rn(reff * (sumr - rijm));
   const Real Kn = Real(2) * sp.hmE * cef1;
   const Real Kt = Real(8) * sp.hmG * cef1;
-  // the same stiffnesses with their overlap dependence frozen (for the damping
-  // coefficients; identical values)
-  const Real Knd = Real(2) * sp.hmE * frozen(cef1), Ktd = Real(8) * sp.hmG * frozen(cef1);
   const Real rbar = half * sumr, rdif = half * (rj - ri);
   const Real sw0 = wj.x + wi.x, sw1 = wj.y + wi.y, sw2 = wj.z + wi.z;
   const Real dw0 = wj.x - wi.x, dw1 = wj.y - wi.y, dw2 = wj.z - wi.z;
@@ -151,7 +151,7 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   const Real vn = n0 * v0 + n1 * v1 + n2 * v2;
   const Real fijnm = (rijm - sumr) * Kn * T::kTwoThirds;
   const Real m2 = mi * ((mj + mj) / (mi + mj));
-  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Knd * half * m2);
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * half * m2);
   const Real fn0 = n0 * (fijnm + cef1), fn1 = n1 * (fijnm + cef1), fn2 = n2 * (fijnm + cef1);
   const Real vt0 = v0 - n0 * vn, vt1 = v1 - n1 * vn, vt2 = v2 - n2 * vn;
   // rotate the old tangential overlap into the new tangent plane, keep its length
@@ -182,7 +182,7 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
     t1 = ft1 * cef1;
     t2 = ft2 * cef1;
   } else {
-    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Ktd * half * m2);
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * half * m2);
     ft0 += vt0 * cef1;
     ft1 += vt1 * cef1;
     ft2 += vt2 * cef1;
@@ -660,14 +660,13 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
   Real cef1 = T::sqrt_rn(ri * T::fabs_(ri - riwm));
   const Real Kn = Real(2) * sp.wallE * cef1;
   const Real Kt = Real(8) * sp.wallG * cef1;
-  const Real Knd = Real(2) * sp.wallE * frozen(cef1), Ktd = Real(8) * sp.wallG * frozen(cef1);
   Real viw[3];
   viw[0] = wv[0] - v.x + ri * (niw[1] * w.z - niw[2] * w.y);
   viw[1] = wv[1] - v.y + ri * (niw[2] * w.x - niw[0] * w.z);
   viw[2] = wv[2] - v.z + ri * (niw[0] * w.y - niw[1] * w.x);
   const Real vn = niw[0] * viw[0] + niw[1] * viw[1] + niw[2] * viw[2];
   const Real fiwnm = (riwm - ri) * Kn * T::kTwoThirds;
-  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Knd * mi);
+  cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * mi);
   const Real fiwn[3] = {niw[0] * (fiwnm + cef1), niw[1] * (fiwnm + cef1), niw[2] * (fiwnm + cef1)};
   const Real vt[3] = {viw[0] - niw[0] * vn, viw[1] - niw[1] * vn, viw[2] - niw[2] * vn};
   cef1 = niw[0] * o[0] + niw[1] * o[1] + niw[2] * o[2];
@@ -698,7 +697,7 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
     ot[1] = ft[1] * cef1;
     ot[2] = ft[2] * cef1;
   } else {
-    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Ktd * mi);
+    cef1 = T::kDamp * sp.pA * T::sqrt_rn(Kt * mi);
     ft[0] += vt[0] * cef1;
     ft[1] += vt[1] * cef1;
     ft[2] += vt[2] * cef1;

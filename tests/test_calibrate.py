@@ -103,3 +103,24 @@ def test_cg_step_runs_its_solves_in_one_context(tmp_path):
         assert np.all(np.isfinite(h["params"])) and h["results"][1] > 0
     assert np.all(np.isfinite(task.params)) and not np.array_equal(task.params, p0)
     assert out.read_text().count("Step:") == 2
+
+
+def test_descent_step_is_the_first_cg_update():
+    """descent_step (any Jacobian, any sizes) reproduces the first update of
+    CGTask.new_parameters (the reference's CalculateNewParameters2 with no
+    previous direction) when given the reference's finite-difference Jacobian."""
+    rng = np.random.default_rng(4)
+    params = np.array([17.1, 0.618, 0.503, 1.64e-3, 5.9e-2])
+    goal = np.array([0.0048, 0.104, 0.0105, 1.0])
+    t = cal.CGTask(params=params, goal=goal, weight_multiplier=np.array([50.0, 100.0, 1.0, 1e4]), variation_type=2,
+                   calc_u=True, calc_b=True)
+    t.start_parameters()
+    t.rfun[:] = goal[None, :] * (1.0 + 0.2 * rng.standard_normal((6, 4)))
+    var = np.array([t.variation[i + 1, i] for i in range(5)])
+    dR = cal.finite_difference_jacobian(t.rfun[0], t.rfun[1:], var)
+    dfun, step = cal.descent_step(t.rfun[0], dR, t.goal, t.weight)
+    new = t.new_parameters()
+    want = params - step * dfun
+    want = np.maximum(want, np.array(cal.FLOORS))
+    assert np.allclose(new, want, rtol=1e-12, atol=0)
+    assert np.allclose(t.dfun[1:], dfun, rtol=1e-12, atol=0)

@@ -501,8 +501,9 @@ def run_surrogate(args, ws, rank, local):
     batch = 256
     sim = None
     if args.sim_data > 0:
-        Xs, Ys, t_sim = S.simulate_dataset(args.sim_data, seed=1 + rank, uni=S.UniaxialSolver(device=local),
-                                           braz=S.BrazilSolver(device=local))
+        Xs, Ys, t_sim = S.simulate_dataset(args.sim_data, seed=1 + rank,
+                                           uni=S.UniaxialSolver(n=args.sim_size, device=local),
+                                           braz=S.BrazilSolver(n=args.sim_size, device=local), batch=args.sim_batch)
         ok = np.all(np.isfinite(Ys), axis=1) & (Ys[:, 0] > 0) & (Ys[:, 3] > 0)
         Xs, Ys = Xs[ok], Ys[ok]
         lo = np.array([v[0] for v in S_space().values()])
@@ -512,7 +513,10 @@ def run_surrogate(args, ws, rank, local):
         Yn = ((Ys - mu_y) / sd_y).astype(np.float32)
         n_test = max(1, len(Xn) // 10)
         X, Y = Xn[n_test:], Yn[n_test:]
-        sim = dict(cases=int(args.sim_data), kept=int(ok.sum()), seconds=t_sim,
+        if args.sim_save:
+            np.savez(args.sim_save, X=Xs, Y=Ys)
+        sim = dict(cases=int(args.sim_data), kept=int(ok.sum()), seconds=t_sim, spheres=args.sim_size,
+                   batch=args.sim_batch, train=int(len(X)), held_out=int(n_test),
                    solves_per_hour=2 * args.sim_data / t_sim * 3600.0,
                    test=(Xn[:n_test], Yn[:n_test], sd_y))
     else:
@@ -850,6 +854,9 @@ def main() -> int:
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sim-size", type=int, default=2000, help="surrogate --sim-data: spheres per specimen")
+    ap.add_argument("--sim-batch", type=int, default=256, help="surrogate --sim-data: parameter sets per context")
+    ap.add_argument("--sim-save", default="", help="surrogate --sim-data: write the dataset (X, Y) to this .npz")
     ap.add_argument("--sim-data", type=int, default=0,
                     help="surrogate: train on this many simulated parameter sets instead of synthetic targets")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],

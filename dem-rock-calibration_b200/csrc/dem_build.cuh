@@ -9,6 +9,7 @@
 #pragma once
 
 #include "dem_common.cuh"
+#include "dem_params.h"
 #include "dem_types.h"
 
 namespace dem {
@@ -123,6 +124,58 @@ static __global__ void k_sort_cells(const uint32_t* __restrict__ cell_start, uin
   }
 }
 
+// --- per-particle state at set-up, built on the device from the caller's
+// arrays: stage = [x | y | z | r | perm] of all samples (each sample's block
+// of x (and y, z, r, perm) at its p_begin, caller order, perm[k] = the
+// caller index stored at position p_begin + k); integration constants with the
+// host's double formulas (particle_constants), so the values are those the
+// host would compute.
+struct InitSample {
+  uint32_t p_begin, n;
+  double m_ro, dt;
+};
+
+template <class Real>
+__global__ void k_init_particles(const float* __restrict__ stage, uint32_t np, const InitSample* __restrict__ smp,
+                                 uint32_t nsamples, typename RT<Real>::V4* __restrict__ pos,
+                                 typename RT<Real>::V4* __restrict__ vel, typename RT<Real>::V4* __restrict__ omg,
+                                 Real* __restrict__ mass, uint32_t* __restrict__ sid, uint32_t* __restrict__ orig) {
+  const float* X = stage;
+  const float* Y = stage + np;
+  const float* Z = stage + 2 * (size_t)np;
+  const float* R = stage + 3 * (size_t)np;
+  const uint32_t* P = reinterpret_cast<const uint32_t*>(stage + 4 * (size_t)np);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+    // the sample of position p: the last one with p_begin <= p
+    uint32_t lo = 0, hi = nsamples;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (smp[mid].p_begin <= p) lo = mid;
+      else hi = mid;
+    }
+    const InitSample S = smp[lo];
+    const uint32_t q = P[p];                  // caller index within the sample
+    const size_t c = (size_t)S.p_begin + q;  // its entry in the stage
+    const double r = (double)R[c];
+    double m, dtm, dtI;
+    particle_constants(r, S.m_ro, S.dt, m, dtm, dtI);
+    typename RT<Real>::V4 v4;
+    v4.x = (Real)X[c];
+    v4.y = (Real)Y[c];
+    v4.z = (Real)Z[c];
+    v4.w = (Real)R[c];
+    pos[p] = v4;
+    v4.x = v4.y = v4.z = Real(0);
+    v4.w = (Real)dtm;
+    vel[p] = v4;
+    v4.w = (Real)dtI;
+    omg[p] = v4;
+    mass[p] = (Real)m;
+    sid[p] = lo;
+    orig[p] = q;
+  }
+}
+
 // --- pair search over the 27 surrounding cells
 enum PairMode : int {
   kModeRefSet = 0,  // reference interaction set: j != i, r^2 < add && !(r^2 > del) && !(r^2 < 1e-10)
@@ -174,68 +227,111 @@ __device__ __forceinline__ bool pair_pred(const PairSearch<Real>& S, uint32_t i,
   return true;
 }
 
-// One thread per particle; fill=false counts pairs, fill=true writes them in
+// One warp per particle; fill=false counts pairs, fill=true writes them in
 // ascending partner order at offset[i] (kModeRefSet: at i*cap).
+//
+// Lane l < 27 holds cell l of the particle's 3 x 3 x 3 neighbourhood (z
+// outermost, x innermost) with its range in the cell list; an inclusive scan
+// of the ranges' lengths over the lanes numbers the candidates of all 27
+// cells consecutively, and the warp takes them 32 at a time (a lane finds its
+// candidate's cell by a binary search over the scanned lengths, fetched by
+// shuffles).  The candidates are therefore visited in the order of a scan of
+// the cells by z, y, x and of each cell in cell-list order; a ballot ranks the
+// accepted ones in that order, the first min(cap, 48) are kept in shared
+// memory and written out sorted by partner index (each lane places one by
+// counting the smaller ones).  With about 60 candidates a sphere this keeps 32
+// independent gathers in flight per warp where one thread per sphere walked
+// its candidates one dependent load after another.
+constexpr uint32_t kSearchWarps = 4;   // warps (spheres in flight) per 128-thread block
+
+inline uint32_t pair_search_blocks(uint32_t np) { return np ? (np + kSearchWarps - 1) / kSearchWarps : 1u; }
+
 template <class Real, bool kFill>
 __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
+  using V4 = typename RT<Real>::V4;
   constexpr uint32_t kMax = 48;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.np; i += gridDim.x * blockDim.x) {
-    const auto xi = ld4(S.pos + i);
+  constexpr unsigned kFull = 0xFFFFFFFFu;
+  __shared__ uint32_t s_buf[kSearchWarps][kMax];
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t* buf = s_buf[wib];
+  for (uint32_t i = blockIdx.x * kSearchWarps + wib; i < S.np; i += gridDim.x * kSearchWarps) {
+    const V4 xi = ld4(S.pos + i);
     const uint32_t s = S.sid[i];
     const Grid<Real> g = S.grids[s];
     if (at_hidden(g, xi) || (S.done && S.done[s])) {
-      if (!kFill) S.count[i] = 0;
+      if (!kFill && lane == 0) S.count[i] = 0;
       continue;
     }
     const int ix = (int)cell_coord<Real>(xi.x, g.ox, g.inv_a, g.nx);
     const int iy = (int)cell_coord<Real>(xi.y, g.oy, g.inv_a, g.ny);
     const int iz = (int)cell_coord<Real>(xi.z, g.oz, g.inv_a, g.nz);
+    uint32_t cstart = 0, ccount = 0;
+    if (lane < 27) {
+      const int cz = iz + (int)(lane / 9) - 1, cy = iy + (int)((lane / 3) % 3) - 1, cx = ix + (int)(lane % 3) - 1;
+      if (cx >= 0 && cx < (int)g.nx && cy >= 0 && cy < (int)g.ny && cz >= 0 && cz < (int)g.nz) {
+        const uint32_t c = g.off + (uint32_t)cx + (uint32_t)cy * g.nx + (uint32_t)cz * g.ny * g.nx;
+        cstart = S.cell_start[c];
+        ccount = S.cell_start[c + 1] - cstart;
+      }
+    }
+    uint32_t pe = ccount;   // inclusive scan of the lengths
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, pe, d);
+      if (lane >= d) pe += o;
+    }
+    const uint32_t pb = pe - ccount;   // exclusive
+    const uint32_t total = __shfl_sync(kFull, pe, 31);
+    const uint32_t lim = S.cap < kMax ? S.cap : kMax;
     uint32_t n = 0;
-    uint32_t buf[kMax];
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int cz = iz + dz;
-      if (cz < 0 || cz >= (int)g.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int cy = iy + dy;
-        if (cy < 0 || cy >= (int)g.ny) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int cx = ix + dx;
-          if (cx < 0 || cx >= (int)g.nx) continue;
-          const uint32_t c = g.off + (uint32_t)cx + (uint32_t)cy * g.nx + (uint32_t)cz * g.ny * g.nx;
-          for (uint32_t k = S.cell_start[c], e = S.cell_start[c + 1]; k < e; ++k) {
-            const uint32_t j = S.cell_list[k];
-            if (S.mode != kModeRefSet && j <= i) continue;   // each pair once, from its lower index
-            const auto xj = ld4(S.pos + j);
-            if (at_hidden(g, xj) || !pair_pred<Real>(S, i, j, xi, xj, s)) continue;
-            if (kFill && n < kMax && n < S.cap) buf[n] = j;
-            ++n;
-          }
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t v = base + lane;
+      // the cell of candidate v: the first lane c whose inclusive end exceeds v
+      uint32_t lo = 0, hi = 26;
+#pragma unroll
+      for (int step = 0; step < 5; ++step) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t e = __shfl_sync(kFull, pe, mid);
+        if (e > v) hi = mid;
+        else lo = mid + 1;
+      }
+      const uint32_t c = lo < hi ? lo : hi;
+      const uint32_t st = __shfl_sync(kFull, cstart, c), bf = __shfl_sync(kFull, pb, c);
+      bool pass = false;
+      uint32_t j = 0;
+      if (v < total) {
+        j = S.cell_list[st + (v - bf)];
+        if (S.mode == kModeRefSet || j > i) {   // each pair once, from its lower index
+          const V4 xj = ld4(S.pos + j);
+          pass = !at_hidden(g, xj) && pair_pred<Real>(S, i, j, xi, xj, s);
         }
       }
-    }
-    if (!kFill) {
-      S.count[i] = n;
-      if (n > S.cap && S.overflow) atomicAdd(S.overflow, 1u);
-      continue;
-    }
-    const uint32_t m = n < S.cap ? (n < kMax ? n : kMax) : (S.cap < kMax ? S.cap : kMax);
-    // insertion sort by partner index
-    for (uint32_t a = 1; a < m; ++a) {
-      const uint32_t v = buf[a];
-      uint32_t q = a;
-      while (q > 0 && buf[q - 1] > v) {
-        buf[q] = buf[q - 1];
-        --q;
+      const unsigned mask = __ballot_sync(kFull, pass);
+      if (kFill && pass) {
+        const uint32_t r = n + __popc(mask & ((1u << lane) - 1u));
+        if (r < lim) buf[r] = j;
       }
-      buf[q] = v;
+      n += __popc(mask);
     }
-    if (S.mode == kModeRefSet) {
-      uint32_t* o = S.out_j + (size_t)i * S.cap;
-      for (uint32_t a = 0; a < S.cap; ++a) o[a] = a < m ? buf[a] : kEmpty;
+    __syncwarp();
+    if (!kFill) {
+      if (lane == 0) {
+        S.count[i] = n;
+        if (n > S.cap && S.overflow) atomicAdd(S.overflow, 1u);
+      }
     } else {
-      uint32_t* o = S.out_j + S.offset[i];
-      for (uint32_t a = 0; a < m; ++a) o[a] = buf[a];
+      const uint32_t m = n < lim ? n : lim;
+      uint32_t* o = S.mode == kModeRefSet ? S.out_j + (size_t)i * S.cap : S.out_j + S.offset[i];
+      for (uint32_t e = lane; e < m; e += 32) {
+        const uint32_t val = buf[e];
+        uint32_t r = 0;
+        for (uint32_t f = 0; f < m; ++f) r += buf[f] < val ? 1u : 0u;
+        o[r] = val;
+      }
+      if (S.mode == kModeRefSet)
+        for (uint32_t a = m + lane; a < S.cap; a += 32) o[a] = kEmpty;
     }
+    __syncwarp();   // the buffer is refilled for the next sphere
   }
 }
 

@@ -4,13 +4,22 @@
 // dem::EngineBase in dem_capi.cpp.
 #include "dem_engine.h"
 
+#include <unistd.h>
+
 #include <algorithm>
+#include <mutex>
+#include <functional>
+#include <condition_variable>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -75,7 +84,10 @@ struct DBuf {
       n = 0;
       return e;
     }
-    return cudaMemset(p, 0, cnt * sizeof(T));
+    // zero-filled before returning: the fill runs on the legacy default
+    // stream, which is not ordered with the engine's non-blocking stream
+    e = cudaMemsetAsync(p, 0, cnt * sizeof(T), 0);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(0);
   }
   cudaError_t upload(const T* h, size_t cnt) { return cudaMemcpy(p, h, cnt * sizeof(T), cudaMemcpyHostToDevice); }
   cudaError_t download(T* h, size_t cnt) const { return cudaMemcpy(h, p, cnt * sizeof(T), cudaMemcpyDeviceToHost); }
@@ -83,25 +95,115 @@ struct DBuf {
 
 static uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
-// fn(begin, end) over [0, n) split into contiguous ranges on up to 16 host
-// threads (set-up loops over hundreds of thousands of particles); fn must not
+// Host worker threads for the set-up loops, started once per process and
+// reused (starting threads for every loop cost milliseconds per set-up).
+// run(T, fn) calls fn(0) ... fn(T - 1), the calling thread taking its share,
+// and returns when all are done; one run at a time (callers on other host
+// threads wait their turn).
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool pool;
+    return pool;
+  }
+  uint32_t width() const { return (uint32_t)workers_.size() + 1; }
+  void run(uint32_t T, const std::function<void(uint32_t)>& fn) {
+    // (a process forked from this one has no workers: it runs serially)
+    if (T <= 1 || workers_.empty() || getpid() != pid_) {
+      for (uint32_t t = 0; t < T; ++t) fn(t);
+      return;
+    }
+    std::lock_guard<std::mutex> one(run_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &fn;
+      njobs_ = T;
+      next_.store(0);
+      left_ = T;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return left_ == 0; });
+    job_ = nullptr;
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (auto& w : workers_) w.join();
+  }
+
+ private:
+  HostPool() : pid_(getpid()) {
+    const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (uint32_t t = 1; t < hw; ++t) workers_.emplace_back([this] { loop(); });
+  }
+  // take job indices until none is left
+  void work() {
+    for (;;) {
+      const uint32_t t = next_.fetch_add(1);
+      if (t >= njobs_) return;
+      (*job_)(t);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) done_cv_.notify_all();
+    }
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      work();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_, run_mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(uint32_t)>* job_ = nullptr;
+  uint32_t njobs_ = 0, left_ = 0;
+  std::atomic<uint32_t> next_{0};
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+  pid_t pid_;
+};
+
+// the chunk count parallel_chunks uses for n items: one per 32,768 items, at
+// most one per host worker
+static uint32_t chunk_count(uint32_t n) {
+  return std::max(1u, std::min(HostPool::get().width(), n / 32768u));
+}
+
+// fn(t, k0, k1) for the T contiguous chunks of [0, n) on the host workers
+// (the same boundaries for the same n and T); fn must not throw
+template <class Fn>
+static void parallel_chunks(uint32_t n, uint32_t T, Fn fn) {
+  if (T <= 1) {
+    fn(0u, 0u, n);
+    return;
+  }
+  HostPool::get().run(T, [&](uint32_t t) {
+    fn(t, (uint32_t)((uint64_t)n * t / T), (uint32_t)((uint64_t)n * (t + 1) / T));
+  });
+}
+
+// fn(begin, end) over [0, n) split into contiguous ranges on the host
+// workers (set-up loops over hundreds of thousands of particles); fn must not
 // throw and its ranges must write disjoint data.
 template <class Fn>
 static void parallel_ranges(uint32_t n, Fn fn) {
-  const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  const uint32_t T = std::max(1u, std::min(hw, n / 32768u));
-  if (T == 1) {
-    fn(0u, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  th.reserve(T);
-  for (uint32_t t = 0; t < T; ++t)
-    th.emplace_back(fn, (uint32_t)((uint64_t)n * t / T), (uint32_t)((uint64_t)n * (t + 1) / T));
-  for (auto& x : th) x.join();
+  parallel_chunks(n, chunk_count(n), [&](uint32_t, uint32_t k0, uint32_t k1) { fn(k0, k1); });
 }
 
-// 30-bit Morton interleave of three 10-bit coordinates
+// 63-bit Morton interleave of three 21-bit coordinates
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   auto spread = [](uint64_t v) {
     v &= 0x1FFFFF;
@@ -192,10 +294,31 @@ class Engine final : public EngineBase {
   }
 
   // ---------------------------------------------------------------- set-up
+  // DEM_TRACE=1 in the environment: set-up phase times on stderr (the
+  // stream is drained at each mark, so the device work of a phase counts in it)
+  struct PhaseTrace {
+    bool on = std::getenv("DEM_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    std::string line;
+    void mark(const char* what, cudaStream_t st) {
+      if (!on) return;
+      cudaStreamSynchronize(st);
+      const auto now = std::chrono::steady_clock::now();
+      char b[96];
+      std::snprintf(b, sizeof b, " %s %.2f ms", what, std::chrono::duration<double, std::milli>(now - t).count());
+      line += b;
+      t = now;
+    }
+    void flush(const char* head) {
+      if (on) std::fprintf(stderr, "dem trace: %s%s\n", head, line.c_str());
+    }
+  };
+
   int setup() override {
     if (setup_done_) return DEM_ERR_STATE;
     if (samples_.empty()) return DEM_ERR_STATE;
     CK(cudaSetDevice(opt_.device));
+    PhaseTrace tr;
     const uint32_t S = (uint32_t)samples_.size();
     np_ = 0;
     for (auto& s : samples_) {
@@ -204,28 +327,9 @@ class Engine final : public EngineBase {
       derive(s);
       morton_order(s);
     }
-    // per-particle host arrays in storage order
-    std::vector<V4> hpos(np_), hvel(np_), homg(np_);
-    std::vector<Real> hmass(np_);
-    std::vector<uint32_t> hsid(np_), horig(np_);
-    for (uint32_t si = 0; si < S; ++si) {
-      const SampleHost& s = samples_[si];
-      parallel_ranges(s.n, [&](uint32_t k0, uint32_t k1) {
-        for (uint32_t k = k0; k < k1; ++k) {
-          const uint32_t q = s.perm[k];
-          const uint32_t p = s.p_begin + k;
-          const double r = s.rad[q];
-          double m, dtm, dtI;
-          particle_constants(r, s.pot.m_ro, s.dt, m, dtm, dtI);
-          hpos[p] = make4((Real)s.xyz[q], (Real)s.xyz[s.n + q], (Real)s.xyz[2 * s.n + q], (Real)s.rad[q]);
-          hvel[p] = make4(Real(0), Real(0), Real(0), (Real)dtm);
-          homg[p] = make4(Real(0), Real(0), Real(0), (Real)dtI);
-          hmass[p] = (Real)m;
-          hsid[p] = si;
-          horig[p] = q;
-        }
-      });
-    }
+    tr.mark("order", stream_);
+    // per-particle state, built on the device from the caller's arrays (one
+    // upload of positions, radii and the storage order per sample)
     CK(pos_.alloc(np_));
     CK(vel_.alloc(np_));
     CK(omg_.alloc(np_));
@@ -241,21 +345,42 @@ class Engine final : public EngineBase {
     CK(mass_.alloc(np_));
     CK(sid_.alloc(np_));
     CK(orig_.alloc(np_));
-    CK(pos_.upload(hpos.data(), np_));
-    CK(vel_.upload(hvel.data(), np_));
-    CK(omg_.upload(homg.data(), np_));
-    CK(mass_.upload(hmass.data(), np_));
-    CK(sid_.upload(hsid.data(), np_));
-    CK(orig_.upload(horig.data(), np_));
+    {
+      DBuf<float> stage;
+      DBuf<InitSample> tab;
+      CK(stage.alloc(5 * (size_t)np_));
+      std::vector<InitSample> ht(S);
+      for (uint32_t si = 0; si < S; ++si) {
+        const SampleHost& s = samples_[si];
+        ht[si] = InitSample{s.p_begin, s.n, s.pot.m_ro, s.dt};
+        for (int d = 0; d < 4; ++d) {
+          const float* src = d < 3 ? s.xyz.data() + (size_t)d * s.n : s.rad.data();
+          CK(cudaMemcpyAsync(stage.p + (size_t)d * np_ + s.p_begin, src, s.n * sizeof(float), cudaMemcpyHostToDevice,
+                             stream_));
+        }
+        CK(cudaMemcpyAsync(stage.p + 4 * (size_t)np_ + s.p_begin, s.perm.data(), s.n * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, stream_));
+      }
+      CK(tab.alloc(S));
+      CK(cudaMemcpyAsync(tab.p, ht.data(), S * sizeof(InitSample), cudaMemcpyHostToDevice, stream_));
+      k_init_particles<Real><<<grid1(np_), 256, 0, stream_>>>(stage.p, np_, tab.p, S, pos_.p, vel_.p, omg_.p, mass_.p,
+                                                             sid_.p, orig_.p);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(stream_));   // the stage and the host table are released here
+    }
+    tr.mark("upload", stream_);
     RC(mark_lateral());
     // per-sample constants and controllers
     RC(upload_params());
     // contact grids
     RC(make_grids());
+    tr.mark("params", stream_);
     // bonds
     RC(build_bonds());
+    tr.mark("bonds", stream_);
     // contact list
     RC(build_contacts(true));
+    tr.mark("contacts", stream_);
     RC(init_controllers());
     CK(blocks_done_.alloc(1));
     if (DualK<Real>::K) CK(sfl_tan_.alloc((size_t)S * (4 * DualK<Real>::K + 2)));
@@ -271,7 +396,10 @@ class Engine final : public EngineBase {
     // the step graphs are captured and instantiated here, so that no later
     // call pays for an instantiation inside its own time (they are captured
     // again only after a change that invalidates them)
+    tr.mark("rest", stream_);
     RC(capture_all());
+    tr.mark("graphs", stream_);
+    tr.flush("setup");
     return DEM_OK;
   }
 
@@ -407,44 +535,85 @@ class Engine final : public EngineBase {
   }
 
   void morton_order(SampleHost& s) {
-    const double q = std::max(s.rmin, 1e-6);
+    const uint32_t n = s.n;
+    const uint32_t T = chunk_count(n);
+    const double inv_q = 1.0 / std::max(s.rmin, 1e-6);
+    // lower corner of the particles (per-chunk minima, then combined)
+    std::vector<double> clo(3 * (size_t)T, 1e300);
+    parallel_chunks(n, T, [&](uint32_t t, uint32_t k0, uint32_t k1) {
+      for (int d = 0; d < 3; ++d) {
+        double m = 1e300;
+        for (uint32_t i = k0; i < k1; ++i) m = std::min(m, (double)s.xyz[d * n + i]);
+        clo[3 * t + d] = m;
+      }
+    });
     double lo[3] = {1e300, 1e300, 1e300};
-    for (uint32_t i = 0; i < s.n; ++i)
-      for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], (double)s.xyz[d * s.n + i]);
-    std::vector<uint64_t> key(s.n);
-    parallel_ranges(s.n, [&](uint32_t i0, uint32_t i1) {
+    for (uint32_t t = 0; t < T; ++t)
+      for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], clo[3 * t + d]);
+    // keys, and their largest value (only the digits below its top bit vary)
+    // (left uninitialised: every entry is written before it is read)
+    std::unique_ptr<uint64_t[]> ka(new uint64_t[n]), kb(new uint64_t[n]);
+    std::unique_ptr<uint32_t[]> pa(new uint32_t[n]), pb(new uint32_t[n]);
+    std::vector<uint64_t> kmax(T, 0);
+    parallel_chunks(n, T, [&](uint32_t t, uint32_t i0, uint32_t i1) {
+      uint64_t m = 0;
       for (uint32_t i = i0; i < i1; ++i) {
         uint32_t c[3];
         for (int d = 0; d < 3; ++d) {
-          double v = ((double)s.xyz[d * s.n + i] - lo[d]) / q;
+          double v = ((double)s.xyz[d * n + i] - lo[d]) * inv_q;
           c[d] = (uint32_t)std::min(std::max(v, 0.0), 2097151.0);
         }
-        key[i] = morton3(c[0], c[1], c[2]);
+        ka[i] = morton3(c[0], c[1], c[2]);
+        pa[i] = i;
+        m = std::max(m, ka[i]);
       }
+      kmax[t] = m;
     });
-    // stable LSD radix sort of the particle indices by key (16-bit digits over
-    // the 63 key bits): equal keys keep ascending index order
-    s.perm.resize(s.n);
-    std::vector<uint32_t> tmp(s.n);
-    for (uint32_t i = 0; i < s.n; ++i) s.perm[i] = i;
-    std::vector<uint32_t> count(65537);
-    for (int shift = 0; shift < 64; shift += 16) {
-      std::fill(count.begin(), count.end(), 0u);
-      for (uint32_t i = 0; i < s.n; ++i) ++count[((key[i] >> shift) & 0xFFFF) + 1];
-      bool one_bucket = false;
-      for (uint32_t b = 0; b < 65536; ++b) {
-        if (count[b + 1] == s.n) one_bucket = true;
-        count[b + 1] += count[b];
-      }
-      if (one_bucket) continue;   // this digit is the same for every key
-      for (uint32_t k = 0; k < s.n; ++k) {
-        const uint32_t i = s.perm[k];
-        tmp[count[(key[i] >> shift) & 0xFFFF]++] = i;
-      }
-      s.perm.swap(tmp);
+    uint64_t km = 0;
+    for (uint64_t m : kmax) km = std::max(km, m);
+    int bits = 0;
+    while (bits < 64 && (km >> bits) != 0) ++bits;
+    // stable LSD radix sort of (key, index) pairs, 8-bit digits, each pass in
+    // parallel: per-chunk digit counts, offsets bucket by bucket and chunk by
+    // chunk, then every chunk scatters its items in order, so equal keys keep
+    // ascending index order
+    std::vector<uint32_t> hist(256 * (size_t)T);
+    for (int shift = 0; shift < bits; shift += 8) {
+      parallel_chunks(n, T, [&](uint32_t t, uint32_t k0, uint32_t k1) {
+        uint32_t* h = &hist[256 * (size_t)t];
+        std::fill(h, h + 256, 0u);
+        for (uint32_t k = k0; k < k1; ++k) ++h[(ka[k] >> shift) & 255];
+      });
+      uint32_t run = 0;
+      for (uint32_t d = 0; d < 256; ++d)
+        for (uint32_t t = 0; t < T; ++t) {
+          const uint32_t c = hist[256 * (size_t)t + d];
+          hist[256 * (size_t)t + d] = run;
+          run += c;
+        }
+      parallel_chunks(n, T, [&](uint32_t t, uint32_t k0, uint32_t k1) {
+        uint32_t* h = &hist[256 * (size_t)t];
+        for (uint32_t k = k0; k < k1; ++k) {
+          const uint32_t o = h[(ka[k] >> shift) & 255]++;
+          kb[o] = ka[k];
+          pb[o] = pa[k];
+        }
+      });
+      ka.swap(kb);
+      pa.swap(pb);
     }
-    s.inv.resize(s.n);
-    for (uint32_t k = 0; k < s.n; ++k) s.inv[s.perm[k]] = k;
+    s.perm.resize(n);
+    parallel_ranges(n, [&](uint32_t k0, uint32_t k1) { std::copy(pa.get() + k0, pa.get() + k1, s.perm.data() + k0); });
+    s.inv.clear();   // built when first needed (inverse())
+  }
+
+  // caller index -> storage position of a sample
+  const std::vector<uint32_t>& inverse(SampleHost& s) {
+    if (s.inv.size() != s.n) {
+      s.inv.resize(s.n);
+      for (uint32_t k = 0; k < s.n; ++k) s.inv[s.perm[k]] = k;
+    }
+    return s.inv;
   }
 
   static V4 make4(Real a, Real b, Real c, Real d) {
@@ -657,7 +826,7 @@ class Engine final : public EngineBase {
     PairSearch<Real> S = search_args(kModeBond);
     S.gap = gap_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
-    k_pair_search<Real, false><<<grid1(np_), 128, 0, stream_>>>(S);
+    k_pair_search<Real, false><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     RC(scan(cnt_.p, offs_.p, np_));
     uint32_t nb = 0, ovf = 0;
     CK(cudaMemcpyAsync(&nb, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
@@ -668,7 +837,7 @@ class Engine final : public EngineBase {
     DBuf<uint32_t> js;
     CK(js.alloc(std::max(nb, 1u)));
     S.out_j = js.p;
-    k_pair_search<Real, true><<<grid1(np_), 128, 0, stream_>>>(S);
+    k_pair_search<Real, true><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     // whole tiles: the pair kernel copies bond state tile by tile
     const size_t nb_pad = ((size_t)std::max(nb, 1u) + 255) / 256 * 256;
     CK(b_ij_.alloc(nb_pad));
@@ -782,7 +951,7 @@ class Engine final : public EngineBase {
     S.b_row = b_row_.p;
     S.b_ij = b_ij_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
-    k_pair_search<Real, false><<<grid1(np_), 128, 0, stream_>>>(S);
+    k_pair_search<Real, false><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     RC(scan(cnt_.p, offs_.p, np_));
     uint32_t nc = 0, ovf = 0;
     CK(cudaMemcpyAsync(&nc, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
@@ -822,7 +991,7 @@ class Engine final : public EngineBase {
       }
     }
     S.out_j = c_js_.p;
-    k_pair_search<Real, true><<<grid1(np_), 128, 0, stream_>>>(S);
+    k_pair_search<Real, true><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_js_.p, c_ij_new_.p);
     if (nc) {
       if (first)
@@ -1271,13 +1440,22 @@ class Engine final : public EngineBase {
   // Runs until max_steps steps or (stop_when_done) until every sample is done.
   // A sample whose state turned non-finite is stopped by the controller; the
   // others run on, and the call then returns DEM_ERR_NUMERIC.
-  int run(uint64_t max_steps, uint64_t* done_steps, bool stop_when_done) {
+  // ev (optional, two events): ev[0] is recorded once the state of the last
+  // call has been read (before any contact-list rebuild of this call), ev[1]
+  // after the launches of each chunk, so that [ev[0], ev[1]] spans the device
+  // work of these steps and the host work between their chunks, and not the
+  // bookkeeping at either end of the call.
+  int run(uint64_t max_steps, uint64_t* done_steps, bool stop_when_done, cudaEvent_t* ev = nullptr) {
     RC(prepare());
     uint64_t steps = 0;
     Flags f{};
     RC(read_flags(f));
     const uint32_t numeric_before = f.numeric;
     RC(update_tiles());
+    if (ev) {
+      CK(cudaEventRecord(ev[0], stream_));
+      CK(cudaEventRecord(ev[1], stream_));
+    }
     while (true) {
       if (f.stale) {
         // a particle outran the speed margin (violent fracture): chunks are
@@ -1300,6 +1478,7 @@ class Engine final : public EngineBase {
       } else {
         RC(run_short_chunk(chunk));
       }
+      if (ev) CK(cudaEventRecord(ev[1], stream_));
       steps += chunk;
       CK(cudaGetLastError());
       RC(read_flags(f));
@@ -1668,7 +1847,8 @@ class Engine final : public EngineBase {
                 const float* st) override {
     if (si < 0 || (size_t)si >= samples_.size() || !setup_done_) return DEM_ERR_ARG;
     RC(prepare());
-    const SampleHost& s = samples_[si];
+    SampleHost& s = samples_[si];
+    const std::vector<uint32_t>& inv = inverse(s);
     CK(cudaStreamSynchronize(stream_));
     std::vector<uint2> bij(nb_), cij(nc_host_);
     std::vector<V4> s0(nb_), s1(nb_), s2(nb_), par(nb_), co(nc_host_);
@@ -1685,7 +1865,7 @@ class Engine final : public EngineBase {
     }
     std::vector<int32_t> delta(samples_.size(), 0);
     for (uint32_t k = 0; k < cnt; ++k) {
-      uint32_t a = s.inv[ii[k]] + s.p_begin, b = s.inv[jj[k]] + s.p_begin;
+      uint32_t a = inv[ii[k]] + s.p_begin, b = inv[jj[k]] + s.p_begin;
       float v[13];
       std::memcpy(v, st + 13 * (size_t)k, sizeof(v));  // set_pairs takes the 13-value state
       if (a > b) {
@@ -1768,18 +1948,21 @@ class Engine final : public EngineBase {
   }
   void* stream() override { return (void*)stream_; }
 
+  // Device time of nsteps steps: from the first step's launch (after the
+  // call has read the state the last call left) to the end of the last step
+  // (the flag read-back after it is not included); rebuilds and host checks
+  // between chunks are.
   int run_timed(uint64_t nsteps, double* ms) override {
     RC(prepare());
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
-    CK(cudaEventRecord(a, stream_));
+    cudaEvent_t ev[2];
+    CK(cudaEventCreate(&ev[0]));
+    CK(cudaEventCreate(&ev[1]));
     uint64_t done = 0;
-    int rc = run(nsteps, &done, false);
-    CK(cudaEventRecord(b, stream_));
-    CK(cudaEventSynchronize(b));
+    int rc = run(nsteps, &done, false, ev);
+    CK(cudaEventSynchronize(ev[1]));
     float t = 0.f;
-    CK(cudaEventElapsedTime(&t, a, b));
+    CK(cudaEventElapsedTime(&t, ev[0], ev[1]));
+    cudaEvent_t a = ev[0], b = ev[1];
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (ms) *ms = t;
@@ -2018,7 +2201,7 @@ int ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32
   S.out_j = out.p;
   S.cap = cap;
   S.overflow = ovf.p;
-  const uint32_t gb = std::max(1u, ceil_div(n, 128));
+  const uint32_t gb = pair_search_blocks(n);
   k_pair_search<float, false><<<gb, 128>>>(S);
   k_pair_search<float, true><<<gb, 128>>>(S);
   if (cudaDeviceSynchronize()) return DEM_ERR_CUDA;

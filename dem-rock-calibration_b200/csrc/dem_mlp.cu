@@ -104,22 +104,28 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 // GELU in the tanh form of Hendrycks & Gimpel (2016),
 //   gelu(z) = z/2 (1 + tanh(u)) = z s,  s = 1 / (1 + exp(-2u)),
 //   u = sqrt(2/pi) (z + 0.044715 z^3),
-// evaluated as z s with the hardware exponential (__expf) and reciprocal
-// (rcp.approx), which keep their relative accuracy in both tails (the form
-// 1 + tanh(u) cancels for large negative z); its derivative
+// evaluated as z s with the hardware base-2 exponential (ex2.approx, with
+// exp(-2u) = 2^(-2u log2 e) and the three constant factors folded into one)
+// and reciprocal (rcp.approx), which keep their relative accuracy in both
+// tails (the form 1 + tanh(u) cancels for large negative z); its derivative
 //   gelu'(z) = s + 2 z s (1 - s) sqrt(2/pi) (1 + 3 0.044715 z^2).
 // ReLU takes 0 as its derivative at 0, as sklearn's MLPRegressor does
 // (NN_MP.py:374 uses its default activation).
 constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2/pi)
 constexpr float kGeluA = 0.044715f;
+constexpr float kGeluE = (float)(-2.0 * 0.7978845608028654 * 1.4426950408889634);   // -2 sqrt(2/pi) log2(e)
 __device__ __forceinline__ float rcp_hw(float x) {
   float y;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ float ex2_hw(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu_s(float z) {
-  const float u = kGeluC * __fmaf_rn(kGeluA * z * z, z, z);
-  return rcp_hw(1.f + __expf(-2.f * u));
+  return rcp_hw(1.f + ex2_hw(kGeluE * __fmaf_rn(kGeluA * z * z, z, z)));
 }
 __device__ __forceinline__ float gelu(float z) { return z * gelu_s(z); }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -142,20 +148,9 @@ struct GemmCfg {
   static constexpr uint32_t kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : (TN <= 128 ? 128 : 256));
 };
 
-// Epilogue of one 32-column chunk of an accumulator row: tcgen05.ld of the
-// thread's 32 consecutive FP32 columns (TMEM address taddr: lane quarter of
-// the warp, column), then + bias and the activation to BF16 and/or the FP32
-// values, written with 16-byte stores (scalar stores at a ragged right edge
-// or when a row is not a multiple of 16 bytes).  Every lane of the warp takes
-// part in the load; rows >= M and columns >= N are not written.  kBias4: the
-// bias is a zero-padded shared-memory copy read as 16-byte vectors (the same
-// address in every lane: one broadcast per vector); otherwise it is read from
-// global memory value by value.
-template <bool kBias4 = false>
-__device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int M, int N,
-                                            const float* __restrict__ bias, int mode, bool act,
-                                            float* __restrict__ outf, __nv_bfloat16* __restrict__ outh) {
-  uint32_t r[32];
+// 32 consecutive FP32 accumulator columns of this thread's row (TMEM address
+// taddr: lane quarter of the warp, column), without waiting for them
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -166,7 +161,20 @@ __device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int
         "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr)
       : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Epilogue of one 32-column chunk of an accumulator row, its values r already
+// loaded from tensor memory: + bias and the activation to BF16 and/or the
+// FP32 values, written with 16-byte stores (scalar stores at a ragged right
+// edge or when a row is not a multiple of 16 bytes); rows >= M and columns >=
+// N are not written.  kBias4: the bias is a zero-padded shared-memory copy
+// read as 16-byte vectors (the same address in every lane: one broadcast per
+// vector); otherwise it is read from global memory value by value.
+template <bool kBias4 = false>
+__device__ __forceinline__ void chunk_out(const uint32_t (&r)[32], int row, int nc, int M, int N,
+                                          const float* __restrict__ bias, int mode, bool act,
+                                          float* __restrict__ outf, __nv_bfloat16* __restrict__ outh) {
   if (row >= M || nc >= N) return;
   const int cols = min(32, N - nc);
   float v[32];
@@ -221,6 +229,18 @@ __device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int
         if (j < cols) dst[j] = (unsigned short)((j & 1) ? (h[j >> 1] >> 16) : (h[j >> 1] & 0xFFFFu));
     }
   }
+}
+
+// One chunk loaded, waited for and written (every lane of the warp takes part
+// in the load).
+template <bool kBias4 = false>
+__device__ __forceinline__ void drain_chunk(uint32_t taddr, int row, int nc, int M, int N,
+                                            const float* __restrict__ bias, int mode, bool act,
+                                            float* __restrict__ outf, __nv_bfloat16* __restrict__ outh) {
+  uint32_t r[32];
+  tmem_ld32(taddr, r);
+  tmem_wait_ld();
+  chunk_out<kBias4>(r, row, nc, M, N, bias, mode, act, outf, outh);
 }
 
 // Warp-specialised: warp 0 lane 0 streams the stages with the TMA (A box
@@ -504,8 +524,17 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
       tc_fence_after();
       const int row = t * kTM + q4 * 32 + lane;
       const uint32_t acc = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)a * kAcc;
-      for (int col0 = 32 * cg; col0 < TN; col0 += 128)
-        drain_chunk<true>(acc + (uint32_t)col0, row, col0, M, N, sbias, mode, act, outf, outh);
+      // a warp's chunks cg and cg + 4 (TN = 256) are loaded together before
+      // one wait, so that their 64 values give the arithmetic independent work
+      for (int col0 = 32 * cg; col0 < TN; col0 += 256) {
+        uint32_t ra[32], rb[32];
+        const bool two = col0 + 128 < TN;
+        tmem_ld32(acc + (uint32_t)col0, ra);
+        if (two) tmem_ld32(acc + (uint32_t)(col0 + 128), rb);
+        tmem_wait_ld();
+        chunk_out<true>(ra, row, col0, M, N, sbias, mode, act, outf, outh);
+        if (two) chunk_out<true>(rb, row, col0 + 128, M, N, sbias, mode, act, outf, outh);
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) bar_arrive(&tempty[a]);
@@ -664,7 +693,10 @@ int err_flag(unsigned int** out) {
   if (!g_err[dev]) {
     unsigned int* p = nullptr;
     if (cudaMalloc((void**)&p, sizeof(unsigned int)) != cudaSuccess) return DEM_ERR_CUDA;
-    if (cudaMemset(p, 0, sizeof(unsigned int)) != cudaSuccess) return DEM_ERR_CUDA;
+    // zeroed before any caller stream uses it (the caller's stream may not be
+    // ordered with the legacy default stream)
+    if (cudaMemsetAsync(p, 0, sizeof(unsigned int), 0) != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess)
+      return DEM_ERR_CUDA;
     g_err[dev] = p;
   }
   *out = g_err[dev];

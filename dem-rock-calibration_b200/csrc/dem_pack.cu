@@ -33,7 +33,10 @@ struct Buf {
     if (!k) return cudaSuccess;
     cudaError_t e = cudaMalloc((void**)&p, k * sizeof(T));
     if (e) return e;
-    return cudaMemset(p, 0, k * sizeof(T));
+    // zero-filled before returning: the fill runs on the legacy default
+    // stream, which is not ordered with the packer's non-blocking stream
+    e = cudaMemsetAsync(p, 0, k * sizeof(T), 0);
+    return e ? e : cudaStreamSynchronize(0);
   }
 };
 
@@ -97,7 +100,7 @@ class Packer {
     CKP(vel.alloc(n));
     CKP(frc.alloc(n));
     CKP(frcq.alloc(4 * (size_t)n));
-    CKP(cudaMemset(frcq.p, 0, 4 * (size_t)n * sizeof(long long)));
+    CKP(cudaMemsetAsync(frcq.p, 0, 4 * (size_t)n * sizeof(long long), st));
     CKP(part.alloc(3 * (size_t)nsm * 8));
     CKP(ref.alloc(n));
     CKP(sid.alloc(n));
@@ -269,8 +272,8 @@ class Packer {
     n_ = m;
     CKP(cudaMemcpy(pos.p, hp.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
     CKP(cudaMemcpy(vel.p, hv.data(), m * sizeof(float4), cudaMemcpyHostToDevice));
-    CKP(cudaMemset(frc.p, 0, n * sizeof(float4)));
-    CKP(cudaMemset(frcq.p, 0, 4 * (size_t)n * sizeof(long long)));
+    CKP(cudaMemsetAsync(frc.p, 0, n * sizeof(float4), st));
+    CKP(cudaMemsetAsync(frcq.p, 0, 4 * (size_t)n * sizeof(long long), st));
     return DEM_OK;
   }
 
@@ -301,7 +304,7 @@ class Packer {
     S.cap = 48;
     S.overflow = ovf.p;
     CKP(cudaMemsetAsync(ovf.p, 0, sizeof(uint32_t), st));
-    k_pair_search<float, false><<<std::max(1u, cdiv(n, 128)), 128, 0, st>>>(S);
+    k_pair_search<float, false><<<pair_search_blocks(n), 128, 0, st>>>(S);
     rc = scan(cnt.p, offs.p, n);
     if (rc) return rc;
     uint32_t nc = 0, o = 0;
@@ -314,7 +317,7 @@ class Packer {
       CKP(js.alloc(nc + nc / 2 + 1024));
     }
     S.out_j = js.p;
-    k_pair_search<float, true><<<std::max(1u, cdiv(n, 128)), 128, 0, st>>>(S);
+    k_pair_search<float, true><<<pair_search_blocks(n), 128, 0, st>>>(S);
     k_expand_pairs<<<g1, 256, 0, st>>>(offs.p, n, js.p, cij.p);
     CKP(cudaMemcpyAsync(nc_dev.p, &nc, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     k_copy_pos<float><<<g1, 256, 0, st>>>(pos.p, ref.p, n);

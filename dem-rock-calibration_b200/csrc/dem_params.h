@@ -47,6 +47,9 @@ struct Potential {
 
 // Per-particle integration constants with the reference's formulas for a
 // particle of radius r (p_V, p_m, p_1d_m, p_I, dt_d_m, dt_d_I).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
 inline void particle_constants(double r, double m_ro, double dt, double& mass, double& dtm, double& dtI) {
   const double V = 4.0 * (1.0 / 3.0) * kPiD * r * r * r;
   mass = m_ro * V;

@@ -228,16 +228,16 @@ __device__ __forceinline__ void scatter_pair(const StepArgs<Real>& A, uint32_t i
   if (!dropJ) acc_m(A, j, mJ[0], mJ[1], mJ[2]);
 }
 
-// Sum of v over the run of lanes of this warp that share key (keys sorted
-// along the lanes, all 32 lanes active): a segmented suffix sum by shuffles;
-// the run's first lane ends with the run's total.
+// Sum of v over the run of lanes of this warp that share a key (keys sorted
+// along the lanes, all 32 lanes active; run_end = the first lane after this
+// lane's run): a segmented suffix sum by shuffles; the run's first lane ends
+// with the run's total.
 template <class T, int N>
-__device__ __forceinline__ void warp_run_sum(uint32_t key, T (&v)[N]) {
+__device__ __forceinline__ void warp_run_sum(uint32_t run_end, T (&v)[N]) {
   const uint32_t lane = threadIdx.x & 31;
 #pragma unroll
   for (uint32_t d = 1; d < 32; d <<= 1) {
-    const uint32_t ko = __shfl_down_sync(0xFFFFFFFFu, key, d);
-    const bool same = lane + d < 32 && ko == key;
+    const bool same = lane + d < run_end;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const T o = __shfl_down_sync(0xFFFFFFFFu, v[k], d);
@@ -264,6 +264,11 @@ __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t
       // every lane takes part in the shuffle (no short-circuit around it)
       const uint32_t iu = __shfl_up_sync(0xFFFFFFFFu, i, 1);
       const bool head = lane == 0 || iu != i;
+      // end of this lane's run: the next run head above it (one ballot
+      // instead of a key shuffle per round of the segmented sum)
+      const unsigned heads = __ballot_sync(0xFFFFFFFFu, head);
+      const unsigned above = lane < 31 ? heads & (~0u << (lane + 1)) : 0u;
+      const uint32_t run_end = above ? (uint32_t)(__ffs(above) - 1) : 32u;
       if (A.det) {
         long long q[6];
         if constexpr (sizeof(Real) == 4) {
@@ -273,7 +278,7 @@ __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t
           q[0] = fix_of(f0); q[1] = fix_of(f1); q[2] = fix_of(f2);
           q[3] = fix_of(m0); q[4] = fix_of(m1); q[5] = fix_of(m2);
         }
-        warp_run_sum(i, q);
+        warp_run_sum(run_end, q);
         if (head) {
           unsigned long long* uf;
           unsigned long long* um;
@@ -292,7 +297,7 @@ __device__ __forceinline__ void scatter_i_warp(const StepArgs<Real>& A, uint32_t
         }
       } else {
         Real v[6] = {f0, f1, f2, m0, m1, m2};
-        warp_run_sum(i, v);
+        warp_run_sum(run_end, v);
         if (head) {
           acc3(A.frc + i, v[0], v[1], v[2]);
           acc3(A.mom + i, v[3], v[4], v[5]);
@@ -654,9 +659,12 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
                                              Real riwm, Real ri, Real mi, const typename RT<Real>::V4& v,
                                              const typename RT<Real>::V4& w, Real o[3], Real F[3], Real M[3]) {
   using T = RT<Real>;
-  Real niw[3] = {0, 0, 0}, wv[3] = {0, 0, 0};
-  niw[axis] = sgn;
-  wv[axis] = wallvel;
+  // the platen normal and velocity lie along the loading axis, y (Brazilian)
+  // or z (uniaxial); selects instead of an indexed store keep them in registers
+  const bool a1 = axis == 1, a2 = axis == 2;
+  const Real zero = Real(0);
+  const Real niw[3] = {zero, a1 ? sgn : zero, a2 ? sgn : zero};
+  const Real wv[3] = {zero, a1 ? wallvel : zero, a2 ? wallvel : zero};
   Real cef1 = T::sqrt_rn(ri * T::fabs_(ri - riwm));
   const Real Kn = Real(2) * sp.wallE * cef1;
   const Real Kt = Real(8) * sp.wallG * cef1;
@@ -721,7 +729,7 @@ __device__ __forceinline__ Real wall_contact(const SampleParams<Real>& sp, int a
   M[0] += mt[0] + madd[0];
   M[1] += mt[1] + madd[1];
   M[2] += mt[2] + madd[2];
-  return fiwn[axis];
+  return a2 ? fiwn[2] : fiwn[1];
 }
 
 // Loading controller of one sample after its platen force sums are complete:
@@ -780,6 +788,28 @@ __device__ inline void controller_step(SampleCtl& C) {
   // loop condition of h_Calculation{UniaxialCompression,BrazilTest}; a sample
   // whose state went non-finite also stops
   if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps || C.numeric) C.done = 1;
+}
+
+// The controllers of all samples, run by the last block of the particle
+// kernel once every block's platen sums are in.  Not inlined: its private
+// copy of a sample's state (one load, one store back instead of a chain of
+// dependent global accesses) lives in this function's frame, not in the
+// particle loop's registers.
+template <class Real>
+__device__ __noinline__ void run_controllers(const StepArgs<Real> A) {
+  for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
+    if (A.ctl[s].done) continue;
+    SampleCtl C = A.ctl[s];
+    // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
+    C.sFL[0] += (double)C.sFLq[0] * kFixInv;
+    C.sFL[1] += (double)C.sFLq[1] * kFixInv;
+    C.lat_sum += (double)C.lat_q * kFixInv;
+    C.sFLq[0] = C.sFLq[1] = C.lat_q = 0;
+    tangent_step_end(A, C, s);
+    controller_step(C);
+    A.ctl[s] = C;
+  }
+  if (threadIdx.x == 0) *A.blocks_done = 0;
 }
 
 template <class Real>
@@ -877,7 +907,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
         // one: nothing to read or write.
         if (lat < Real(sp.wall_RR) && r[2] < Real(sp.zcut)) {
           const Real wtop = Real(cached ? c_wall[s][0] : (float)C.Top), wbot = Real(cached ? c_wall[s][1] : (float)C.Bottom);
-          const bool top = wtop - r[ax] < x.w, bot = r[ax] - wbot < x.w;
+          const Real rax = ax == 2 ? r[2] : r[1];   // coordinate along the loading axis
+          const bool top = wtop - rax < x.w, bot = rax - wbot < x.w;
           const uint8_t had = A.wflag[p];
           if (top || bot || had) {
             const Real wvel = Real(cached ? c_wall[s][2] : (float)C.V);
@@ -885,7 +916,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
             Real o[3] = {o4.x, o4.y, o4.z};
             const Real ri = x.w, mi = A.mass[p];
             if (top) {
-              const Real f = wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - r[ax]), ri, mi, v, w, o, F, M);
+              const Real f = wall_contact<Real>(sp, ax, Real(1), wvel, T::fabs_(wtop - rax), ri, mi, v, w, o, F, M);
               st = -(double)f;
               tangent_wall(A, s, 1, f);
             } else {
@@ -893,7 +924,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
             }
             if (bot) {
               const Real f =
-                  wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - r[ax]), ri, mi, v, w, o, F, M);
+                  wall_contact<Real>(sp, ax, Real(-1), -wvel, T::fabs_(wbot - rax), ri, mi, v, w, o, F, M);
               sb = -(double)f;
               tangent_wall(A, s, 0, f);
             } else {
@@ -974,6 +1005,12 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
     // issues one atomic; otherwise each contributing lane adds its own value.  In
     // deterministic mode every particle's terms are first rounded to fixed point
     // and summed as integers (exact, independent of the warp a particle falls in).
+    // Most warps hold no platen or lateral-record sphere: a full warp with
+    // nothing to add skips the reduction.
+    {
+      const unsigned am = __activemask();
+      if (am == 0xFFFFFFFFu && !__any_sync(am, sb != 0.0 || st != 0.0 || sl != 0.0)) continue;
+    }
     if (A.det) {
       long long qb = to_fix(sb), qt = to_fix(st), ql = to_fix(sl);
       const unsigned fm = __activemask();
@@ -1047,28 +1084,19 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
     atomicMax(reinterpret_cast<int*>(A.stat), __float_as_int(a));
     atomicMax(reinterpret_cast<int*>(A.stat) + 1, __float_as_int(b));
   }
-  // the last block to finish runs the controllers
-  __threadfence();
+  // the last block to finish runs the controllers.  The barrier orders the
+  // block's flag stores and sum atomics before thread 0's fence and count
+  // (one fence per block, as a grid barrier does; a fence in every thread
+  // would also wait for the particle-state stores, which no controller reads)
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = (atomicAdd(A.blocks_done, 1u) == gridDim.x - 1);
+  }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
-    if (A.ctl[s].done) continue;
-    // the controller works on a private copy (one load of the state, one store
-    // back) instead of a chain of dependent global reads and writes
-    SampleCtl C = A.ctl[s];
-    // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
-    C.sFL[0] += (double)C.sFLq[0] * kFixInv;
-    C.sFL[1] += (double)C.sFLq[1] * kFixInv;
-    C.lat_sum += (double)C.lat_q * kFixInv;
-    C.sFLq[0] = C.sFLq[1] = C.lat_q = 0;
-    tangent_step_end(A, C, s);
-    controller_step(C);
-    A.ctl[s] = C;
-  }
-  if (threadIdx.x == 0) *A.blocks_done = 0;
+  run_controllers<Real>(A);
 }
 
 }  // namespace dem

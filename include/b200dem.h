@@ -232,8 +232,11 @@ int dem_set_pairs(dem_ctx* ctx, int32_t sample, uint32_t n, const uint32_t* i, c
 int dem_set_platens(dem_ctx* ctx, int32_t sample, double top, double bottom, double velocity);
 /* Rebuilds the contact list now (normally automatic). */
 int dem_rebuild_contacts(dem_ctx* ctx);
-/* Advances nsteps steps from the captured step graph; *ms = device time of
- * the whole run (CUDA events on the context's stream, rebuilds included). */
+/* Advances nsteps steps from the captured step graphs; *ms = device time of
+ * the steps (CUDA events on the context's stream, from the first step's
+ * launch to the end of the last step: rebuilds and host checks between
+ * chunks of steps included, the state read-back at either end of the call
+ * not). */
 int dem_run_timed(dem_ctx* ctx, uint64_t nsteps, double* ms);
 /* Advances nsteps steps as one captured graph with a CUDA event record node
  * before, between and after the two step kernels of every step (the way the

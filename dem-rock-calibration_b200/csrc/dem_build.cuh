@@ -246,10 +246,17 @@ constexpr uint32_t kSearchWarps = 4;   // warps (spheres in flight) per 128-thre
 
 inline uint32_t pair_search_blocks(uint32_t np) { return np ? (np + kSearchWarps - 1) / kSearchWarps : 1u; }
 
-template <class Real, bool kFill>
+// kPass 0 counts, 1 fills the CSR lists at offset[i], 2 does both at once:
+// count[i] and up to kSearchStride partners, sorted, at out_j + i *
+// kSearchStride (the caller then compacts them with k_expand_stride).
+constexpr uint32_t kSearchStride = 48;
+
+template <class Real, int kPass>
 __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
+  constexpr bool kCount = kPass != 1, kFill = kPass != 0;
   using V4 = typename RT<Real>::V4;
   constexpr uint32_t kMax = 48;
+  static_assert(kMax <= kSearchStride, "one-pass slots hold every kept partner");
   constexpr unsigned kFull = 0xFFFFFFFFu;
   __shared__ uint32_t s_buf[kSearchWarps][kMax];
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -259,7 +266,7 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
     const uint32_t s = S.sid[i];
     const Grid<Real> g = S.grids[s];
     if (at_hidden(g, xi) || (S.done && S.done[s])) {
-      if (!kFill && lane == 0) S.count[i] = 0;
+      if (kCount && lane == 0) S.count[i] = 0;
       continue;
     }
     const int ix = (int)cell_coord<Real>(xi.x, g.ox, g.inv_a, g.nx);
@@ -314,14 +321,14 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
       n += __popc(mask);
     }
     __syncwarp();
-    if (!kFill) {
-      if (lane == 0) {
-        S.count[i] = n;
-        if (n > S.cap && S.overflow) atomicAdd(S.overflow, 1u);
-      }
-    } else {
+    if (kCount && lane == 0) {
+      S.count[i] = n;
+      if (n > S.cap && S.overflow) atomicAdd(S.overflow, 1u);
+    }
+    if (kFill) {
       const uint32_t m = n < lim ? n : lim;
-      uint32_t* o = S.mode == kModeRefSet ? S.out_j + (size_t)i * S.cap : S.out_j + S.offset[i];
+      uint32_t* o = kPass == 2 ? S.out_j + (size_t)i * kSearchStride
+                               : (S.mode == kModeRefSet ? S.out_j + (size_t)i * S.cap : S.out_j + S.offset[i]);
       for (uint32_t e = lane; e < m; e += 32) {
         const uint32_t val = buf[e];
         uint32_t r = 0;
@@ -332,6 +339,17 @@ __global__ void __launch_bounds__(128) k_pair_search(PairSearch<Real> S) {
         for (uint32_t a = m + lane; a < S.cap; a += 32) o[a] = kEmpty;
     }
     __syncwarp();   // the buffer is refilled for the next sphere
+  }
+}
+
+// The one-pass lists (kPass 2, kSearchStride slots a particle) compacted into
+// (i, j) pairs at the scanned offsets.
+static __global__ void k_expand_stride(const uint32_t* __restrict__ offset, uint32_t np,
+                                       const uint32_t* __restrict__ js, uint2* __restrict__ ij) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const uint32_t k0 = offset[i], n = offset[i + 1] - k0;
+    const uint32_t m = n < kSearchStride ? n : kSearchStride;
+    for (uint32_t r = 0; r < m; ++r) ij[k0 + r] = make_uint2(i, js[(size_t)i * kSearchStride + r]);
   }
 }
 

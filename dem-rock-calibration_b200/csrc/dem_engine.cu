@@ -951,7 +951,19 @@ class Engine final : public EngineBase {
     S.b_row = b_row_.p;
     S.b_ij = b_ij_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
-    k_pair_search<Real, false><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
+    // rebuilds during a run: one search pass (the counts and every particle's
+    // partners, sorted, in kSearchStride slots of its own, compacted below once
+    // the counts are scanned).  The first build (at set-up) counts, then fills
+    // the exact-size list in a second pass: it does not allocate the slots
+    // (np x kSearchStride indices) a short run would never use.
+    const bool one_pass = !first;
+    if (one_pass) {
+      if (c_jstride_.n < (size_t)np_ * kSearchStride) CK(c_jstride_.alloc((size_t)np_ * kSearchStride));
+      S.out_j = c_jstride_.p;
+      k_pair_search<Real, 2><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
+    } else {
+      k_pair_search<Real, 0><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
+    }
     RC(scan(cnt_.p, offs_.p, np_));
     uint32_t nc = 0, ovf = 0;
     CK(cudaMemcpyAsync(&nc, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
@@ -979,7 +991,6 @@ class Engine final : public EngineBase {
       CK(c_o_.alloc(cap));
       CK(c_ij_new_.alloc(cap));
       CK(c_o_new_.alloc(cap));
-      CK(c_js_.alloc(cap));
       CK(c_row_.alloc(np_ + 1));
       CK(nc_dev_.alloc(1));
       invalidate_graph();
@@ -990,9 +1001,16 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(stream_));
       }
     }
-    S.out_j = c_js_.p;
-    k_pair_search<Real, true><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
-    k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_js_.p, c_ij_new_.p);
+    if (one_pass) {
+      k_expand_stride<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_jstride_.p, c_ij_new_.p);
+    } else {
+      DBuf<uint32_t> js;
+      CK(js.alloc(std::max<size_t>(nc, 1)));
+      S.out_j = js.p;
+      k_pair_search<Real, 1><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
+      k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, js.p, c_ij_new_.p);
+      CK(cudaStreamSynchronize(stream_));   // js is released at the end of this block
+    }
     if (nc) {
       if (first)
         CK(cudaMemsetAsync(c_row_.p, 0, (np_ + 1) * sizeof(uint32_t), stream_));
@@ -2074,7 +2092,7 @@ class Engine final : public EngineBase {
   DBuf<uint32_t> b_row_;
   DBuf<uint2> c_ij_, c_ij_new_;
   DBuf<V4> c_o_, c_o_new_;
-  DBuf<uint32_t> c_js_, c_row_, nc_dev_;
+  DBuf<uint32_t> c_jstride_, c_row_, nc_dev_;
   DBuf<SampleParams<Real>> sp_;
   DBuf<BondLaw<Real>> law_;
   DBuf<double> gap_, skin_;

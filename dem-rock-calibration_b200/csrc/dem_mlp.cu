@@ -524,17 +524,10 @@ __global__ void __launch_bounds__(PersistCfg<TN>::kThreads, 1)
       tc_fence_after();
       const int row = t * kTM + q4 * 32 + lane;
       const uint32_t acc = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)a * kAcc;
-      // a warp's chunks cg and cg + 4 (TN = 256) are loaded together before
-      // one wait, so that their 64 values give the arithmetic independent work
-      for (int col0 = 32 * cg; col0 < TN; col0 += 256) {
-        uint32_t ra[32], rb[32];
-        const bool two = col0 + 128 < TN;
-        tmem_ld32(acc + (uint32_t)col0, ra);
-        if (two) tmem_ld32(acc + (uint32_t)(col0 + 128), rb);
-        tmem_wait_ld();
-        chunk_out<true>(ra, row, col0, M, N, sbias, mode, act, outf, outh);
-        if (two) chunk_out<true>(rb, row, col0 + 128, M, N, sbias, mode, act, outf, outh);
-      }
+      // (loading a warp's two chunks before one wait was measured slower:
+      // 23.4 against 21.4 us on the 65,536 x 256 x 256 layer)
+      for (int col0 = 32 * cg; col0 < TN; col0 += 128)
+        drain_chunk<true>(acc + (uint32_t)col0, row, col0, M, N, sbias, mode, act, outf, outh);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) bar_arrive(&tempty[a]);

@@ -304,7 +304,11 @@ class Packer {
     S.cap = 48;
     S.overflow = ovf.p;
     CKP(cudaMemsetAsync(ovf.p, 0, sizeof(uint32_t), st));
-    k_pair_search<float, false><<<pair_search_blocks(n), 128, 0, st>>>(S);
+    // one search pass (counts and sorted partners in kSearchStride slots per
+    // sphere), compacted once the counts are scanned
+    if (js.n < (size_t)n * kSearchStride) CKP(js.alloc((size_t)n * kSearchStride));
+    S.out_j = js.p;
+    k_pair_search<float, 2><<<pair_search_blocks(n), 128, 0, st>>>(S);
     rc = scan(cnt.p, offs.p, n);
     if (rc) return rc;
     uint32_t nc = 0, o = 0;
@@ -312,13 +316,8 @@ class Packer {
     CKP(cudaMemcpyAsync(&o, ovf.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CKP(cudaStreamSynchronize(st));
     if (o) return DEM_ERR_CAPACITY;
-    if (nc + 1 > cij.n) {
-      CKP(cij.alloc(nc + nc / 2 + 1024));
-      CKP(js.alloc(nc + nc / 2 + 1024));
-    }
-    S.out_j = js.p;
-    k_pair_search<float, true><<<pair_search_blocks(n), 128, 0, st>>>(S);
-    k_expand_pairs<<<g1, 256, 0, st>>>(offs.p, n, js.p, cij.p);
+    if (nc + 1 > cij.n) CKP(cij.alloc(nc + nc / 2 + 1024));
+    k_expand_stride<<<g1, 256, 0, st>>>(offs.p, n, js.p, cij.p);
     CKP(cudaMemcpyAsync(nc_dev.p, &nc, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     k_copy_pos<float><<<g1, 256, 0, st>>>(pos.p, ref.p, n);
     CKP(cudaGetLastError());

@@ -1067,6 +1067,7 @@ class Engine final : public EngineBase {
       C.V = 0;
       C.dt = s.dt;
       C.max_steps = L.max_steps ? L.max_steps : ~0ull;
+      C.stop_at = ~0ull;
       C.bonds = s.bonds_initial;
       C.dNsave = L.dNsave;
       uint64_t nsave = 16;
@@ -1392,6 +1393,8 @@ class Engine final : public EngineBase {
   struct Flags {
     uint32_t done, rebuild, stale, numeric;
     float v2max, d2max;
+    uint32_t active;       // samples neither done nor at their stop
+    uint64_t remaining;    // largest number of steps an active sample still has to go
   };
 
   int read_flags(Flags& f) {
@@ -1401,24 +1404,37 @@ class Engine final : public EngineBase {
     CK(cudaMemcpyAsync(hctl_.data(), ctl_.p, S * sizeof(SampleCtl), cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(st, stat_.p, 2 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
-    f = {1, 0, 0, 0, st[0], st[1]};
+    f = {1, 0, 0, 0, st[0], st[1], 0, 0};
     for (auto& c : hctl_) {
       f.done &= c.done ? 1u : 0u;
       f.rebuild |= c.rebuild;
       f.stale |= c.stale;
       f.numeric |= c.numeric;
+      if (!c.done && c.step < c.stop_at) {
+        ++f.active;
+        f.remaining = std::max<uint64_t>(f.remaining, c.stop_at - c.step);
+      }
     }
+    return DEM_OK;
+  }
+
+  // Every sample stops at its current step + n (n = ~0: runs on until done);
+  // the hold flags follow.
+  int set_stop(uint64_t n) {
+    const uint32_t S = (uint32_t)samples_.size();
+    k_set_hold<<<ceil_div(S, 128), 128, 0, stream_>>>(ctl_.p, S, n, 0);
+    CK(cudaGetLastError());
     return DEM_OK;
   }
 
   // after a rebuild: clear the per-sample rebuild/stale flags and the
   // displacement maximum (positions are the new reference)
   int clear_rebuild_flags() {
-    for (uint32_t si = 0; si < hctl_.size(); ++si) {
-      const uint32_t z[2] = {0, 0};
-      static_assert(offsetof(SampleCtl, stale) == offsetof(SampleCtl, rebuild) + sizeof(uint32_t), "layout");
-      CK(cudaMemcpyAsync(&ctl_.p[si].rebuild, z, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
-    }
+    // rebuild and stale flags cleared, hold flags refreshed (a sample held on a
+    // stale list runs again), in one launch
+    const uint32_t S = (uint32_t)samples_.size();
+    k_set_hold<<<ceil_div(S, 128), 128, 0, stream_>>>(ctl_.p, S, 0ull, 1);
+    CK(cudaGetLastError());
     CK(cudaMemsetAsync(stat_.p + 1, 0, sizeof(float), stream_));
     CK(cudaStreamSynchronize(stream_));
     return DEM_OK;
@@ -1455,7 +1471,7 @@ class Engine final : public EngineBase {
     return DEM_OK;
   }
 
-  // Runs until max_steps steps or (stop_when_done) until every sample is done.
+  // Runs until every sample has advanced max_steps steps or is done.
   // A sample whose state turned non-finite is stopped by the controller; the
   // others run on, and the call then returns DEM_ERR_NUMERIC.
   // ev (optional, two events): ev[0] is recorded once the state of the last
@@ -1463,11 +1479,20 @@ class Engine final : public EngineBase {
   // after the launches of each chunk, so that [ev[0], ev[1]] spans the device
   // work of these steps and the host work between their chunks, and not the
   // bookkeeping at either end of the call.
+  // Every sample advances max_steps steps (fewer if it finishes): the step
+  // kernels hold a sample at its stop while the others catch up, and hold a
+  // sample whose contact list went stale inside a chunk (a particle past half
+  // the skin) until the list is rebuilt, so that no step runs on a list that
+  // may miss a contact; the held steps are run again after the rebuild.
+  // done_steps: the largest number of steps a sample advanced.
   int run(uint64_t max_steps, uint64_t* done_steps, bool stop_when_done, cudaEvent_t* ev = nullptr) {
+    (void)stop_when_done;   // the loop ends once no sample is active either way
     RC(prepare());
-    uint64_t steps = 0;
+    if (max_steps) RC(set_stop(max_steps));
     Flags f{};
     RC(read_flags(f));
+    std::vector<uint64_t> step0(hctl_.size());
+    for (size_t k = 0; k < hctl_.size(); ++k) step0[k] = hctl_[k].step;
     const uint32_t numeric_before = f.numeric;
     RC(update_tiles());
     if (ev) {
@@ -1486,9 +1511,8 @@ class Engine final : public EngineBase {
         RC(clear_rebuild_flags());
         f.d2max = 0.f;
       }
-      if (steps >= max_steps || (stop_when_done && f.done)) break;
-      const uint64_t left = max_steps - steps;
-      const uint64_t chunk = std::min(left, chunk_steps(f));
+      if (!max_steps || !f.active) break;
+      const uint64_t chunk = std::min(f.remaining, chunk_steps(f));
       CK(cudaMemsetAsync(stat_.p, 0, sizeof(float), stream_));  // speed maximum of this chunk
       if (chunk == opt_.graph_steps) {
         if (!graph_exec_) RC(capture_steps(opt_.graph_steps, &graph_exec_));
@@ -1497,11 +1521,12 @@ class Engine final : public EngineBase {
         RC(run_short_chunk(chunk));
       }
       if (ev) CK(cudaEventRecord(ev[1], stream_));
-      steps += chunk;
       CK(cudaGetLastError());
       RC(read_flags(f));
       RC(update_tiles());
     }
+    uint64_t steps = 0;
+    for (size_t k = 0; k < hctl_.size(); ++k) steps = std::max<uint64_t>(steps, hctl_[k].step - step0[k]);
     total_steps_ += steps;
     if (done_steps) *done_steps = steps;
     return (f.numeric && !numeric_before) ? DEM_ERR_NUMERIC : DEM_OK;
@@ -1512,6 +1537,16 @@ class Engine final : public EngineBase {
 
   int step_stages(int stages) override {
     RC(prepare());
+    // the contact list is rebuilt by the rule of run(): once a particle has
+    // moved a quarter of the skin since the last build (or past half of it)
+    Flags f{};
+    RC(read_flags(f));
+    if (f.rebuild || f.stale || (double)f.d2max > 0.0625 * min_skin_ * min_skin_) {
+      if (f.stale) ++stale_events_;
+      RC(build_contacts(false));
+      RC(clear_rebuild_flags());
+    }
+    RC(set_stop(1));
     StepArgs<Real> A = args();
     A.keep_forces = (stages & 4) ? 1 : 0;
     launch_step(A, stages & 3);
@@ -1961,6 +1996,7 @@ class Engine final : public EngineBase {
 
   // device pointers of the step kernel for external timing
   void launch_raw(int stages) override {
+    if (set_stop(1) != DEM_OK) return;
     StepArgs<Real> A = args();
     launch_step(A, stages);
   }
@@ -1988,70 +2024,92 @@ class Engine final : public EngineBase {
   }
 
   // Per-kernel device time of nsteps steps run the way the timed steps run:
-  // one captured graph of the steps, with an event record node before the
-  // pair kernel, between the two kernels and after the particle kernel of
-  // every step; the graph is replayed once and the event pairs give each
-  // launch's duration.  Also counts the touching contacts (algorithmic-byte
-  // accounting).
+  // captured graphs of the steps, with an event record node before the pair
+  // kernel, between the two kernels and after the particle kernel of every
+  // step; each graph is replayed once and the event pairs give each launch's
+  // duration.  The steps go in chunks sized and separated by contact-list
+  // rebuilds as in run(); a chunk in which a list went stale (its sample then
+  // holds, skipping work) is run but not counted.  Also counts the touching
+  // contacts (algorithmic-byte accounting).
   int profile(uint32_t nsteps, double* pair_ms, double* particle_ms, double* touching) override {
     RC(prepare());
     if (nsteps == 0) return DEM_ERR_ARG;
-    std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
-    for (auto& e : ev) CK(cudaEventCreate(&e));
     DBuf<unsigned long long> cnt;
     CK(cnt.alloc(1));
-    StepArgs<Real> A = args();
-    A.touching = cnt.p;
     const uint32_t g = particle_grid();
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    // an event recorded during capture becomes an event record node only
-    // with cudaEventRecordExternal (a plain record is a capture-internal
-    // dependency and is never recorded when the graph runs)
-    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    cudaError_t ce = cudaSuccess;
-    for (uint32_t k = 0; k < nsteps && ce == cudaSuccess; ++k) {
-      ce = cudaEventRecordWithFlags(ev[3 * k], stream_, cudaEventRecordExternal);
-      launch_pairs(A);
-      if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 1], stream_, cudaEventRecordExternal);
-      k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
-      if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 2], stream_, cudaEventRecordExternal);
-    }
-    cudaError_t e = cudaStreamEndCapture(stream_, &graph);
-    if (e == cudaSuccess && ce != cudaSuccess) e = ce;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream_);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
-    if (exec) cudaGraphExecDestroy(exec);
-    if (e != cudaSuccess) {
-      for (auto& x : ev) cudaEventDestroy(x);
-      last_cuda_ = e;
-      note_cuda_error(e, __FILE__, __LINE__);
-      return DEM_ERR_CUDA;
-    }
-    double sp = 0, sq = 0;
-    for (uint32_t k = 0; k < nsteps; ++k) {
-      float t1 = 0, t2 = 0;
-      CK(cudaEventElapsedTime(&t1, ev[3 * k], ev[3 * k + 1]));
-      CK(cudaEventElapsedTime(&t2, ev[3 * k + 1], ev[3 * k + 2]));
-      sp += t1;
-      sq += t2;
-    }
-    for (auto& x : ev) cudaEventDestroy(x);
-    unsigned long long tc = 0;
-    CK(cnt.download(&tc, 1));
-    if (pair_ms) *pair_ms = sp / nsteps;
-    if (particle_ms) *particle_ms = sq / nsteps;
-    if (touching) *touching = (double)tc / nsteps;
+    double sp = 0, sq = 0, tc_sum = 0;
+    uint32_t counted = 0, attempts = 0;
     Flags f{};
     RC(read_flags(f));
-    if (f.stale) ++stale_events_;
+    while (counted < nsteps && attempts < 4 * nsteps) {
+      if (f.rebuild || f.stale || (double)f.d2max > 0.0625 * min_skin_ * min_skin_) {
+        if (f.stale) ++stale_events_;
+        RC(build_contacts(false));
+        RC(clear_rebuild_flags());
+        f.d2max = 0.f;
+      }
+      const uint32_t chunk = (uint32_t)std::min<uint64_t>(nsteps - counted, chunk_steps(f));
+      RC(set_stop(chunk));
+      CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), stream_));
+      CK(cudaMemsetAsync(stat_.p, 0, sizeof(float), stream_));
+      StepArgs<Real> A = args();
+      A.touching = cnt.p;
+      std::vector<cudaEvent_t> ev(3 * (size_t)chunk);
+      for (auto& e : ev) CK(cudaEventCreate(&e));
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      // an event recorded during capture becomes an event record node only
+      // with cudaEventRecordExternal (a plain record is a capture-internal
+      // dependency and is never recorded when the graph runs)
+      CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      cudaError_t ce = cudaSuccess;
+      for (uint32_t k = 0; k < chunk && ce == cudaSuccess; ++k) {
+        ce = cudaEventRecordWithFlags(ev[3 * k], stream_, cudaEventRecordExternal);
+        launch_pairs(A);
+        if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 1], stream_, cudaEventRecordExternal);
+        k_particles<Real><<<g, opt_.particle_block, 0, stream_>>>(A);
+        if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(ev[3 * k + 2], stream_, cudaEventRecordExternal);
+      }
+      cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+      if (e == cudaSuccess && ce != cudaSuccess) e = ce;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream_);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+      if (exec) cudaGraphExecDestroy(exec);
+      if (e != cudaSuccess) {
+        for (auto& x : ev) cudaEventDestroy(x);
+        last_cuda_ = e;
+        note_cuda_error(e, __FILE__, __LINE__);
+        return DEM_ERR_CUDA;
+      }
+      attempts += chunk;
+      total_steps_ += chunk;
+      RC(read_flags(f));
+      if (!f.stale) {
+        for (uint32_t k = 0; k < chunk; ++k) {
+          float t1 = 0, t2 = 0;
+          CK(cudaEventElapsedTime(&t1, ev[3 * k], ev[3 * k + 1]));
+          CK(cudaEventElapsedTime(&t2, ev[3 * k + 1], ev[3 * k + 2]));
+          sp += t1;
+          sq += t2;
+        }
+        unsigned long long tc = 0;
+        CK(cnt.download(&tc, 1));
+        tc_sum += (double)tc;
+        counted += chunk;
+      }
+      for (auto& x : ev) cudaEventDestroy(x);
+    }
     if (f.rebuild || f.stale) {
+      if (f.stale) ++stale_events_;
       RC(build_contacts(false));
       RC(clear_rebuild_flags());
     }
-    total_steps_ += nsteps;
+    if (!counted) return DEM_ERR_STATE;
+    if (pair_ms) *pair_ms = sp / counted;
+    if (particle_ms) *particle_ms = sq / counted;
+    if (touching) *touching = tc_sum / counted;
     return DEM_OK;
   }
 

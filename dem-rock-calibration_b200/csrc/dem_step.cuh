@@ -150,7 +150,10 @@ __device__ __forceinline__ void hm_pair(const SampleParams<Real>& sp, Real rx, R
   const Real v2 = vj.z - vi.z + rbar * (n0 * sw1 - n1 * sw0) + rdif * (n0 * dw1 - n1 * dw0);
   const Real vn = n0 * v0 + n1 * v1 + n2 * v2;
   const Real fijnm = (rijm - sumr) * Kn * T::kTwoThirds;
-  const Real m2 = mi * ((mj + mj) / (mi + mj));
+  // 2 m* = m_a (2 m_b / (m_a + m_b)) with m_a the smaller mass: the same bits
+  // from either side of the pair, and m_i when the masses are equal
+  const Real ma = mi < mj ? mi : mj, mb = mi < mj ? mj : mi;
+  const Real m2 = ma * ((mb + mb) / (ma + mb));
   cef1 = T::kDamp * sp.pA * vn * T::sqrt_rn(Kn * half * m2);
   const Real fn0 = n0 * (fijnm + cef1), fn1 = n1 * (fijnm + cef1), fn2 = n2 * (fijnm + cef1);
   const Real vt0 = v0 - n0 * vn, vt1 = v1 - n1 * vn, vt2 = v2 - n2 * vn;
@@ -428,7 +431,7 @@ __device__ __forceinline__ void do_bond_core(const StepArgs<Real>& A, uint32_t b
   using T = RT<Real>;
   const uint32_t i = ij.x, j = ij.y;
   const uint32_t s = ts != ~0u ? ts : A.sid[i];
-  if (A.ctl[s].done) return;
+  if (A.ctl[s].hold) return;
   const SampleParams<Real>& sp = A.sp[s];
   const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
   const Real rr = (rx * rx + ry * ry) + rz * rz;
@@ -573,7 +576,7 @@ __device__ __forceinline__ void do_contact(const StepArgs<Real>& A, uint32_t c) 
   const uint32_t i = ij.x, j = ij.y & 0x7FFFFFFFu;
   const bool has_hist = (ij.y >> 31) != 0;
   const uint32_t s = A.sid[i];
-  if (A.ctl[s].done) return;
+  if (A.ctl[s].hold) return;
   const V4 pi = ld4(A.pos + i), pj = ld4(A.pos + j);
   const Real rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
   const Real rr = (rx * rx + ry * ry) + rz * rz;
@@ -788,6 +791,22 @@ __device__ inline void controller_step(SampleCtl& C) {
   // loop condition of h_Calculation{UniaxialCompression,BrazilTest}; a sample
   // whose state went non-finite also stops
   if (!(fabs(C.Strain) < C.MaxStrain) || C.Fracture || C.step >= C.max_steps || C.numeric) C.done = 1;
+  C.hold = (C.done || C.stale || C.step >= C.stop_at) ? 1u : 0u;
+}
+
+// After the host has cleared the rebuild flags or moved the stop: the hold
+// flag of every sample again (stop_steps: new stop_at = step + stop_steps,
+// saturating; 0 keeps stop_at).
+__global__ void k_set_hold(SampleCtl* ctl, uint32_t S, unsigned long long stop_steps, int clear_rebuild) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    SampleCtl& C = ctl[s];
+    if (clear_rebuild) {
+      C.rebuild = 0;
+      C.stale = 0;
+    }
+    if (stop_steps) C.stop_at = C.step + stop_steps < C.step ? ~0ull : C.step + stop_steps;
+    C.hold = (C.done || C.stale || C.step >= C.stop_at) ? 1u : 0u;
+  }
 }
 
 // The controllers of all samples, run by the last block of the particle
@@ -798,7 +817,7 @@ __device__ inline void controller_step(SampleCtl& C) {
 template <class Real>
 __device__ __noinline__ void run_controllers(const StepArgs<Real> A) {
   for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
-    if (A.ctl[s].done) continue;
+    if (A.ctl[s].hold) continue;
     SampleCtl C = A.ctl[s];
     // fixed-point platen and lateral sums of the deterministic mode (zero otherwise)
     C.sFL[0] += (double)C.sFLq[0] * kFixInv;
@@ -826,7 +845,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
   constexpr bool kCacheable = sizeof(Real) <= 8;
   __shared__ SampleParams<Real> c_sp[kCacheable ? kCacheSamples : 1];
   __shared__ float c_wall[kCacheable ? kCacheSamples : 1][3];   // platen top, bottom, velocity (as float)
-  __shared__ uint32_t c_flag[kCacheable ? kCacheSamples : 1];   // bit 0: done; bit 1: a lateral-record step
+  __shared__ uint32_t c_flag[kCacheable ? kCacheSamples : 1];   // bit 0: held (done, stale, at its stop); bit 1: a lateral-record step
   const bool cached = kCacheable && A.nsamples <= kCacheSamples;
   if (cached) {
     for (uint32_t s = threadIdx.x; s < A.nsamples; s += blockDim.x) {
@@ -835,7 +854,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
       c_wall[s][0] = (float)C.Top;
       c_wall[s][1] = (float)C.Bottom;
       c_wall[s][2] = (float)C.V;
-      c_flag[s] = (C.done ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u);
+      c_flag[s] = (C.hold ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u);
     }
     __syncthreads();
   }
@@ -860,7 +879,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 1) k_particles(St
     const uint32_t s = A.sid[p];
     SampleCtl& C = A.ctl[s];
     double sb = 0.0, st = 0.0, sl = 0.0;
-    const uint32_t flag = cached ? c_flag[s] : ((C.done ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u));
+    const uint32_t flag = cached ? c_flag[s] : ((C.hold ? 1u : 0u) | ((C.dNsave && C.step % C.dNsave == 0) ? 2u : 0u));
     if (!(flag & 1u)) {
       const SampleParams<Real>& sp = cached ? c_sp[s] : A.sp[s];
       if constexpr (sizeof(Real) == 4) {

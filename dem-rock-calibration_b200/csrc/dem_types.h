@@ -72,6 +72,15 @@ struct SampleCtl {
   long long sFLq[2];
   long long lat_q;
   long long q_pad;
+  // The step kernels skip a sample while `hold` is set: finished (done), its
+  // contact list no longer valid (stale: a particle moved past half the skin,
+  // so the next step would miss contacts until the host rebuilds the list),
+  // or at the step the current host call asked for (stop_at).  The controller
+  // sets it at the end of each step; the host refreshes it when it clears
+  // stale or sets stop_at.
+  unsigned long long stop_at;
+  uint32_t hold;
+  uint32_t hold_pad;
 };
 
 }  // namespace dem

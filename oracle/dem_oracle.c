@@ -106,6 +106,11 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #define RSQRT_RN orc_rsqrt_rn_f
 #define NORM3_RN orc_norm3_f
 #define ULP(x) (nextafterf(fabsf(x), INFINITY) - fabsf(x))
+/* fixed-point sums of the engine's deterministic FP32 mode: multiples of 2^-40,
+ * the product x * 2^40 exact in float, rounded to the nearest integer (ties to
+ * even), converted back through double */
+#define FIXQ(x) llrintf((x) * 0x1p40f)
+#define UNFIXQ(q) ((float)((double)(q) * 0x1p-40))
 #include "dem_oracle_impl.h"
 #undef REAL
 #undef SFX
@@ -126,6 +131,8 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #undef RSQRT_RN
 #undef NORM3_RN
 #undef ULP
+#undef FIXQ
+#undef UNFIXQ
 
 /* ---- double instantiation (FP64 build extension) ---- */
 #define REAL double
@@ -147,6 +154,9 @@ static inline double orc_norm3_d(double x, double y, double z) { return sqrt((x 
 #define RSQRT_RN orc_rsqrt_rn_d
 #define NORM3_RN orc_norm3_d
 #define ULP(x) (nextafter(fabs(x), INFINITY) - fabs(x))
+/* FP64 deterministic mode: multiples of 2^-50 */
+#define FIXQ(x) llrint((x) * 0x1p50)
+#define UNFIXQ(q) ((double)(q) * 0x1p-50)
 #include "dem_oracle_impl.h"
 
 /* md_results.cu:207-272 with the host sum of :189-205 */

@@ -92,6 +92,27 @@ int orc_get_threads(void);
                         REAL mP, REAL rP, const REAL* rad, const REAL* mass, const REAL* center,   \
                         REAL wall_RR, REAL wall_top, REAL wall_bot, REAL wall_V, REAL Zcut,        \
                         REAL* FL, double* sFL);                                                    \
+  /* Order-independent sums (the engine's deterministic mode): the same per-slot values as      \
+   * orc_forces_bpm / orc_forces_hm, each slot's force and moment rounded to fixed point (2^-40   \
+   * in float, 2^-50 in double) and added into 64-bit accumulators Fq, Mq (3N each, SoA, added   \
+   * to, not cleared); orc_fix_to_real converts them back.  orc_platen_q sums the platen forces  \
+   * of the spheres in fixed point (2^-40) into sFL. */                                            \
+  void orc_forces_bpm_q_##SFX(const REAL* R, const REAL* V, const REAL* W, uint32_t N,               \
+                              const uint32_t* IL, uint32_t* ILtype, const REAL* inv_L0, REAL* Rij,  \
+                              REAL* Oijt, REAL* Mijn, REAL* Mijt, uint32_t IonP, REAL dt, REAL E,   \
+                              REAL G, REAL b_r, REAL Ec, REAL Gc, const REAL* slot_br,              \
+                              const REAL* slot_sn, const REAL* slot_st, int nobreak, int64_t* Fq,   \
+                              int64_t* Mq);                                                         \
+  void orc_forces_hm_q_##SFX(const REAL* R, const REAL* V, const REAL* W, uint32_t N,                \
+                             const uint32_t* IL, const uint32_t* ILtype, REAL* Oijt, uint32_t IonP, \
+                             REAL dt, REAL hmE, REAL hmG, REAL pA, REAL mu, REAL mur, REAL mP,      \
+                             REAL rP, const REAL* rad, const REAL* mass, int64_t* Fq, int64_t* Mq); \
+  void orc_fix_to_real_##SFX(const int64_t* q, REAL* out, uint64_t n);                              \
+  void orc_platen_q_##SFX(int axis, const REAL* R, const REAL* V, const REAL* W, REAL* Oiwt,          \
+                          REAL* F, REAL* M, uint32_t N, REAL dt, REAL wE, REAL wG, REAL pA, REAL mu, \
+                          REAL mur, REAL mP, REAL rP, const REAL* rad, const REAL* mass,           \
+                          const REAL* center, REAL wall_RR, REAL wall_top, REAL wall_bot,          \
+                          REAL wall_V, REAL Zcut, double* sFL);                                    \
   /* md_calculateincrementsdem.cu:128-158 ; dtm_i/dtI_i per particle (NULL = scalars) */          \
   void orc_increments_##SFX(const REAL* F, REAL* V, REAL* R, const REAL* M, REAL* W, uint32_t N,     \
                             REAL dtm, REAL dt, REAL dtI, const REAL* dtm_i, const REAL* dtI_i);    \

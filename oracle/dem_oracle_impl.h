@@ -221,15 +221,23 @@ void FN(orc_construct_bonds)(const REAL* R, uint32_t N, const uint32_t* IL, uint
   }
 }
 
-void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
-                        uint32_t* ILtype, const REAL* inv_L0, REAL* Rij, REAL* Oijt, REAL* Mijn,
-                        REAL* Mijt, REAL* F, REAL* M, uint32_t IonP, REAL dt, REAL E, REAL G,
-                        REAL b_r0, REAL Ec0, REAL Gc0, const REAL* slot_br, const REAL* slot_sn,
-                        const REAL* slot_st, REAL* Fabs, REAL* Mabs, REAL* Fsens, int nobreak) {
+/* Fq/Mq non-null: order-independent sums.  Each slot's force (normal plus
+ * shear) and moment ((twisting plus bending) plus the unsymmetric shear
+ * moment) is rounded to fixed point (FIXQ) and added to the particle's 64-bit
+ * accumulators, instead of the reference's running float sum over the slots.
+ * These are the per-pair values and the exact sums of the engine's
+ * deterministic mode; every per-slot quantity is the reference's. */
+static void FN(forces_bpm_body)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                                uint32_t* ILtype, const REAL* inv_L0, REAL* Rij, REAL* Oijt, REAL* Mijn,
+                                REAL* Mijt, REAL* F, REAL* M, uint32_t IonP, REAL dt, REAL E, REAL G,
+                                REAL b_r0, REAL Ec0, REAL Gc0, const REAL* slot_br, const REAL* slot_sn,
+                                const REAL* slot_st, REAL* Fabs, REAL* Mabs, REAL* Fsens, int nobreak,
+                                int64_t* Fq, int64_t* Mq) {
 #pragma omp parallel for schedule(static)
   for (int64_t ii = 0; ii < (int64_t)N; ++ii) {
     uint32_t idx = (uint32_t)ii;
     REAL fs[3] = {0, 0, 0}, ms[3] = {0, 0, 0};
+    int64_t fq[3] = {0, 0, 0}, mq[3] = {0, 0, 0};
     REAL fa[3] = {0, 0, 0}, ma[3] = {0, 0, 0};
     double fsens = 0;
     const REAL Wi[3] = {W[idx], W[idx + N], W[idx + 2 * N]};
@@ -329,6 +337,11 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
       mu[1] = HALF * FMA(rz, ot[0], -(rx * ot[2])) * cef;
       mu[2] = HALF * FMA(rx, ot[1], -(ry * ot[0])) * cef;
       for (int d = 0; d < 3; ++d) ms[d] += mu[d];
+      if (Fq)
+        for (int d = 0; d < 3; ++d) {
+          fq[d] += FIXQ(fn[d] + ft[d]);
+          mq[d] += FIXQ((tn[d] + tt[d]) + mu[d]);
+        }
       if (Fabs)
         for (int d = 0; d < 3; ++d) fa[d] += FABS(fn[d]) + FABS(ft[d]);
       if (Mabs)
@@ -352,12 +365,19 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
         }
       }
     }
-    F[idx] += fs[0];
-    F[idx + N] += fs[1];
-    F[idx + 2 * N] += fs[2];
-    M[idx] += ms[0];
-    M[idx + N] += ms[1];
-    M[idx + 2 * N] += ms[2];
+    if (Fq) {
+      for (int d = 0; d < 3; ++d) {
+        Fq[idx + (size_t)d * N] += fq[d];
+        Mq[idx + (size_t)d * N] += mq[d];
+      }
+    } else {
+      F[idx] += fs[0];
+      F[idx + N] += fs[1];
+      F[idx + 2 * N] += fs[2];
+      M[idx] += ms[0];
+      M[idx + N] += ms[1];
+      M[idx + 2 * N] += ms[2];
+    }
     if (Fabs) {
       Fabs[idx] += fa[0];
       Fabs[idx + N] += fa[1];
@@ -372,14 +392,18 @@ void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N,
   }
 }
 
-void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
-                       const uint32_t* ILtype, REAL* Oijt, REAL* F, REAL* M, uint32_t IonP, REAL dt,
-                       REAL hmE, REAL hmG, REAL pA, REAL mu, REAL mur, REAL mP, REAL rP,
-                       const REAL* rad, const REAL* mass, REAL* Fabs, REAL* Mabs, REAL* Fsens) {
+/* Fq/Mq non-null: as forces_bpm_body, per contact the force (normal plus
+ * tangential) and the moment (tangential plus rolling) in fixed point. */
+static void FN(forces_hm_body)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                               const uint32_t* ILtype, REAL* Oijt, REAL* F, REAL* M, uint32_t IonP, REAL dt,
+                               REAL hmE, REAL hmG, REAL pA, REAL mu, REAL mur, REAL mP, REAL rP,
+                               const REAL* rad, const REAL* mass, REAL* Fabs, REAL* Mabs, REAL* Fsens,
+                               int64_t* Fq, int64_t* Mq) {
 #pragma omp parallel for schedule(static)
   for (int64_t ii = 0; ii < (int64_t)N; ++ii) {
     uint32_t idx = (uint32_t)ii;
     REAL fs[3] = {0, 0, 0}, ms[3] = {0, 0, 0};
+    int64_t fq[3] = {0, 0, 0}, mq[3] = {0, 0, 0};
     REAL fa[3] = {0, 0, 0}, ma[3] = {0, 0, 0};
     double fsens = 0;
     int any_touch = 0;
@@ -423,7 +447,8 @@ void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, 
       } else {
         /* polydisperse generalisation: R* = r_i r_j/(r_i+r_j), overlap r_i+r_j-r,
          * contact velocity Vj-Vi + r_i n x Wi + r_j n x Wj, m* = m_i m_j/(m_i+m_j)
-         * carried as 2 m* = m_i * (2 m_j/(m_i+m_j)) so equal masses give m_i. */
+         * carried as 2 m* = m_a * (2 m_b/(m_a+m_b)), m_a the smaller mass, so
+         * equal masses give m_i and both slots of the pair the same value. */
         REAL reff = ri * rj / sumr;
         cef1 = SQRT(reff * (sumr - rijm));
         REAL rbar = HALF * sumr, rdif = HALF * (rj - ri);
@@ -433,7 +458,8 @@ void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, 
         vij[1] = Vj[1] - Vi[1] + rbar * (n[2] * sw[0] - n[0] * sw[2]) + rdif * (n[2] * dw[0] - n[0] * dw[2]);
         vij[2] = Vj[2] - Vi[2] + rbar * (n[0] * sw[1] - n[1] * sw[0]) + rdif * (n[0] * dw[1] - n[1] * dw[0]);
         REAL mi = mass[idx], mj = mass[jdx];
-        m2 = mi * ((mj + mj) / (mi + mj));
+        REAL ma = mi < mj ? mi : mj, mb = mi < mj ? mj : mi; /* symmetric in the pair */
+        m2 = ma * ((mb + mb) / (ma + mb));
       }
       Kn = TWO * hmE * cef1;
       Kt = EIGHT * hmG * cef1;
@@ -494,6 +520,11 @@ void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, 
         mr[2] = Wi[2] * cef1;
         for (int d = 0; d < 3; ++d) ms[d] += mr[d];
       }
+      if (Fq)
+        for (int d = 0; d < 3; ++d) {
+          fq[d] += FIXQ(fnv[d] + ft[d]);
+          mq[d] += FIXQ(mt[d] + mr[d]);
+        }
       if (Fabs)
         for (int d = 0; d < 3; ++d) fa[d] += FABS(fnv[d]) + FABS(ft[d]);
       if (Mabs)
@@ -508,13 +539,23 @@ void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, 
       ms[0] = 0;
       ms[1] = 0;
       ms[2] = 0;
+      mq[0] = 0;
+      mq[1] = 0;
+      mq[2] = 0;
     }
-    F[idx] += fs[0];
-    F[idx + N] += fs[1];
-    F[idx + 2 * N] += fs[2];
-    M[idx] += ms[0];
-    M[idx + N] += ms[1];
-    M[idx + 2 * N] += ms[2];
+    if (Fq) {
+      for (int d = 0; d < 3; ++d) {
+        Fq[idx + (size_t)d * N] += fq[d];
+        Mq[idx + (size_t)d * N] += mq[d];
+      }
+    } else {
+      F[idx] += fs[0];
+      F[idx + N] += fs[1];
+      F[idx + 2 * N] += fs[2];
+      M[idx] += ms[0];
+      M[idx + N] += ms[1];
+      M[idx + 2 * N] += ms[2];
+    }
     if (Fabs) {
       Fabs[idx] += fa[0];
       Fabs[idx + N] += fa[1];
@@ -527,6 +568,46 @@ void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, 
     }
     if (Fsens) Fsens[idx] += (REAL)fsens;
   }
+}
+
+void FN(orc_forces_bpm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                        uint32_t* ILtype, const REAL* inv_L0, REAL* Rij, REAL* Oijt, REAL* Mijn,
+                        REAL* Mijt, REAL* F, REAL* M, uint32_t IonP, REAL dt, REAL E, REAL G,
+                        REAL b_r0, REAL Ec0, REAL Gc0, const REAL* slot_br, const REAL* slot_sn,
+                        const REAL* slot_st, REAL* Fabs, REAL* Mabs, REAL* Fsens, int nobreak) {
+  FN(forces_bpm_body)(R, V, W, N, IL, ILtype, inv_L0, Rij, Oijt, Mijn, Mijt, F, M, IonP, dt, E, G, b_r0, Ec0,
+                      Gc0, slot_br, slot_sn, slot_st, Fabs, Mabs, Fsens, nobreak, NULL, NULL);
+}
+
+void FN(orc_forces_bpm_q)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                          uint32_t* ILtype, const REAL* inv_L0, REAL* Rij, REAL* Oijt, REAL* Mijn,
+                          REAL* Mijt, uint32_t IonP, REAL dt, REAL E, REAL G, REAL b_r0, REAL Ec0,
+                          REAL Gc0, const REAL* slot_br, const REAL* slot_sn, const REAL* slot_st,
+                          int nobreak, int64_t* Fq, int64_t* Mq) {
+  FN(forces_bpm_body)(R, V, W, N, IL, ILtype, inv_L0, Rij, Oijt, Mijn, Mijt, NULL, NULL, IonP, dt, E, G, b_r0,
+                      Ec0, Gc0, slot_br, slot_sn, slot_st, NULL, NULL, NULL, nobreak, Fq, Mq);
+}
+
+void FN(orc_forces_hm)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                       const uint32_t* ILtype, REAL* Oijt, REAL* F, REAL* M, uint32_t IonP, REAL dt,
+                       REAL hmE, REAL hmG, REAL pA, REAL mu, REAL mur, REAL mP, REAL rP,
+                       const REAL* rad, const REAL* mass, REAL* Fabs, REAL* Mabs, REAL* Fsens) {
+  FN(forces_hm_body)(R, V, W, N, IL, ILtype, Oijt, F, M, IonP, dt, hmE, hmG, pA, mu, mur, mP, rP, rad, mass,
+                     Fabs, Mabs, Fsens, NULL, NULL);
+}
+
+void FN(orc_forces_hm_q)(const REAL* R, const REAL* V, const REAL* W, uint32_t N, const uint32_t* IL,
+                         const uint32_t* ILtype, REAL* Oijt, uint32_t IonP, REAL dt, REAL hmE, REAL hmG,
+                         REAL pA, REAL mu, REAL mur, REAL mP, REAL rP, const REAL* rad, const REAL* mass,
+                         int64_t* Fq, int64_t* Mq) {
+  FN(forces_hm_body)(R, V, W, N, IL, ILtype, Oijt, NULL, NULL, IonP, dt, hmE, hmG, pA, mu, mur, mP, rP, rad,
+                     mass, NULL, NULL, NULL, Fq, Mq);
+}
+
+/* F = the fixed-point sums converted back (UNFIXQ), one value per element */
+void FN(orc_fix_to_real)(const int64_t* q, REAL* out, uint64_t n) {
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < (int64_t)n; ++k) out[k] = UNFIXQ(q[k]);
 }
 
 /* one particle-platen contact, md_compression_hm.cu:20-154 ; returns the
@@ -609,10 +690,36 @@ static inline REAL FN(wall_contact)(int axis, REAL sgn, const REAL* V, const REA
   return fiwn[axis];
 }
 
+static void FN(platen_body)(int axis, const REAL* R, const REAL* V, const REAL* W, REAL* Oiwt, REAL* F,
+                           REAL* M, uint32_t N, REAL dt, REAL wE, REAL wG, REAL pA, REAL mu, REAL mur,
+                           REAL mP, REAL rP, const REAL* rad, const REAL* mass, const REAL* c,
+                           REAL wall_RR, REAL wall_top, REAL wall_bot, REAL wall_V, REAL Zcut, REAL* FL,
+                           double* sFL, int fixsum);
+
 void FN(orc_platen)(int axis, const REAL* R, const REAL* V, const REAL* W, REAL* Oiwt, REAL* F, REAL* M,
                     uint32_t N, REAL dt, REAL wE, REAL wG, REAL pA, REAL mu, REAL mur, REAL mP, REAL rP,
                     const REAL* rad, const REAL* mass, const REAL* c, REAL wall_RR, REAL wall_top,
                     REAL wall_bot, REAL wall_V, REAL Zcut, REAL* FL, double* sFL) {
+  FN(platen_body)(axis, R, V, W, Oiwt, F, M, N, dt, wE, wG, pA, mu, mur, mP, rP, rad, mass, c, wall_RR, wall_top,
+                  wall_bot, wall_V, Zcut, FL, sFL, 0);
+}
+
+/* The platen step with sFL summed as the engine's deterministic mode does:
+ * every sphere's normal platen force, widened to double, rounded to a
+ * multiple of 2^-40 and added as an integer (exact, order-independent). */
+void FN(orc_platen_q)(int axis, const REAL* R, const REAL* V, const REAL* W, REAL* Oiwt, REAL* F, REAL* M,
+                      uint32_t N, REAL dt, REAL wE, REAL wG, REAL pA, REAL mu, REAL mur, REAL mP, REAL rP,
+                      const REAL* rad, const REAL* mass, const REAL* c, REAL wall_RR, REAL wall_top,
+                      REAL wall_bot, REAL wall_V, REAL Zcut, double* sFL) {
+  FN(platen_body)(axis, R, V, W, Oiwt, F, M, N, dt, wE, wG, pA, mu, mur, mP, rP, rad, mass, c, wall_RR, wall_top,
+                  wall_bot, wall_V, Zcut, NULL, sFL, 1);
+}
+
+static void FN(platen_body)(int axis, const REAL* R, const REAL* V, const REAL* W, REAL* Oiwt, REAL* F,
+                           REAL* M, uint32_t N, REAL dt, REAL wE, REAL wG, REAL pA, REAL mu, REAL mur,
+                           REAL mP, REAL rP, const REAL* rad, const REAL* mass, const REAL* c,
+                           REAL wall_RR, REAL wall_top, REAL wall_bot, REAL wall_V, REAL Zcut, REAL* FL,
+                           double* sFL, int fixsum) {
   const uint32_t B = N / 64 + 1; /* md_data_types.h:66-70 */
   REAL* contrib_b = (REAL*)calloc((size_t)B * 64, sizeof(REAL));
   REAL* contrib_t = (REAL*)calloc((size_t)B * 64, sizeof(REAL));
@@ -658,6 +765,20 @@ void FN(orc_platen)(int axis, const REAL* R, const REAL* V, const REAL* W, REAL*
     }
     contrib_t[idx] = -s_t;
     contrib_b[idx] = -s_b;
+  }
+  if (fixsum) {
+    int64_t qb = 0, qt = 0;
+    for (uint32_t idx = 0; idx < N; ++idx) {
+      qb += llrint((double)contrib_b[idx] * 0x1p40);
+      qt += llrint((double)contrib_t[idx] * 0x1p40);
+    }
+    if (sFL) {
+      sFL[0] = (double)qb * 0x1p-40;
+      sFL[1] = (double)qt * 0x1p-40;
+    }
+    free(contrib_b);
+    free(contrib_t);
+    return;
   }
   /* 64-thread shared-memory tree of md_compression_hm.cu:243-300, then the
    * host double sum of md_results.cu:58-69 */

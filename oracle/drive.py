@@ -24,10 +24,16 @@ from . import sim
 
 def loading_run(st: sim.RefState, sc: sim.Scalars, *, brazil: bool, size_real, center_real, p_r: float,
                 min_stress: float, max_strain: float, cond_fracture: float, velocity: float, dt: float,
-                dNsave: int, max_steps: int, nobreak: int = 0, lateral=None, axis_center=None, **kw) -> dict:
+                dNsave: int, max_steps: int, nobreak: int = 0, lateral=None, axis_center=None,
+                fixsum: bool = False, on_step=None, **kw) -> dict:
     """Runs until the strain limit, fracture or max_steps.  `lateral`: indices
     of spheres whose mean distance from the vertical axis through
     axis_center (x, y) is recorded on every record step.
+    fixsum=True: pair, platen and lateral sums in 64-bit fixed point, as the
+    engine's deterministic mode sums them (sim.oracle_step), so that a whole
+    run of the engine in that mode can be compared with this one exactly.
+    on_step(step, st, comp), if given, is called after every step (the
+    controller updated); a true return value ends the run.
     Returns the record (strain, sigma_bottom, sigma_top per entry), the
     lateral record, the controller's results and the step count."""
     lib = L.lib()
@@ -48,18 +54,24 @@ def loading_run(st: sim.RefState, sc: sim.Scalars, *, brazil: bool, size_real, c
         sc.wall_top = float(np.float32(comp.Top))
         sc.wall_bot = float(np.float32(comp.Bottom))
         sc.wall_V = float(np.float32(comp.V))
-        out = sim.oracle_step(st, sc, sim.STAGE_ALL, nobreak=nobreak, **kw)
+        out = sim.oracle_step(st, sc, sim.STAGE_ALL, nobreak=nobreak, fixsum=fixsum, **kw)
         comp.sFL[0], comp.sFL[1] = float(out.sFL[0]), float(out.sFL[1])
         before = comp.stepsave
         if lateral is not None and dNsave and steps % dNsave == 0:
             x = st.R[lateral].astype(np.float64)
             y = st.R[n + lateral].astype(np.float64)
-            lat_val = float(np.sum(np.sqrt((x - axis_center[0]) ** 2 + (y - axis_center[1]) ** 2))) / lateral.size
+            d = np.sqrt((x - axis_center[0]) * (x - axis_center[0]) + (y - axis_center[1]) * (y - axis_center[1]))
+            if fixsum:
+                lat_val = float(np.rint(d * 2.0 ** 40).astype(np.int64).sum()) * 2.0 ** -40 / lateral.size
+            else:
+                lat_val = float(np.sum(d)) / lateral.size
         lib.orc_sum_forces(C.byref(comp), steps)
         if lateral is not None and comp.stepsave > before:
             lat.append(lat_val)
         lib.orc_compress_s3(C.byref(comp), dt, p_r)
         steps += 1
+        if on_step is not None and on_step(steps, st, comp):
+            break
         if not (abs(comp.Strain) < comp.MaxStrain) or comp.Fracture:
             break
     m = comp.stepsave

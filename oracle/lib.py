@@ -98,6 +98,13 @@ def _declare(L):
                                        R, _vp, _vp, _vp, _vp, _vp]
         g("orc_platen").argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _u32, R, R, R, R, R, R, R, R, _vp, _vp,
                                     _vp, R, R, R, R, R, _vp, _vp]
+        g("orc_forces_bpm_q").argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, R, R, R,
+                                          R, R, R, _vp, _vp, _vp, C.c_int, _vp, _vp]
+        g("orc_forces_hm_q").argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp, _u32, R, R, R, R, R, R, R, R, _vp,
+                                         _vp, _vp, _vp]
+        g("orc_fix_to_real").argtypes = [_vp, _vp, C.c_uint64]
+        g("orc_platen_q").argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _u32, R, R, R, R, R, R, R, R, _vp,
+                                      _vp, _vp, R, R, R, R, R, _vp]
         g("orc_increments").argtypes = [_vp, _vp, _vp, _vp, _vp, _u32, R, R, R, _vp, _vp]
         g("orc_cut_restriction").argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp]
         g("orc_soft_forces").argtypes = [_vp, _vp, _u32, _vp, _vp, _u32, R, R, _vp]

@@ -164,7 +164,8 @@ class RefState:
         IonP = d[prefix + "IL"].size // N
         s = cls(N=N, IonP=IonP, dtype=R.dtype.type)
         for k in cls.ARRAYS:
-            setattr(s, k, np.ascontiguousarray(d[prefix + k]))
+            # a copy: the steps work in place and must not change the caller's arrays
+            setattr(s, k, np.array(d[prefix + k], order="C", copy=True))
         return s
 
 
@@ -193,8 +194,15 @@ def oracle_setup_bonds(st: RefState, sc: Scalars, rad=None, gap: float = 0.0) ->
 
 
 def oracle_step(st: RefState, sc: Scalars, stages: int = STAGE_ALL, *, rad=None, mass=None, slot_br=None,
-                slot_sn=None, slot_st=None, dtm_i=None, dtI_i=None, want_abs: bool = False, nobreak: int = 0):
-    """One pass of the loop body; returns a StepOut (tolerance scales with want_abs)."""
+                slot_sn=None, slot_st=None, dtm_i=None, dtI_i=None, want_abs: bool = False, nobreak: int = 0,
+                fixsum: bool = False):
+    """One pass of the loop body; returns a StepOut (tolerance scales with want_abs).
+
+    fixsum=True sums the pair forces and moments of every particle, and the
+    platen forces, in 64-bit fixed point (orc_forces_*_q, orc_platen_q) -
+    the exact, order-independent sums of the engine's deterministic mode -
+    instead of the reference's running float sum over a particle's slots;
+    every per-pair value is the same."""
     N, R = st.N, st.R
     ov = 0
     if stages & STAGE_IL:
@@ -202,7 +210,19 @@ def oracle_step(st: RefState, sc: Scalars, stages: int = STAGE_ALL, *, rad=None,
         ov = L.fn("orc_il_reconstruct_bpm", R)(L.P(R), N, L.P(CIs), L.P(pnC), L.P(st.IL), L.P(st.ILtype),
                                                st.IonP, sc.a, sc.inv_a, sc.il_aacut, sc.nx, sc.ny, sc.nz)
     Fabs = Mabs = Fsens = None
-    if stages & STAGE_FORCES:
+    if stages & STAGE_FORCES and fixsum:
+        Fq = np.zeros(3 * N, np.int64)
+        Mq = np.zeros(3 * N, np.int64)
+        L.fn("orc_forces_bpm_q", R)(L.P(R), L.P(st.V), L.P(st.W), N, L.P(st.IL), L.P(st.ILtype), L.P(st.invL0),
+                                    L.P(st.Rij), L.P(st.Oijt), L.P(st.Mijn), L.P(st.Mijt), st.IonP, sc.dt, sc.m_E,
+                                    sc.m_G, sc.b_r, sc.m_Ec, sc.m_Gc, L.P(slot_br), L.P(slot_sn), L.P(slot_st),
+                                    nobreak, L.P(Fq), L.P(Mq))
+        L.fn("orc_forces_hm_q", R)(L.P(R), L.P(st.V), L.P(st.W), N, L.P(st.IL), L.P(st.ILtype), L.P(st.Oijt),
+                                   st.IonP, sc.dt, sc.hm_E, sc.hm_G, sc.p_A, sc.p_mu, sc.p_mur, sc.p_m, sc.p_r,
+                                   L.P(rad), L.P(mass), L.P(Fq), L.P(Mq))
+        L.fn("orc_fix_to_real", R)(L.P(Fq), L.P(st.F), 3 * N)
+        L.fn("orc_fix_to_real", R)(L.P(Mq), L.P(st.M), 3 * N)
+    elif stages & STAGE_FORCES:
         st.F[:] = 0
         st.M[:] = 0
         if want_abs:
@@ -218,7 +238,13 @@ def oracle_step(st: RefState, sc: Scalars, stages: int = STAGE_ALL, *, rad=None,
                                  sc.p_m, sc.p_r, L.P(rad), L.P(mass), L.P(Fabs), L.P(Mabs), L.P(Fsens))
     sFL = np.zeros(2, np.float64)
     FL = np.zeros(2 * (N // 64 + 1), st.dtype)
-    if stages & STAGE_PLATEN:
+    if stages & STAGE_PLATEN and fixsum:
+        c = np.asarray(sc.center, st.dtype)
+        L.fn("orc_platen_q", R)(1 if sc.brazil else 2, L.P(R), L.P(st.V), L.P(st.W), L.P(st.Oiwt), L.P(st.F),
+                                L.P(st.M), N, sc.dt, sc.wall_E, sc.wall_G, sc.p_A, sc.p_mu, sc.p_mur, sc.p_m, sc.p_r,
+                                L.P(rad), L.P(mass), L.P(c), sc.wall_RR, sc.wall_top, sc.wall_bot, sc.wall_V,
+                                sc.Zcut, L.P(sFL))
+    elif stages & STAGE_PLATEN:
         c = np.asarray(sc.center, st.dtype)
         L.fn("orc_platen", R)(1 if sc.brazil else 2, L.P(R), L.P(st.V), L.P(st.W), L.P(st.Oiwt), L.P(st.F),
                               L.P(st.M), N, sc.dt, sc.wall_E, sc.wall_G, sc.p_A, sc.p_mu, sc.p_mur, sc.p_m, sc.p_r,

@@ -142,3 +142,45 @@ def test_rsqrt_rn_is_correctly_rounded():
         exact = 1.0 / np.sqrt(np.float64(x))  # close to exact; correct rounding lies within 0.5 ulp
         ulp = np.spacing(y)
         assert abs(np.float64(y) - exact) <= 0.5 * np.float64(ulp) * (1 + 1e-6)
+
+
+def _shuffle_slots(st: sim.RefState, rng) -> sim.RefState:
+    """The same state with every particle's interaction-list slots in another
+    order (each slot's partner, type, 1/L0 and histories move together)."""
+    s = st.copy()
+    N, P = st.N, st.IonP
+    perm = np.argsort(rng.random((N, P)), axis=1)
+    src = (np.arange(N)[:, None] * P + perm).reshape(-1)
+    for k in ("IL", "ILtype", "invL0"):
+        getattr(s, k)[:] = getattr(st, k)[src]
+    for k in ("Rij", "Oijt", "Mijn", "Mijt"):
+        getattr(s, k)[:] = getattr(st, k).reshape(-1, 3)[src].reshape(-1)
+    return s
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fixed_point_sums_change_only_the_summation(name):
+    """oracle_step(fixsum=True), the sums of the engine's deterministic mode:
+    the same step as the reference's running float sums up to the rounding of
+    the sums (topology and histories identical, forces, moments and platen
+    sums within the reordering tolerance), and a result that does not depend
+    on the order of a particle's slots (bit for bit after shuffling them)."""
+    c, g = _case(name)
+    stages = sim.STAGE_FORCES | sim.STAGE_PLATEN | sim.STAGE_INCR
+    a = sim.RefState.from_dict(g, "in_")
+    b = a.copy()
+    out_a = sim.oracle_step(a, c.sc, stages, want_abs=True)
+    out_b = sim.oracle_step(b, c.sc, stages, fixsum=True)
+    used = a.IL != L.EMPTY
+    assert np.array_equal(a.ILtype[used], b.ILtype[used])
+    for k in ("Rij", "Oijt", "Mijn", "Mijt"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    assert (np.abs(a.F.astype(np.float64) - b.F) <= out_a.f_tol(a.F)).all()
+    assert (np.abs(a.M.astype(np.float64) - b.M) <= out_a.m_tol(a.M)).all()
+    assert np.allclose(out_b.sFL, out_a.sFL, rtol=1e-5, atol=1e-12)
+    # order independence: shuffled slots give the same bits
+    s = _shuffle_slots(sim.RefState.from_dict(g, "in_"), np.random.default_rng(3))
+    out_s = sim.oracle_step(s, c.sc, stages, fixsum=True)
+    for k in ("F", "M", "V", "R", "W", "Oiwt"):
+        assert np.array_equal(getattr(s, k), getattr(b, k)), k
+    assert np.array_equal(out_s.sFL, out_b.sFL)

@@ -121,6 +121,8 @@ def _declare(L):
     L.dem_create.argtypes = [P(Options), P(_vp)]
     L.dem_destroy.argtypes = [_vp]
     L.dem_destroy.restype = None
+    L.dem_release_cached_memory.argtypes = []
+    L.dem_release_cached_memory.restype = C.c_int
     L.dem_add_sample.argtypes = [_vp, P(Material), P(Loading), _vp, _vp, _u32, P(_i32)]
     L.dem_setup.argtypes = [_vp]
     L.dem_run.argtypes = [_vp, _u64, P(_u64)]
@@ -459,6 +461,12 @@ class Context:
 
 
 # --------------------------------------------------------------------------- stateless entry points
+
+def release_cached_memory() -> None:
+    """Device memory of closed contexts, kept for reuse by later contexts,
+    goes back to the driver (dem_release_cached_memory)."""
+    _ck(_lib().dem_release_cached_memory(), "dem_release_cached_memory")
+
 
 def ref_cells(xyz: np.ndarray, a: float, nx: int, ny: int, nz: int):
     xyz = np.ascontiguousarray(xyz, np.float32)

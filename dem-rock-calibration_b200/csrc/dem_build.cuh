@@ -176,6 +176,129 @@ __global__ void k_init_particles(const float* __restrict__ stage, uint32_t np, c
   }
 }
 
+// --- Morton order of the particles at set-up (device)
+
+// Interleaves the low 21 bits of x, y, z (x in bit 0).
+__host__ __device__ inline uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1FFFFF;
+    v = (v | v << 32) & 0x1F00000000FFFFull;
+    v = (v | v << 16) & 0x1F0000FF0000FFull;
+    v = (v | v << 8) & 0x100F00F00F00F00Full;
+    v = (v | v << 4) & 0x10C30C30C30C30C3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+// Quantisation frame of one sample: lower corner of its particles and 1/r_min.
+struct MortonFrame {
+  double lo[3];
+  double inv_q;
+  uint32_t p_begin, n;
+};
+
+// Key of set-up position p (the caller's order, samples one after another):
+// the sample's index above mbits, below it the Morton code of the position
+// quantised by r_min from the sample's lower corner (the host rule, bit for
+// bit); idx[p] = p.
+static __global__ void k_morton_keys(const float* __restrict__ stage, uint32_t np, const MortonFrame* __restrict__ fr,
+                              uint32_t nsamples, int mbits, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nsamples;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (fr[mid].p_begin <= p) lo = mid;
+      else hi = mid;
+    }
+    const MortonFrame F = fr[lo];
+    uint32_t c[3];
+    for (int d = 0; d < 3; ++d) {
+      const double v = ((double)stage[(size_t)d * np + p] - F.lo[d]) * F.inv_q;
+      c[d] = (uint32_t)fmin(fmax(v, 0.0), 2097151.0);
+    }
+    keys[p] = ((uint64_t)lo << mbits) | morton3(c[0], c[1], c[2]);
+    idx[p] = p;
+  }
+}
+
+// Stable LSD radix sort of (key, index) pairs, 8-bit digits: each block owns a
+// contiguous run of kSortItems items.  Pass 1 counts the block's digits
+// (hist[digit * blocks + block]); after an exclusive scan of hist, pass 2
+// scatters the block's items tile by tile in input order (within a tile a
+// warp match ranks equal digits by lane, warps are ranked by index), so equal
+// keys keep their input order.
+constexpr uint32_t kSortItems = 4096;
+
+static __global__ void __launch_bounds__(256) k_radix_hist(const uint64_t* __restrict__ keys, uint32_t n, int shift,
+                                                    uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t i0 = blockIdx.x * kSortItems, i1 = min(n, i0 + kSortItems);
+  for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & 255u], 1u);
+  __syncthreads();
+  hist[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+}
+
+static __global__ void __launch_bounds__(256) k_radix_scatter(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                       uint32_t n, int shift, const uint32_t* __restrict__ offs,
+                                                       uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+  __shared__ uint32_t base[256];     // next output slot of each digit for this block
+  __shared__ uint32_t wcnt[8][256];  // per warp: digit counts, then the digit's offset of the warp in the tile
+  __shared__ uint32_t tot[256];      // digit counts of the tile
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  base[threadIdx.x] = offs[(size_t)threadIdx.x * gridDim.x + blockIdx.x];
+  const uint32_t i0 = blockIdx.x * kSortItems, i1 = min(n, i0 + kSortItems);
+  for (uint32_t t0 = i0; t0 < i1; t0 += 256) {
+    for (uint32_t w = 0; w < 8; ++w) wcnt[w][threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t i = t0 + threadIdx.x;
+    const bool ok = i < i1;
+    const uint64_t k = ok ? kin[i] : 0ull;
+    const uint32_t v = ok ? vin[i] : 0u;
+    const uint32_t dg = ok ? ((uint32_t)(k >> shift) & 255u) : 256u;   // 256: no item
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (ok && rank == 0) wcnt[warp][dg] = __popc(peers);
+    __syncthreads();
+    {
+      uint32_t run = 0;
+      for (uint32_t w = 0; w < 8; ++w) {
+        const uint32_t c = wcnt[w][threadIdx.x];
+        wcnt[w][threadIdx.x] = run;
+        run += c;
+      }
+      tot[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (ok) {
+      const uint32_t o = base[dg] + wcnt[warp][dg] + rank;
+      kout[o] = k;
+      vout[o] = v;
+    }
+    __syncthreads();
+    base[threadIdx.x] += tot[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+// Storage position k holds set-up position idx[k]: the caller index within its
+// sample (the stage's order slot, read by k_init_particles).
+static __global__ void k_morton_perm(const uint32_t* __restrict__ idx, uint32_t np, const MortonFrame* __restrict__ fr,
+                              uint32_t nsamples, uint32_t* __restrict__ perm) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nsamples;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (fr[mid].p_begin <= k) lo = mid;
+      else hi = mid;
+    }
+    perm[k] = idx[k] - fr[lo].p_begin;
+  }
+}
+
 // --- pair search over the 27 surrounding cells
 enum PairMode : int {
   kModeRefSet = 0,  // reference interaction set: j != i, r^2 < add && !(r^2 > del) && !(r^2 < 1e-10)

@@ -96,6 +96,8 @@ void dem_destroy(dem_ctx* ctx) {
   delete ctx;
 }
 
+int dem_release_cached_memory(void) { GUARD(return dem::release_cached_memory();) }
+
 #define CTX_CALL(expr)                          \
   do {                                          \
     if (!ctx || !ctx->e) return DEM_ERR_ARG;    \

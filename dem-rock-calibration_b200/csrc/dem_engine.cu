@@ -4,9 +4,13 @@
 // dem::EngineBase in dem_capi.cpp.
 #include "dem_engine.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <unistd.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <functional>
 #include <condition_variable>
@@ -61,27 +65,186 @@ const char* last_error_detail() { return g_detail; }
     if (r_ != DEM_OK) return r_; \
   } while (0)
 
+// Time spent in device allocation and release (set-up trace, DEM_TRACE=1).
+static std::atomic<uint64_t> g_alloc_ns{0}, g_free_ns{0}, g_alloc_calls{0};
+static uint64_t now_ns() {
+  return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device blocks released by a context are kept for reuse by later allocations
+// in this process.  Calibration work creates many contexts of similar sizes
+// one after another, and a cudaMalloc cost about 230 us on average in the
+// set-up of a 490k-sphere context (12 ms of its 28 ms), while cudaFree
+// synchronises the device.  A cached block serves a request of at most its
+// size and at least about 4/5 of it.  A block enters the cache only after its
+// device has finished all queued work (a device synchronisation, the ordering
+// cudaFree gives), so a later user cannot race with kernels of the releasing
+// context.  Blocks are kept per CUDA context (its unique id): after a context
+// reset none of the old blocks is offered again.  Before a block is handed
+// out, the driver must still know it as an allocation of at least its size
+// starting at its address (a block that other code freed behind the cache's
+// back is dropped).  When cudaMalloc fails, the cached blocks of the current
+// context go back to the driver and the allocation is retried;
+// dem_release_cached_memory() returns them all on request.
+namespace blockcache {
+std::mutex mu;
+std::multimap<std::pair<unsigned long long, size_t>, void*> blocks;   // (context id, bytes) -> block
+PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+PFN_cuCtxGetId_v12000 get_id = nullptr;
+PFN_cuMemGetAddressRange_v3020 get_range = nullptr;
+bool resolved = false;
+
+// the driver functions, through the runtime's entry-point query (no link-time
+// dependency on the driver library); called with mu held
+bool resolve() {
+  if (resolved) return get_current && get_id && get_range;
+  resolved = true;
+  void* f[3] = {nullptr, nullptr, nullptr};
+  cudaDriverEntryPointQueryResult q[3];
+  if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f[0], 4000, cudaEnableDefault, &q[0]) != cudaSuccess ||
+      cudaGetDriverEntryPointByVersion("cuCtxGetId", &f[1], 12000, cudaEnableDefault, &q[1]) != cudaSuccess ||
+      cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &f[2], 3020, cudaEnableDefault, &q[2]) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  for (int k = 0; k < 3; ++k)
+    if (q[k] != cudaDriverEntryPointSuccess || !f[k]) return false;
+  get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f[0]);
+  get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f[1]);
+  get_range = reinterpret_cast<PFN_cuMemGetAddressRange_v3020>(f[2]);
+  return true;
+}
+
+// unique id of the calling thread's current context (0: unknown, no caching)
+unsigned long long context_id() {
+  std::lock_guard<std::mutex> lk(mu);
+  if (!resolve()) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+void* take(unsigned long long ctx, size_t bytes, size_t* got) {
+  if (!ctx) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = blocks.lower_bound({ctx, bytes});
+  while (it != blocks.end() && it->first.first == ctx && it->first.second <= bytes + bytes / 4 + (64u << 10)) {
+    void* p = it->second;
+    const size_t b = it->first.second;
+    it = blocks.erase(it);
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (get_range(&base, &size, (CUdeviceptr)p) == CUDA_SUCCESS && base == (CUdeviceptr)p && size >= b) {
+      *got = b;
+      return p;
+    }
+  }
+  return nullptr;
+}
+
+void give(unsigned long long ctx, int dev, void* p, size_t bytes) {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+  if (cur != dev && cur >= 0) cudaSetDevice(cur);
+  if (!idle || !ctx) {   // a device in an error state, or no context id: back to the driver
+    cudaFree(p);
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  blocks.emplace(std::make_pair(ctx, bytes), p);
+}
+
+// returns the cached blocks of context ctx (every context for ctx == 0) to the driver
+void trim(unsigned long long ctx) {
+  std::vector<void*> out;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto it = blocks.begin(); it != blocks.end();) {
+      if (!ctx || it->first.first == ctx) {
+        out.push_back(it->second);
+        it = blocks.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  for (void* p : out) cudaFree(p);
+}
+}  // namespace blockcache
+
+int release_cached_memory() {
+  blockcache::trim(0);
+  cudaGetLastError();   // a block of a context that no longer exists fails to free; nothing to report
+  return DEM_OK;
+}
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t cap = 0;   // bytes of the block held (at least n * sizeof(T))
+  int dev = 0;
+  unsigned long long ctx = 0;   // unique id of the CUDA context the block belongs to
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
+  // exchanges the blocks of two buffers (each keeps its block's capacity)
+  void swap(DBuf& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+    std::swap(cap, o.cap);
+    std::swap(dev, o.dev);
+    std::swap(ctx, o.ctx);
+  }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      const uint64_t t0 = now_ns();
+      blockcache::give(ctx, dev, p, cap);
+      g_free_ns += now_ns() - t0;
+    }
     p = nullptr;
     n = 0;
+    cap = 0;
   }
   cudaError_t alloc(size_t cnt) {
     release();
     n = cnt;
     if (cnt == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc((void**)&p, cnt * sizeof(T));
+    const uint64_t t0 = now_ns();
+    struct Acc {
+      uint64_t t0;
+      ~Acc() {
+        g_alloc_ns += now_ns() - t0;
+        ++g_alloc_calls;
+      }
+    } acc{t0};
+    cudaGetDevice(&dev);
+    ctx = blockcache::context_id();
+    const size_t bytes = (cnt * sizeof(T) + 255) & ~(size_t)255;
+    size_t got = 0;
+    p = (T*)blockcache::take(ctx, bytes, &got);
+    cudaError_t e = cudaSuccess;
+    if (p) {
+      cap = got;
+    } else {
+      e = cudaMalloc((void**)&p, bytes);
+      if (e == cudaErrorMemoryAllocation) {   // the cache's blocks back to the driver, then once more
+        cudaGetLastError();
+        blockcache::trim(ctx);
+        e = cudaMalloc((void**)&p, bytes);
+      }
+      cap = bytes;
+    }
     if (e != cudaSuccess) {
       p = nullptr;
       n = 0;
+      cap = 0;
       return e;
     }
     // zero-filled before returning: the fill runs on the legacy default
@@ -204,18 +367,6 @@ static void parallel_ranges(uint32_t n, Fn fn) {
 }
 
 // 63-bit Morton interleave of three 21-bit coordinates
-static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
-  auto spread = [](uint64_t v) {
-    v &= 0x1FFFFF;
-    v = (v | v << 32) & 0x1F00000000FFFFull;
-    v = (v | v << 16) & 0x1F0000FF0000FFull;
-    v = (v | v << 8) & 0x100F00F00F00F00Full;
-    v = (v | v << 4) & 0x10C30C30C30C30C3ull;
-    v = (v | v << 2) & 0x1249249249249249ull;
-    return v;
-  };
-  return spread(x) | (spread(y) << 1) | (spread(z) << 2);
-}
 
 struct SampleHost {
   dem_material mat{};
@@ -309,8 +460,12 @@ class Engine final : public EngineBase {
       line += b;
       t = now;
     }
+    uint64_t a0 = g_alloc_ns.load(), f0 = g_free_ns.load(), c0 = g_alloc_calls.load();
     void flush(const char* head) {
-      if (on) std::fprintf(stderr, "dem trace: %s%s\n", head, line.c_str());
+      if (on)
+        std::fprintf(stderr, "dem trace: %s%s (device allocations %llu: %.2f ms, releases %.2f ms)\n", head,
+                     line.c_str(), (unsigned long long)(g_alloc_calls.load() - c0),
+                     1e-6 * (double)(g_alloc_ns.load() - a0), 1e-6 * (double)(g_free_ns.load() - f0));
     }
   };
 
@@ -325,8 +480,18 @@ class Engine final : public EngineBase {
       s.p_begin = np_;
       np_ += s.n;
       derive(s);
-      morton_order(s);
     }
+    // Morton order of each sample (keys from its positions quantised by r_min,
+    // a stable sort): on the device, unless the sample index and the keys
+    // need more than 64 bits, then on the host (the same order either way)
+    std::vector<MortonFrame> frames(S);
+    int mbits = 0;
+    for (uint32_t si = 0; si < S; ++si) mbits = std::max(mbits, morton_frame(samples_[si], frames[si]));
+    int sbits = 0;
+    while (sbits < 32 && ((uint64_t)(S - 1) >> sbits) != 0) ++sbits;
+    const bool dev_order = mbits + sbits <= 64;
+    if (!dev_order)
+      for (auto& s : samples_) morton_order(s);
     tr.mark("order", stream_);
     // per-particle state, built on the device from the caller's arrays (one
     // upload of positions, radii and the storage order per sample)
@@ -358,9 +523,11 @@ class Engine final : public EngineBase {
           CK(cudaMemcpyAsync(stage.p + (size_t)d * np_ + s.p_begin, src, s.n * sizeof(float), cudaMemcpyHostToDevice,
                              stream_));
         }
-        CK(cudaMemcpyAsync(stage.p + 4 * (size_t)np_ + s.p_begin, s.perm.data(), s.n * sizeof(uint32_t),
-                           cudaMemcpyHostToDevice, stream_));
+        if (!dev_order)
+          CK(cudaMemcpyAsync(stage.p + 4 * (size_t)np_ + s.p_begin, s.perm.data(), s.n * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, stream_));
       }
+      if (dev_order) RC(device_morton(stage.p, frames, mbits, mbits + sbits));
       CK(tab.alloc(S));
       CK(cudaMemcpyAsync(tab.p, ht.data(), S * sizeof(InitSample), cudaMemcpyHostToDevice, stream_));
       k_init_particles<Real><<<grid1(np_), 256, 0, stream_>>>(stage.p, np_, tab.p, S, pos_.p, vel_.p, omg_.p, mass_.p,
@@ -370,11 +537,13 @@ class Engine final : public EngineBase {
     }
     tr.mark("upload", stream_);
     RC(mark_lateral());
+    tr.mark("lateral", stream_);
     // per-sample constants and controllers
     RC(upload_params());
+    tr.mark("params", stream_);
     // contact grids
     RC(make_grids());
-    tr.mark("params", stream_);
+    tr.mark("grids", stream_);
     // bonds
     RC(build_bonds());
     tr.mark("bonds", stream_);
@@ -534,22 +703,90 @@ class Engine final : public EngineBase {
     s.hm_G = P.hm_G;
   }
 
+  // Quantisation frame of a sample's Morton keys (lower corner of its
+  // particles, 1/r_min); returns the bits a key may need (3 x the bit length
+  // of the largest cell coordinate).
+  int morton_frame(const SampleHost& s, MortonFrame& F) {
+    const uint32_t n = s.n;
+    const uint32_t T = chunk_count(n);
+    F.inv_q = 1.0 / std::max(s.rmin, 1e-6);
+    F.p_begin = s.p_begin;
+    F.n = n;
+    // lower and upper corner of the particles (per-chunk extrema, then combined)
+    std::vector<double> clo(3 * (size_t)T, 1e300), chi(3 * (size_t)T, -1e300);
+    parallel_chunks(n, T, [&](uint32_t t, uint32_t k0, uint32_t k1) {
+      for (int d = 0; d < 3; ++d) {
+        double m = 1e300, M = -1e300;
+        for (uint32_t i = k0; i < k1; ++i) {
+          const double v = (double)s.xyz[d * n + i];
+          m = std::min(m, v);
+          M = std::max(M, v);
+        }
+        clo[3 * t + d] = m;
+        chi[3 * t + d] = M;
+      }
+    });
+    double hi[3] = {-1e300, -1e300, -1e300};
+    for (int d = 0; d < 3; ++d) F.lo[d] = 1e300;
+    for (uint32_t t = 0; t < T; ++t)
+      for (int d = 0; d < 3; ++d) {
+        F.lo[d] = std::min(F.lo[d], clo[3 * t + d]);
+        hi[d] = std::max(hi[d], chi[3 * t + d]);
+      }
+    int bits = 0;
+    for (int d = 0; d < 3; ++d) {
+      const uint32_t c = (uint32_t)std::min(std::max((hi[d] - F.lo[d]) * F.inv_q, 0.0), 2097151.0);
+      int b = 0;
+      while (b < 32 && (c >> b) != 0) ++b;
+      bits = std::max(bits, 3 * b);
+    }
+    return bits;
+  }
+
+  // Morton order on the device: keys of every sample's particles (the sample
+  // index above mbits), a stable LSD radix sort over `bits` bits, and the
+  // storage order written into the stage's order slot (and to the host).
+  int device_morton(float* stage, const std::vector<MortonFrame>& frames, int mbits, int bits) {
+    const uint32_t S = (uint32_t)frames.size();
+    DBuf<MortonFrame> fr;
+    DBuf<uint64_t> ka, kb;
+    DBuf<uint32_t> va, vb, hist, offs;
+    CK(fr.alloc(S));
+    CK(cudaMemcpyAsync(fr.p, frames.data(), S * sizeof(MortonFrame), cudaMemcpyHostToDevice, stream_));
+    const uint32_t nblk = ceil_div(np_, kSortItems);
+    CK(ka.alloc(np_));
+    CK(kb.alloc(np_));
+    CK(va.alloc(np_));
+    CK(vb.alloc(np_));
+    CK(hist.alloc(256 * (size_t)nblk));
+    CK(offs.alloc(256 * (size_t)nblk + 1));
+    k_morton_keys<<<grid1(np_), 256, 0, stream_>>>(stage, np_, fr.p, S, mbits, ka.p, va.p);
+    for (int shift = 0; shift < bits; shift += 8) {
+      k_radix_hist<<<nblk, 256, 0, stream_>>>(ka.p, np_, shift, hist.p);
+      RC(scan(hist.p, offs.p, 256 * nblk));
+      k_radix_scatter<<<nblk, 256, 0, stream_>>>(ka.p, va.p, np_, shift, offs.p, kb.p, vb.p);
+      ka.swap(kb);
+      va.swap(vb);
+    }
+    uint32_t* perm = reinterpret_cast<uint32_t*>(stage + 4 * (size_t)np_);
+    k_morton_perm<<<grid1(np_), 256, 0, stream_>>>(va.p, np_, fr.p, S, perm);
+    CK(cudaGetLastError());
+    for (auto& s : samples_) {
+      s.perm.resize(s.n);
+      CK(cudaMemcpyAsync(s.perm.data(), perm + s.p_begin, s.n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+      s.inv.clear();   // built when first needed (inverse())
+    }
+    CK(cudaStreamSynchronize(stream_));   // before the sort's buffers are released
+    return DEM_OK;
+  }
+
   void morton_order(SampleHost& s) {
     const uint32_t n = s.n;
     const uint32_t T = chunk_count(n);
-    const double inv_q = 1.0 / std::max(s.rmin, 1e-6);
-    // lower corner of the particles (per-chunk minima, then combined)
-    std::vector<double> clo(3 * (size_t)T, 1e300);
-    parallel_chunks(n, T, [&](uint32_t t, uint32_t k0, uint32_t k1) {
-      for (int d = 0; d < 3; ++d) {
-        double m = 1e300;
-        for (uint32_t i = k0; i < k1; ++i) m = std::min(m, (double)s.xyz[d * n + i]);
-        clo[3 * t + d] = m;
-      }
-    });
-    double lo[3] = {1e300, 1e300, 1e300};
-    for (uint32_t t = 0; t < T; ++t)
-      for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], clo[3 * t + d]);
+    MortonFrame F;
+    morton_frame(s, F);
+    const double inv_q = F.inv_q;
+    const double* lo = F.lo;
     // keys, and their largest value (only the digits below its top bit vary)
     // (left uninitialised: every entry is written before it is read)
     std::unique_ptr<uint64_t[]> ka(new uint64_t[n]), kb(new uint64_t[n]);

@@ -57,6 +57,8 @@ class EngineBase {
 };
 
 EngineBase* make_engine(const dem_options& o, int* err);
+// device blocks kept for reuse after their contexts closed go back to the driver
+int release_cached_memory();
 int ref_cells(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* CI,
               uint32_t* CIs, uint32_t* pnC);
 int ref_neighbor_sets(const float* xyz, uint32_t n, float a, uint32_t nx, uint32_t ny, uint32_t nz, float add_thr,

@@ -149,7 +149,14 @@ typedef struct {
 
 /* --- context and specimens --- */
 int dem_create(const dem_options* opt, dem_ctx** out);
+/* Device memory of a destroyed context stays with the library for reuse by
+ * later contexts of this process (a calibration creates many of similar
+ * sizes; a fresh allocation costs far more than reuse).  It goes back to the
+ * driver when an allocation would otherwise fail, and on
+ * dem_release_cached_memory() (no counterpart in the reference), for a host
+ * that needs the memory for something else. */
 void dem_destroy(dem_ctx* ctx);
+int dem_release_cached_memory(void);
 const char* dem_strerror(int code);
 /* Text of the last CUDA error the library saw on this host thread (error name,
  * message, source location), "" if none; kept until the next CUDA error. */

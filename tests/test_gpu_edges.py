@@ -184,3 +184,24 @@ def test_non_finite_state_stops_its_sample_and_is_reported():
         ctx.add_sample(_mat(J), ld, bad, J.rad)
     assert e.value.code == -1
     ctx.close()
+
+
+def test_contexts_reusing_cached_memory_repeat_exactly():
+    """A closed context's device memory is reused by the next one (the
+    library's block cache): every reused block starts zeroed, so the same
+    run repeats bit for bit in a context of reused memory, after the cache
+    went back to the driver (dem_release_cached_memory), and in a fresh one."""
+    J = _spec(n=2000, seed=8)
+    out = []
+    for k in range(3):
+        ctx = dem.Context(deterministic=True)
+        sid = ctx.add_sample(_mat(J), _loading(J, max_steps=1500), J.xyz, J.rad)
+        ctx.setup()
+        ctx.run(10 ** 6)
+        rec, _ = ctx.record(sid)
+        out.append((ctx.result(sid)["FractureStress"], ctx.particles(sid)["R"].copy(), rec))
+        ctx.close()
+        if k == 1:
+            dem.release_cached_memory()
+    for fs, R, rec in out[1:]:
+        assert fs == out[0][0] and np.array_equal(R, out[0][1]) and np.array_equal(rec, out[0][2])

@@ -48,7 +48,7 @@ METRIC = "BPM particle-steps/s"
 UNIT = "particle-steps/s"
 # DRAM bytes (read + write) of one k_pairs launch on the default workload (two
 # 245,098-sphere Brazilian discs), ncu --set full early in the loading
-PAIR_TRAFFIC_DISC_X2 = 193.8e6
+PAIR_TRAFFIC_DISC_X2 = 195.5e6
 
 
 def dist_env():
@@ -762,16 +762,13 @@ def run_solves(args, ws, rank, local):
     return 0
 
 
-def run_postpeak(args, ws, rank, local):
-    """The default workload's discs loaded past the peak first: platens at
-    ten times the configuration's speed, no stop condition, until every disc
-    has lost `--damage` of its bonds; then the timed steps, where broken
+def postpeak_measure(dem, args, specs, local, steps: int, warmup: int, D=None) -> dict:
+    """The discs `specs` loaded past the peak first (platens at ten times the
+    configuration's speed, no stop condition) until every disc has lost
+    `args.damage` of its bonds, then `steps` timed steps in which broken
     bonds and new touching pairs make the Hertz-Mindlin contacts and the
-    contact-list rebuilds part of every step.  Every rank loads its own discs
-    (weak scaling)."""
-    dem = importlib.import_module("dem-rock-calibration_b200")
-    D = Dist(ws)
-    specs = [build_specimen(dem, "brazilian_disc", sd, local) for sd in specimen_seeds(args, rank)]
+    contact-list rebuilds part of every step.  D (optional): the timing
+    barrier and max over ranks."""
     ctx = dem.Context(precision=args.precision, device=local, graph_steps=200, pair_min_blocks=args.pair_min_blocks,
                       deterministic=args.deterministic, skin_factor=args.skin)
     sids = []
@@ -791,19 +788,18 @@ def run_postpeak(args, ws, rank, local):
         if all(r["bonds_now"] <= (1.0 - args.damage) * r["bonds_initial"] for r in res):
             break
     t_prep = time.perf_counter() - t0
-    cnt = ctx.counts()
-    n_gpu = cnt["particles"]
-    ctx.run_timed(args.warmup)
+    n_gpu = ctx.counts()["particles"]
+    ctx.run_timed(warmup)
     rb0 = ctx.result(sids[0])["rebuilds"]
-    D.barrier()
+    if D is not None:
+        D.barrier()
     clk = Clocks(local)
-    ms = ctx.run_timed(args.steps)
+    ms = ctx.run_timed(steps)
     clocks = clk.stop()
-    D.barrier()
+    if D is not None:
+        D.barrier()
     rb1 = ctx.result(sids[0])["rebuilds"]
-    ms_max = D.max(ms)
-    value = D.sum(float(n_gpu)) * args.steps / (ms_max * 1e-3)
-    prof = ctx.profile(min(args.steps, 300))
+    prof = ctx.profile(min(steps, 300))
     res = [ctx.result(s) for s in sids]
     cnt = ctx.counts()
     ctx.close()
@@ -811,24 +807,40 @@ def run_postpeak(args, ws, rank, local):
     A = algorithmic_bytes(n_gpu, bonds, prof["touching"], fp64=args.precision == 1)
     achieved = A / (prof["pair_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
+    return dict(n_gpu=n_gpu, ms=ms, clocks=clocks, prep=prep, t_prep=t_prep, rebuilds_timed=rb1 - rb0, prof=prof,
+                bonds=bonds, bonds_initial=sum(r["bonds_initial"] for r in res), contacts=cnt["contacts"],
+                stale=sum(r["stale"] for r in res), done=[r["done"] for r in res], A=A, achieved=achieved, peak=peak,
+                peak_kind=peak_kind)
+
+
+def run_postpeak(args, ws, rank, local):
+    """The default workload's discs loaded past the peak, then timed
+    (postpeak_measure).  Every rank loads its own discs (weak scaling)."""
+    dem = importlib.import_module("dem-rock-calibration_b200")
+    D = Dist(ws)
+    specs = [build_specimen(dem, "brazilian_disc", sd, local) for sd in specimen_seeds(args, rank)]
+    m = postpeak_measure(dem, args, specs, local, args.steps, args.warmup, D)
+    ms_max = D.max(m["ms"])
+    value = D.sum(float(m["n_gpu"])) * args.steps / (ms_max * 1e-3)
+    prof = m["prof"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == 1 else "f32", "data": "synthetic (seeded packings, FIRE-relaxed)",
         "config": {"workload": f"{args.specimens} x brazilian_disc loaded past the peak ({args.damage:.0%} of the "
-                               f"bonds broken)", "particles_per_gpu": n_gpu, "specimens": args.specimens,
+                               f"bonds broken)", "particles_per_gpu": m["n_gpu"], "specimens": args.specimens,
                    "seeds": specimen_seeds(args, 0), "parallelism": f"{ws} GPU(s), independent specimens",
                    "l2": "inputs larger than L2, no flush"},
-        "details": {"bonds_intact": bonds, "bonds_initial": sum(r["bonds_initial"] for r in res),
-                    "contacts_listed": cnt["contacts"], "touching_contacts": prof["touching"],
-                    "contact_list_builds_timed": rb1 - rb0, "preparation_steps": prep,
-                    "preparation_seconds_untimed": t_prep, "stale_lists": sum(r["stale"] for r in res),
-                    "done": [r["done"] for r in res]},
-        "gpu_launches": None, "clocks": clocks,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
+        "details": {"bonds_intact": m["bonds"], "bonds_initial": m["bonds_initial"],
+                    "contacts_listed": m["contacts"], "touching_contacts": prof["touching"],
+                    "contact_list_builds_timed": m["rebuilds_timed"], "preparation_steps": m["prep"],
+                    "preparation_seconds_untimed": m["t_prep"], "stale_lists": m["stale"], "done": m["done"]},
+        "gpu_launches": None, "clocks": m["clocks"],
+        "roofline": {"bound": "hbm", "achieved": m["achieved"], "peak": m["peak"], "unit": "GB/s",
+                     "frac": m["achieved"] / m["peak"], "traffic": None,
+                     "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
                      "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
-                     "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
+                     "algorithmic_bytes_per_step": m["A"], "peak_kind": m["peak_kind"]},
         "e2e": None, "cpu_baseline": None,
     }
     if rank == 0:
@@ -853,6 +865,8 @@ def main() -> int:
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--post-peak-steps", type=int, default=200,
+                    help="brazilian_disc: also time this many steps of the discs after the peak (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sim-size", type=int, default=2000, help="surrogate --sim-data: spheres per specimen")
     ap.add_argument("--sim-batch", type=int, default=256, help="surrogate --sim-data: parameter sets per context")
@@ -949,6 +963,19 @@ def main() -> int:
     e2e_val = D.sum(n_gpu * args.steps / t_e2e)
     h2d = sum(sp.xyz.nbytes + sp.radii.nbytes for sp in specs)
     d2h = sum(r.nbytes + b.nbytes for r, b in recs) + len(specs) * 160
+    # the same discs after the peak (Hertz-Mindlin contacts and list rebuilds in
+    # every step), this rank's GPU
+    post = None
+    if args.post_peak_steps > 0 and args.workload == "brazilian_disc":
+        m = postpeak_measure(dem, args, specs, local, args.post_peak_steps, 20)
+        post = {"value": m["n_gpu"] * args.post_peak_steps / (m["ms"] * 1e-3), "unit": UNIT,
+                "ms_per_step": m["ms"] / args.post_peak_steps, "steps": args.post_peak_steps,
+                "bonds_broken": 1.0 - m["bonds"] / m["bonds_initial"],
+                "touching_contacts": m["prof"]["touching"], "contact_list_builds_timed": m["rebuilds_timed"],
+                "stale_lists": m["stale"], "pair_ms": m["prof"]["pair_ms"], "particle_ms": m["prof"]["particle_ms"],
+                "roofline_frac": m["achieved"] / m["peak"], "clocks": m["clocks"],
+                "note": "rank 0's discs loaded past the peak at ten times the platen speed until "
+                        f"{args.damage:.0%} of the bonds broke (untimed), then timed"}
     cpu = cpu_bpm = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, el, th, steps = cpu_baseline([spec], args.cpu_steps, 1, os.cpu_count() or 1)
@@ -969,7 +996,8 @@ def main() -> int:
                     "contact_list_builds_timed": rb1 - rb0, "state_mb": state_mb,
                     "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
                                         "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
-                                        "note": "state inside the L2"}},
+                                        "note": "state inside the L2"},
+                    "post_peak": post},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -18,7 +18,7 @@ the same bit for bit: the same number of steps, the same stress-strain and
 lateral records, and so the same uniaxial compressive strength, strain at
 peak, Young's modulus, Poisson ratio and Brazilian tensile strength.
 
-Five seeds each of:
+Five seeds each of (and the FP64 build on three of the physics cases):
 * the configurations' physics: polydisperse radii U[0.20, 0.30] mm (4 x 8 mm
   cylinders, 30% post-peak stress drop) and U[0.18, 0.30] mm (6 x 3 mm
   discs, to the Brazilian controller's fracture), bond modulus 30 GPa, kn/ks
@@ -50,11 +50,12 @@ SEEDS = (1, 2, 3, 4, 5)
 PK = dict(growth_stages=20, steps_per_stage=150, max_fire_steps=4000)
 
 
-def _engine(mat, ld, xyz, radii=None):
-    ctx = dem.Context(deterministic=True)
+def _engine(mat, ld, xyz, radii=None, precision=0):
+    fp64 = precision == 1
+    ctx = dem.Context(deterministic=True, precision=precision)
     sid = ctx.add_sample(mat, ld, xyz, radii)
     ctx.setup()
-    init = (ctx.particles(sid), ctx.pairs(sid), ctx.result(sid))
+    init = (ctx.particles(sid, double=fp64), ctx.pairs(sid, double=fp64), ctx.result(sid))
     ctx.run(10 ** 7)
     res = ctx.result(sid)
     rec, _ = ctx.record(sid)
@@ -103,12 +104,10 @@ def _physics(kind, seed):
     return sp, mat, ld
 
 
-@pytest.mark.parametrize("seed", SEEDS)
-@pytest.mark.parametrize("kind", ["uniaxial", "brazilian"])
-def test_configuration_physics_runs_are_identical(kind, seed):
+def _physics_runs_are_identical(kind, seed, precision):
     sp, mat, ld = _physics(kind, seed)
-    (p0, pr0, r0), res, rec, lat = _engine(mat, ld, sp.xyz, sp.radii)
-    pc = PH.physics_case(mat, ld, sp.radii, dt=r0["dt"])
+    (p0, pr0, r0), res, rec, lat = _engine(mat, ld, sp.xyz, sp.radii, precision)
+    pc = PH.physics_case(mat, ld, sp.radii, dt=r0["dt"], dtype=np.float64 if precision == 1 else np.float32)
     # the oracle starts from the engine's bonded state (the bond set and 1/L0
     # are pinned separately, test_gpu_physics_parity.py)
     st, sbr, ssn, sst = PH.ref_state_from_pairs(p0["R"], p0["V"], p0["W"], p0["Oiwt"], pr0, pc)
@@ -118,12 +117,26 @@ def test_configuration_physics_runs_are_identical(kind, seed):
                                         float(np.mean(sp.radii.astype(np.float64))))
         axis = np.float32(np.array(ld.center_real[:2])).astype(np.float64)
     o = _oracle(st, pc.sc, ld, r0["dt"], ld.p_r_platen, lateral, axis, **pc.kw(sbr, ssn, sst))
-    _same(f"\n{kind} seed {seed} ({sp.n} spheres)", res, rec, o, lat if kind == "uniaxial" else None)
+    _same(f"\n{kind} seed {seed} ({sp.n} spheres, {'FP64' if precision == 1 else 'FP32'})", res, rec, o,
+          lat if kind == "uniaxial" else None)
     if kind == "uniaxial":
         E_e, nu_e = drive.chord_moduli(rec, lat)
         E_o, nu_o = drive.chord_moduli(o["rec"], o["lat"])
         assert E_e == E_o and nu_e == nu_o and E_e == pytest.approx(res["E_chord"], rel=1e-12)
         print(f"  E {E_e:.6g} GPa, nu {nu_e:.6g} (both)")
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+@pytest.mark.parametrize("kind", ["uniaxial", "brazilian"])
+def test_configuration_physics_runs_are_identical(kind, seed):
+    _physics_runs_are_identical(kind, seed, 0)
+
+
+@pytest.mark.parametrize("kind,seed", [("uniaxial", 1), ("uniaxial", 2), ("brazilian", 2)])
+def test_fp64_runs_are_identical(kind, seed):
+    """The FP64 build (double state and arithmetic, pair sums in 2^-50 fixed
+    point) against the oracle's double path with the same sums."""
+    _physics_runs_are_identical(kind, seed, 1)
 
 
 def _ref_specimen(kind, seed):

@@ -287,6 +287,14 @@ def algorithmic_bytes(n, bonds, touching, fp64=False):
     return 60.0 * n + 104.0 * bonds + 28.0 * touching
 
 
+def particle_bytes(n, fp64=False):
+    """Per step, the particle kernel: position, velocity, spin, list reference,
+    force and moment read (6 x 16 B), sample id and platen flag (5 B);
+    position, velocity and spin written and the force and moment
+    accumulators reset (5 x 16 B): 181 B per particle (FP64: 357 B)."""
+    return (357.0 if fp64 else 181.0) * n
+
+
 def cpu_baseline(specs, nsteps: int, warmup: int, threads: int):
     """Times nsteps loop bodies of every specimen (after `warmup` untimed
     ones) on `threads` host threads: particle-steps/s, seconds, threads."""
@@ -1006,7 +1014,14 @@ def main() -> int:
                      "traffic": PAIR_TRAFFIC_DISC_X2 if default_disc else None,
                      "kernel": "k_pairs (BPM bonds + Hertz-Mindlin contacts)",
                      "pair_ms": prof["pair_ms"], "particle_ms": prof["particle_ms"],
-                     "algorithmic_bytes_per_step": A, "peak_kind": peak_kind},
+                     "algorithmic_bytes_per_step": A, "peak_kind": peak_kind,
+                     # the whole step (both kernels, launch gaps, rebuilds): bytes of the pair
+                     # and particle kernels over the measured time per step
+                     "step": {"bytes": A + particle_bytes(n_gpu, args.precision == 1),
+                              "achieved": (A + particle_bytes(n_gpu, args.precision == 1))
+                              / (ms_max / args.steps * 1e-3) / 1e9,
+                              "frac": (A + particle_bytes(n_gpu, args.precision == 1))
+                              / (ms_max / args.steps * 1e-3) / 1e9 / peak}},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps, "seconds": t_e2e, "setup_seconds": t_setup,
                 "run_seconds": t_run, "close_seconds_untimed": t_close,

@@ -84,12 +84,17 @@ static uint64_t now_ns() {
 // reset none of the old blocks is offered again.  Before a block is handed
 // out, the driver must still know it as an allocation of at least its size
 // starting at its address (a block that other code freed behind the cache's
-// back is dropped).  When cudaMalloc fails, the cached blocks of the current
-// context go back to the driver and the allocation is retried;
-// dem_release_cached_memory() returns them all on request.
+// back is dropped).  The cache holds at most 40% of the device's memory.
+// When cudaMalloc fails, the cached blocks of the current context go back to
+// the driver and the allocation is retried; dem_release_cached_memory()
+// returns them all on request.
 namespace blockcache {
 std::mutex mu;
 std::multimap<std::pair<unsigned long long, size_t>, void*> blocks;   // (context id, bytes) -> block
+size_t cached_bytes = 0;
+// the cache holds at most this share of the device's memory; a block released
+// beyond it goes back to the driver at once
+constexpr double kMaxShare = 0.4;
 PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
 PFN_cuCtxGetId_v12000 get_id = nullptr;
 PFN_cuMemGetAddressRange_v3020 get_range = nullptr;
@@ -135,6 +140,7 @@ void* take(unsigned long long ctx, size_t bytes, size_t* got) {
     void* p = it->second;
     const size_t b = it->first.second;
     it = blocks.erase(it);
+    cached_bytes -= b;
     CUdeviceptr base = 0;
     size_t size = 0;
     if (get_range(&base, &size, (CUdeviceptr)p) == CUDA_SUCCESS && base == (CUdeviceptr)p && size >= b) {
@@ -150,13 +156,19 @@ void give(unsigned long long ctx, int dev, void* p, size_t bytes) {
   cudaGetDevice(&cur);
   if (cur != dev) cudaSetDevice(dev);
   const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+  size_t free_b = 0, total_b = 0;
+  if (idle && cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) total_b = 0;
   if (cur != dev && cur >= 0) cudaSetDevice(cur);
-  if (!idle || !ctx) {   // a device in an error state, or no context id: back to the driver
-    cudaFree(p);
-    return;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (idle && ctx && cached_bytes + bytes <= (size_t)(kMaxShare * (double)total_b)) {
+      blocks.emplace(std::make_pair(ctx, bytes), p);
+      cached_bytes += bytes;
+      return;
+    }
   }
-  std::lock_guard<std::mutex> lk(mu);
-  blocks.emplace(std::make_pair(ctx, bytes), p);
+  // a device in an error state, no context id, or a full cache: back to the driver
+  cudaFree(p);
 }
 
 // returns the cached blocks of context ctx (every context for ctx == 0) to the driver
@@ -167,6 +179,7 @@ void trim(unsigned long long ctx) {
     for (auto it = blocks.begin(); it != blocks.end();) {
       if (!ctx || it->first.first == ctx) {
         out.push_back(it->second);
+        cached_bytes -= it->first.second;
         it = blocks.erase(it);
       } else {
         ++it;

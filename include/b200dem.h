@@ -151,8 +151,9 @@ typedef struct {
 int dem_create(const dem_options* opt, dem_ctx** out);
 /* Device memory of a destroyed context stays with the library for reuse by
  * later contexts of this process (a calibration creates many of similar
- * sizes; a fresh allocation costs far more than reuse).  It goes back to the
- * driver when an allocation would otherwise fail, and on
+ * sizes; a fresh allocation costs far more than reuse), up to 40% of the
+ * device's memory.  It goes back to the driver when an allocation would
+ * otherwise fail, and on
  * dem_release_cached_memory() (no counterpart in the reference), for a host
  * that needs the memory for something else. */
 void dem_destroy(dem_ctx* ctx);

@@ -176,6 +176,12 @@ __global__ void k_init_particles(const float* __restrict__ stage, uint32_t np, c
   }
 }
 
+// out[k] = src[idx[k]]
+static __global__ void k_gather_u32(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint32_t n,
+                                    uint32_t* __restrict__ out) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[k] = src[idx[k]];
+}
+
 // --- Morton order of the particles at set-up (device)
 
 // Interleaves the low 21 bits of x, y, z (x in bit 0).
@@ -474,13 +480,6 @@ static __global__ void k_expand_stride(const uint32_t* __restrict__ offset, uint
     const uint32_t m = n < kSearchStride ? n : kSearchStride;
     for (uint32_t r = 0; r < m; ++r) ij[k0 + r] = make_uint2(i, js[(size_t)i * kSearchStride + r]);
   }
-}
-
-// Expand per-particle partner lists (CSR by i) into (i, j) pairs.
-static __global__ void k_expand_pairs(const uint32_t* __restrict__ offset, uint32_t np, const uint32_t* __restrict__ js,
-                               uint2* __restrict__ ij) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x)
-    for (uint32_t k = offset[i], e = offset[i + 1]; k < e; ++k) ij[k] = make_uint2(i, js[k]);
 }
 
 // Bond state at creation (d_ConstructBoundInteractions, md_boundinteractions_construct.cu:57-98):

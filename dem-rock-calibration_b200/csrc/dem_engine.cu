@@ -1076,7 +1076,12 @@ class Engine final : public EngineBase {
     PairSearch<Real> S = search_args(kModeBond);
     S.gap = gap_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
-    k_pair_search<Real, false><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
+    // one search pass: every sphere's count and its sorted partners in
+    // kSearchStride slots of its own (the slots serve the contact-list builds
+    // too), compacted below once the counts are scanned
+    if (c_jstride_.n < (size_t)np_ * kSearchStride) CK(c_jstride_.alloc((size_t)np_ * kSearchStride));
+    S.out_j = c_jstride_.p;
+    k_pair_search<Real, 2><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     RC(scan(cnt_.p, offs_.p, np_));
     uint32_t nb = 0, ovf = 0;
     CK(cudaMemcpyAsync(&nb, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
@@ -1084,10 +1089,6 @@ class Engine final : public EngineBase {
     CK(cudaStreamSynchronize(stream_));
     if (ovf) return DEM_ERR_CAPACITY;
     nb_ = nb;
-    DBuf<uint32_t> js;
-    CK(js.alloc(std::max(nb, 1u)));
-    S.out_j = js.p;
-    k_pair_search<Real, true><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     // whole tiles: the pair kernel copies bond state tile by tile
     const size_t nb_pad = ((size_t)std::max(nb, 1u) + 255) / 256 * 256;
     CK(b_ij_.alloc(nb_pad));
@@ -1099,25 +1100,33 @@ class Engine final : public EngineBase {
     const uint32_t S_ = (uint32_t)samples_.size();
     DBuf<int32_t> counts;
     CK(counts.alloc(S_));
-    k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, js.p, b_ij_.p);
+    k_expand_stride<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_jstride_.p, b_ij_.p);
     CK(cudaMemcpyAsync(b_row_.p, offs_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
     if (nb)
       k_bond_init<Real><<<grid1(nb), 256, 0, stream_>>>(b_ij_.p, nb, pos_.p, sid_.p, orig_.p, law_.p, b_s0_.p,
                                                        b_s1_.p, b_s2_.p, b_par_.p, counts.p);
+    // bond range of every sample (bonds are stored in particle order, and the
+    // particles of a sample are contiguous): the bond row at each sample's
+    // first particle, and at the end, gathered on the device
+    std::vector<uint32_t> hidx(S_ + 1), hrow(S_ + 1);
+    for (uint32_t si = 0; si < S_; ++si) hidx[si] = samples_[si].p_begin;
+    hidx[S_] = np_;
+    DBuf<uint32_t> ridx, rval;
+    CK(ridx.alloc(S_ + 1));
+    CK(rval.alloc(S_ + 1));
+    CK(cudaMemcpyAsync(ridx.p, hidx.data(), (S_ + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+    k_gather_u32<<<ceil_div(S_ + 1, 256), 256, 0, stream_>>>(b_row_.p, ridx.p, S_ + 1, rval.p);
     CK(cudaGetLastError());
     std::vector<int32_t> hc(S_);
     CK(cudaMemcpyAsync(hc.data(), counts.p, S_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hrow.data(), rval.p, (S_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     for (uint32_t si = 0; si < S_; ++si) samples_[si].bonds_initial = hc[si];
-    // bond range of every sample (bonds are stored in particle order, and the
-    // particles of a sample are contiguous)
-    std::vector<uint32_t> row(np_ + 1);
-    CK(cudaMemcpy(row.data(), b_row_.p, (np_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     sb_begin_.assign(S_, 0);
     sb_end_.assign(S_, 0);
     for (uint32_t si = 0; si < S_; ++si) {
-      sb_begin_[si] = row[samples_[si].p_begin];
-      sb_end_[si] = row[samples_[si].p_begin + samples_[si].n];
+      sb_begin_[si] = hrow[si];
+      sb_end_[si] = hrow[si + 1];
     }
     tiles_.release();
     ntiles_.release();
@@ -1201,19 +1210,12 @@ class Engine final : public EngineBase {
     S.b_row = b_row_.p;
     S.b_ij = b_ij_.p;
     CK(cudaMemsetAsync(ovf_.p, 0, sizeof(uint32_t), stream_));
-    // rebuilds during a run: one search pass (the counts and every particle's
-    // partners, sorted, in kSearchStride slots of its own, compacted below once
-    // the counts are scanned).  The first build (at set-up) counts, then fills
-    // the exact-size list in a second pass: it does not allocate the slots
-    // (np x kSearchStride indices) a short run would never use.
-    const bool one_pass = !first;
-    if (one_pass) {
-      if (c_jstride_.n < (size_t)np_ * kSearchStride) CK(c_jstride_.alloc((size_t)np_ * kSearchStride));
-      S.out_j = c_jstride_.p;
-      k_pair_search<Real, 2><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
-    } else {
-      k_pair_search<Real, 0><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
-    }
+    // one search pass (the counts and every particle's partners, sorted, in
+    // kSearchStride slots of its own, compacted below once the counts are
+    // scanned)
+    if (c_jstride_.n < (size_t)np_ * kSearchStride) CK(c_jstride_.alloc((size_t)np_ * kSearchStride));
+    S.out_j = c_jstride_.p;
+    k_pair_search<Real, 2><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
     RC(scan(cnt_.p, offs_.p, np_));
     uint32_t nc = 0, ovf = 0;
     CK(cudaMemcpyAsync(&nc, offs_.p + np_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
@@ -1251,16 +1253,7 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(stream_));
       }
     }
-    if (one_pass) {
-      k_expand_stride<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_jstride_.p, c_ij_new_.p);
-    } else {
-      DBuf<uint32_t> js;
-      CK(js.alloc(std::max<size_t>(nc, 1)));
-      S.out_j = js.p;
-      k_pair_search<Real, 1><<<pair_search_blocks(np_), 128, 0, stream_>>>(S);
-      k_expand_pairs<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, js.p, c_ij_new_.p);
-      CK(cudaStreamSynchronize(stream_));   // js is released at the end of this block
-    }
+    k_expand_stride<<<grid1(np_), 256, 0, stream_>>>(offs_.p, np_, c_jstride_.p, c_ij_new_.p);
     if (nc) {
       if (first)
         CK(cudaMemsetAsync(c_row_.p, 0, (np_ + 1) * sizeof(uint32_t), stream_));

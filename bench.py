@@ -713,56 +713,66 @@ def run_solves_cfg2(args, ws, rank, local):
     return 0
 
 
-def run_solves(args, ws, rank, local):
+def solves_measure(args, rank, local, cases: int, plain_cases: int, D=None) -> dict:
     """Calibration solves per hour: `cases` uniaxial tests of one packed
     cylinder of about 2,000 spheres (Latin-hypercube micro-parameters over the
     sweep box), each run until its peak has passed (stress down to 70% of the
     peak) or 1% strain, all in one context; against the same solves one
     context at a time (the plain method: one specimen per run, as the
-    reference's CalculateOneSample), on a bounded sample of the cases.  Times
+    reference's CalculateOneSample), on the first `plain_cases` cases.  Times
     are wall-clock per whole solve (context, set-up, loading to the end,
-    results back), the unit a calibration pays for; every rank solves its own
-    cases (weak scaling)."""
+    results back), the unit a calibration pays for.  D (optional): the timing
+    barrier and max over ranks."""
     import torch
     S = importlib.import_module("dem-rock-calibration_b200.surrogate")
     sweep = importlib.import_module("dem-rock-calibration_b200.sweep")
-    D = Dist(ws)
     torch.cuda.set_device(local)
     J = S.UniaxialSolver(n=2000, seed=5 + rank, device=local)
     lo = np.array([v[0] for v in sweep.SWEEP_SPACE.values()])
     hi = np.array([v[1] for v in sweep.SWEEP_SPACE.values()])
-    X = S.latin_box(args.cases, lo, hi, 1 + rank)
+    X = S.latin_box(cases, lo, hi, 1 + rank)
     for _ in range(max(1, min(args.warmup, 3))):
         J(X[:2])                                       # kernel loading, allocator warm-up
-    D.barrier()
+    if D is not None:
+        D.barrier()
     clk = Clocks(local)
     t0 = time.perf_counter()
     Yb = J(X)
     t_b = time.perf_counter() - t0
     clocks = clk.stop()
-    t_b = D.max(t_b)
-    k = min(args.cases, 32)
+    if D is not None:
+        t_b = D.max(t_b)
+    k = min(cases, plain_cases)
     t0 = time.perf_counter()
     Ys = np.vstack([J(X[i:i + 1]) for i in range(k)])
     t_s = time.perf_counter() - t0
     agree = float(np.max(np.abs(Yb[:k] - Ys) / np.maximum(np.abs(Ys), 1e-30)))
-    value = D.sum(float(args.cases)) / t_b * 3600.0
-    plain = D.sum(float(k) / t_s * 3600.0)
+    return dict(n=J.rad.size, cases=cases, t_b=t_b, plain_cases=k, t_s=t_s, agree=agree, clocks=clocks,
+                ucs=[float(Yb[:, 0].min()), float(Yb[:, 0].max())])
+
+
+def run_solves(args, ws, rank, local):
+    """Calibration solves per hour, batched against plain (solves_measure);
+    every rank solves its own cases (weak scaling)."""
+    D = Dist(ws)
+    m = solves_measure(args, rank, local, args.cases, 32, D)
+    value = D.sum(float(args.cases)) / m["t_b"] * 3600.0
+    plain = D.sum(float(m["plain_cases"]) / m["t_s"] * 3600.0)
     line = {
         "metric": "calibration solves/hour", "value": value, "unit": "solves/hour", "n_gpus": ws, "steps": 1,
-        "warmup": max(1, min(args.warmup, 3)), "ms_per_step": t_b * 1e3, "higher_is_better": True,
+        "warmup": max(1, min(args.warmup, 3)), "ms_per_step": m["t_b"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded packing, Latin-hypercube micro-parameters)",
-        "config": {"workload": f"{args.cases} uniaxial solves of a {J.rad.size}-sphere cylinder to 70% post-peak "
+        "config": {"workload": f"{args.cases} uniaxial solves of a {m['n']}-sphere cylinder to 70% post-peak "
                                f"(or 1% strain) in one context",
                    "step": "the whole batch of solves, wall-clock (context, set-up, loading, results)",
-                   "plain": {"solves": k, "seconds": t_s, "value": plain,
+                   "plain": {"solves": m["plain_cases"], "seconds": m["t_s"], "value": plain,
                              "note": "one context per solve, one after another"},
                    "batched_over_plain": value / plain,
-                   "max_rel_difference_batched_vs_plain": agree,
-                   "ucs_gpa_range": [float(Yb[:, 0].min()), float(Yb[:, 0].max())],
+                   "max_rel_difference_batched_vs_plain": m["agree"],
+                   "ucs_gpa_range": m["ucs"],
                    "l2": "whole state inside the L2 (small specimens); no flush"},
-        "gpu_launches": None, "clocks": clocks, "roofline": None, "e2e": None, "cpu_baseline": None,
+        "gpu_launches": None, "clocks": m["clocks"], "roofline": None, "e2e": None, "cpu_baseline": None,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -873,6 +883,8 @@ def main() -> int:
     ap.add_argument("--cases", type=int, default=256, help="calibration_sweep: parameter sets")
     ap.add_argument("--pair-min-blocks", type=int, default=0, help="pair kernel register budget (blocks per SM)")
     ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--solves-cases", type=int, default=256,
+                    help="brazilian_disc: also time this many batched calibration solves (0: skip)")
     ap.add_argument("--post-peak-steps", type=int, default=200,
                     help="brazilian_disc: also time this many steps of the discs after the peak (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -984,6 +996,18 @@ def main() -> int:
                 "roofline_frac": m["achieved"] / m["peak"], "clocks": m["clocks"],
                 "note": "rank 0's discs loaded past the peak at ten times the platen speed until "
                         f"{args.damage:.0%} of the bonds broke (untimed), then timed"}
+    # calibration solves per hour, batched against one context per solve (this
+    # rank's GPU): the batching half of the configurations' second metric
+    solves = None
+    if args.solves_cases > 0 and args.workload == "brazilian_disc":
+        m = solves_measure(args, rank, local, args.solves_cases, 16)
+        b, pl = m["cases"] / m["t_b"] * 3600.0, m["plain_cases"] / m["t_s"] * 3600.0
+        solves = {"batched": b, "plain": pl, "unit": "solves/hour", "batched_over_plain": b / pl,
+                  "cases": m["cases"], "plain_solves": m["plain_cases"], "spheres": m["n"],
+                  "max_rel_difference_batched_vs_plain": m["agree"], "clocks": m["clocks"],
+                  "note": f"{m['cases']} uniaxial solves of a {m['n']}-sphere cylinder to 70% post-peak (or 1% "
+                          "strain), deterministic sums, Latin-hypercube micro-parameters, in one context, against "
+                          f"the first {m['plain_cases']} solved one context at a time; wall-clock per whole solve"}
     cpu = cpu_bpm = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, el, th, steps = cpu_baseline([spec], args.cpu_steps, 1, os.cpu_count() or 1)
@@ -1005,7 +1029,8 @@ def main() -> int:
                     "single_specimen": {"particles": spec.n, "value": spec.n * args.steps / (ms1 * 1e-3),
                                         "ms_per_step": ms1 / args.steps, "pair_ms": prof1["pair_ms"],
                                         "note": "state inside the L2"},
-                    "post_peak": post},
+                    "post_peak": post,
+                    "calibration_solves": solves},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

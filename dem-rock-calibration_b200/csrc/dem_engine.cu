@@ -76,8 +76,8 @@ static uint64_t now_ns() {
 // in this process.  Calibration work creates many contexts of similar sizes
 // one after another, and a cudaMalloc cost about 230 us on average in the
 // set-up of a 490k-sphere context (12 ms of its 28 ms), while cudaFree
-// synchronises the device.  A cached block serves a request of at most its
-// size and at least about 4/5 of it.  A block enters the cache only after its
+// synchronises the device.  Allocations are rounded up to size classes (four
+// per octave) and a cached block serves requests of its class.  A block enters the cache only after its
 // device has finished all queued work (a device synchronisation, the ordering
 // cudaFree gives), so a later user cannot race with kernels of the releasing
 // context.  Blocks are kept per CUDA context (its unique id): after a context
@@ -92,6 +92,15 @@ namespace blockcache {
 std::mutex mu;
 std::multimap<std::pair<unsigned long long, size_t>, void*> blocks;   // (context id, bytes) -> block
 size_t cached_bytes = 0;
+std::map<int, size_t> total_mem;   // device -> bytes of device memory
+
+// total memory of a device (cudaDeviceProp::totalGlobalMem)
+cudaError_t device_total_mem(int dev, size_t* out) {
+  cudaDeviceProp prop;
+  const cudaError_t e = cudaGetDeviceProperties(&prop, dev);
+  if (e == cudaSuccess) *out = prop.totalGlobalMem;
+  return e;
+}
 // the cache holds at most this share of the device's memory; a block released
 // beyond it goes back to the driver at once
 constexpr double kMaxShare = 0.4;
@@ -132,11 +141,21 @@ unsigned long long context_id() {
   return id;
 }
 
+// Block sizes come in classes, four per octave (256 B granularity below
+// 4 KiB): requests of slightly different sizes (a contact list that grows
+// between rebuilds) share blocks, at most 19% above the request.
+size_t size_class(size_t bytes) {
+  if (bytes <= 4096) return (bytes + 255) & ~(size_t)255;
+  int e = 63 - __builtin_clzll((unsigned long long)(bytes - 1));   // 2^e < bytes <= 2^(e+1)
+  const size_t step = (size_t)1 << (e - 2);                        // quarter of the octave
+  return (bytes + step - 1) / step * step;
+}
+
 void* take(unsigned long long ctx, size_t bytes, size_t* got) {
   if (!ctx) return nullptr;
   std::lock_guard<std::mutex> lk(mu);
   auto it = blocks.lower_bound({ctx, bytes});
-  while (it != blocks.end() && it->first.first == ctx && it->first.second <= bytes + bytes / 4 + (64u << 10)) {
+  while (it != blocks.end() && it->first.first == ctx && it->first.second == bytes) {
     void* p = it->second;
     const size_t b = it->first.second;
     it = blocks.erase(it);
@@ -156,12 +175,18 @@ void give(unsigned long long ctx, int dev, void* p, size_t bytes) {
   cudaGetDevice(&cur);
   if (cur != dev) cudaSetDevice(dev);
   const bool idle = cudaDeviceSynchronize() == cudaSuccess;
-  size_t free_b = 0, total_b = 0;
-  if (idle && cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) total_b = 0;
   if (cur != dev && cur >= 0) cudaSetDevice(cur);
   {
     std::lock_guard<std::mutex> lk(mu);
-    if (idle && ctx && cached_bytes + bytes <= (size_t)(kMaxShare * (double)total_b)) {
+    // the device's memory size, asked once per device (the query costs far
+    // more than a release)
+    auto tm = total_mem.find(dev);
+    if (tm == total_mem.end()) {
+      size_t t = 0;
+      if (device_total_mem(dev, &t) != cudaSuccess) t = 0;
+      tm = total_mem.emplace(dev, t).first;
+    }
+    if (idle && ctx && cached_bytes + bytes <= (size_t)(kMaxShare * (double)tm->second)) {
       blocks.emplace(std::make_pair(ctx, bytes), p);
       cached_bytes += bytes;
       return;
@@ -239,7 +264,7 @@ struct DBuf {
     } acc{t0};
     cudaGetDevice(&dev);
     ctx = blockcache::context_id();
-    const size_t bytes = (cnt * sizeof(T) + 255) & ~(size_t)255;
+    const size_t bytes = blockcache::size_class(cnt * sizeof(T));
     size_t got = 0;
     p = (T*)blockcache::take(ctx, bytes, &got);
     cudaError_t e = cudaSuccess;

@@ -77,10 +77,10 @@ static uint64_t now_ns() {
 // one after another, and a cudaMalloc cost about 230 us on average in the
 // set-up of a 490k-sphere context (12 ms of its 28 ms), while cudaFree
 // synchronises the device.  Allocations are rounded up to size classes (four
-// per octave) and a cached block serves requests of its class.  A block enters the cache only after its
-// device has finished all queued work (a device synchronisation, the ordering
-// cudaFree gives), so a later user cannot race with kernels of the releasing
-// context.  Blocks are kept per CUDA context (its unique id): after a context
+// per octave) and a cached block serves requests of its class.  A block
+// enters the cache only after its device has finished all queued work (a
+// device synchronisation, the ordering cudaFree gives), so a later user cannot
+// race with kernels of the releasing context.  Blocks are kept per CUDA context (its unique id): after a context
 // reset none of the old blocks is offered again.  Before a block is handed
 // out, the driver must still know it as an allocation of at least its size
 // starting at its address (a block that other code freed behind the cache's
@@ -143,7 +143,7 @@ unsigned long long context_id() {
 
 // Block sizes come in classes, four per octave (256 B granularity below
 // 4 KiB): requests of slightly different sizes (a contact list that grows
-// between rebuilds) share blocks, at most 19% above the request.
+// between rebuilds) share blocks, less than 25% above the request.
 size_t size_class(size_t bytes) {
   if (bytes <= 4096) return (bytes + 255) & ~(size_t)255;
   int e = 63 - __builtin_clzll((unsigned long long)(bytes - 1));   // 2^e < bytes <= 2^(e+1)
@@ -403,8 +403,6 @@ template <class Fn>
 static void parallel_ranges(uint32_t n, Fn fn) {
   parallel_chunks(n, chunk_count(n), [&](uint32_t, uint32_t k0, uint32_t k1) { fn(k0, k1); });
 }
-
-// 63-bit Morton interleave of three 21-bit coordinates
 
 struct SampleHost {
   dem_material mat{};
@@ -1739,7 +1737,6 @@ class Engine final : public EngineBase {
     return DEM_OK;
   }
 
-  // Runs until every sample has advanced max_steps steps or is done.
   // A sample whose state turned non-finite is stopped by the controller; the
   // others run on, and the call then returns DEM_ERR_NUMERIC.
   // ev (optional, two events): ev[0] is recorded once the state of the last

@@ -133,6 +133,10 @@ typedef struct {
   uint64_t steps;
   uint32_t stepsave;         /* number of records */
   uint32_t bonds_initial, bonds_now;  /* intact undirected bonds */
+  /* stale: events in which a particle moved past half the contact-list skin
+   * within a chunk of steps; the specimen then waited, without stepping,
+   * until the list was rebuilt, so no step ran on a list that could miss a
+   * contact (the count is informative: results do not depend on it) */
   int fracture, done, stale;
   int rebuilds;              /* contact-list builds of the context so far (all samples) */
   /* extensions (the reference outputs neither): chord Young modulus (GPa)
@@ -171,13 +175,17 @@ int dem_add_sample(dem_ctx* ctx, const dem_material* mat, const dem_loading* loa
                    const float* radii, uint32_t n, int32_t* sample);
 /* Uploads, Morton-sorts, creates bonds and the contact list. */
 int dem_setup(dem_ctx* ctx);
-/* Advances until every specimen met its stop condition or max_steps steps ran. */
+/* Advances every specimen max_steps steps or until it met its stop
+ * condition (a specimen that is ahead waits for the others); *steps_done:
+ * the largest number of steps a specimen advanced. */
 int dem_run(dem_ctx* ctx, uint64_t max_steps, uint64_t* steps_done);
-/* Advances exactly nsteps steps (finished specimens stay frozen). */
+/* Advances every specimen exactly nsteps steps (finished specimens stay frozen). */
 int dem_step(dem_ctx* ctx, uint32_t nsteps);
-/* Stage control for parity checks: bit 0 pair forces, bit 1 platens +
- * integration; bit 2 keeps the total force/moment of the step readable by
- * dem_get_particles instead of clearing the accumulators. */
+/* Stage control for parity checks: one step of the given stages, bit 0 pair
+ * forces, bit 1 platens + integration; bit 2 keeps the total force/moment of
+ * the step readable by dem_get_particles instead of clearing the
+ * accumulators.  The contact list is rebuilt first when dem_run would rebuild
+ * it. */
 int dem_step_stages(dem_ctx* ctx, int stages);
 int dem_sync(dem_ctx* ctx);
 

@@ -52,11 +52,13 @@ def ref():
 
 
 def P(a):
-    """data pointer of a numpy array (or NULL)."""
+    """Data pointer of a numpy array (or NULL), as an integer: every function
+    it is passed to declares the argument c_void_p, and the caller keeps the
+    array alive for the call."""
     if a is None:
         return None
-    assert a.flags["C_CONTIGUOUS"]
-    return a.ctypes.data_as(C.c_void_p)
+    assert a.flags.c_contiguous
+    return a.ctypes.data
 
 
 _vp = C.c_void_p
